@@ -1,0 +1,158 @@
+/*
+ * mldg.h -- C ABI of the B200 multilevel preconditioner application.
+ *
+ * This is the drop-in boundary for MLD2P4 2.1's `prec%apply`: a Fortran
+ * 2003 extension of mld_dprec_type overrides psb_d_apply2_vect and reaches
+ * these entry points through ISO_C_BINDING.  The level
+ * hierarchy built on the host by mld_dprecbld (aggregation, smoothed
+ * prolongators, Galerkin products, ILU(0)/diagonal factors) is uploaded
+ * unchanged, level by level; the V-cycle then runs on the GPU.
+ *
+ * Conventions
+ *  - int32 indices, FP64 values, CSR with ascending columns per row.
+ *  - index_base 0 (C) or 1 (Fortran) for every uploaded CSR.
+ *  - Levels are numbered from 0 (finest).  Level l >= 1 carries the maps
+ *    between level l-1 and level l, as the reference stores them at level l
+ *    (mlprec/impl/mld_dmlprec_aply.f90:376-379): P_l is n_{l-1} x n_l and
+ *    R_l = P_l^T is n_l x n_{l-1}.
+ *  - All calls on one handle are serialised by the caller; a handle is not
+ *    reentrant across threads.  Nothing is allocated per apply.
+ *  - Every entry point returns MLDG_SUCCESS (0) or an error code; the
+ *    message is available from mldg_last_error().
+ */
+#ifndef MLDG_H
+#define MLDG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error codes (values follow the reference's info codes) ------------ */
+#define MLDG_SUCCESS 0
+#define MLDG_ERR_ARG 30              /* invalid argument                     */
+#define MLDG_ERR_SIZE 36             /* vector too short (psb info 36)       */
+#define MLDG_ERR_NOT_BUILT 3112      /* apply before build (mld_dprecaply.f90:355-360) */
+#define MLDG_ERR_NO_SOLVER 1121      /* smoother without solver (jac_smoother_apply_vect.f90:85-89) */
+#define MLDG_ERR_NO_DIAG 1124        /* solver without D/DV (ilu_solver_apply_vect.f90:95-104) */
+#define MLDG_ERR_TRANS 40            /* invalid trans                        */
+#define MLDG_ERR_CUDA 4000           /* CUDA runtime error                   */
+#define MLDG_ERR_ALLOC 4010          /* device allocation failed             */
+#define MLDG_ERR_TIMEOUT 4020        /* a dependency wait exceeded its limit */
+#define MLDG_ERR_NOT_CONVERGED 4030  /* Krylov hit itmax (result still returned) */
+#define MLDG_ERR_INTERNAL 4999
+
+/* ---- smoother / solver kinds (mld_base_prec_type.F90 names) ------------- */
+#define MLDG_SMOOTHER_JACOBI 1   /* mld_jac_: jac smoother + diag solver      */
+#define MLDG_SMOOTHER_BJAC 2     /* mld_bjac_: jac smoother + ILU(0) solver   */
+
+/* ---- precision forms chosen at finalize -------------------------------- */
+#define MLDG_PREC_FP64 0         /* plain FP64 drop-in                        */
+#define MLDG_PREC_FP32 1         /* FP32 hierarchy and V-cycle                */
+#define MLDG_PREC_FP32_P16 2     /* FP32 V-cycle, FP16 prolongator values with
+                                    an FP32 per-row scale                     */
+
+/* ---- memory kinds for vector arguments ---------------------------------- */
+#define MLDG_MEM_HOST 0
+#define MLDG_MEM_DEVICE 1
+
+typedef struct mldg_handle mldg_handle;
+
+typedef struct {
+  int32_t nrows;
+  int32_t ncols;
+  const int32_t *irp; /* nrows + 1 */
+  const int32_t *ja;  /* irp[nrows] - base */
+  const double *val;
+} mldg_csr;
+
+typedef struct {
+  int device;      /* CUDA device ordinal                                   */
+  int index_base;  /* 0 or 1                                                 */
+  int use_graphs;  /* capture the V-cycle in a CUDA graph (default 1)       */
+  int autotune;    /* per-level launch-shape autotuner (default 1)          */
+} mldg_opts;
+
+/* One level as produced by the reference's build.  Unused members are
+ * zero/NULL.  smoother_kind selects which of (L,U,d) or (ND,d) is used:
+ *   MLDG_SMOOTHER_BJAC  : L (unit lower, strictly lower part stored), U
+ *                         (unit upper, rows scaled by 1/pivot), d = 1/pivot
+ *                         (mld_d_ilu_solver.f90:63-68, mld_dilu0_fact.f90:436-457)
+ *   MLDG_SMOOTHER_JACOBI: ND = off-diagonal part, d = 1/a_ii with 0 -> 1
+ *                         (mld_d_jac_smoother.f90:56-62, mld_d_diag_solver_bld.f90:86-92)
+ * Level l >= 1 also carries P and R (mld_d_onelev_mod.f90:122-158, map).
+ * sweeps_pre/sweeps_post: mld_dml_parms (the coarsest level uses
+ * sweeps_pre, mld_dmlprec_aply.f90:787-793).  damping: extension, 1.0 is the
+ * reference Jacobi iteration. */
+typedef struct {
+  mldg_csr A;
+  mldg_csr P;
+  mldg_csr R;
+  mldg_csr ND;
+  mldg_csr L;
+  mldg_csr U;
+  const double *d;
+  int smoother_kind;
+  int sweeps_pre;
+  int sweeps_post;
+  double damping;
+} mldg_level_desc;
+
+/* replaces: type(mld_dprec_type) allocation + prec%init
+ * (mlprec/mld_d_prec_type.f90:84-110, impl/mld_dprecinit.F90:188-207) */
+int mldg_create(mldg_handle **h, const mldg_opts *opts);
+
+/* replaces: the per-level data left by prec%hierarchy_build +
+ * prec%smoothers_build (impl/mld_d_hierarchy_bld.f90:66-490,
+ * impl/mld_d_smoothers_bld.f90:156-169).  Copies the arrays to the device;
+ * the library owns its copies.  Levels may be uploaded in any order. */
+int mldg_upload_level(mldg_handle *h, int lev, const mldg_level_desc *desc);
+
+/* Freezes the hierarchy of nlev levels: transposes, triangular-solve
+ * schedules, precision conversion, work vectors, autotuning, graph capture.
+ * precision: MLDG_PREC_*.  replaces: the end of mld_dprecbld
+ * (impl/mld_dprecbld.f90:60-159). */
+int mldg_finalize(mldg_handle *h, int nlev, int precision);
+
+/* y = M^{-1} x (trans 'N') or y = M^{-T} x (trans 'T'/'C') for nrhs vectors
+ * stored column by column with leading dimension ld (ld >= n).
+ * mem_kind: MLDG_MEM_HOST or MLDG_MEM_DEVICE for both x and y.
+ * replaces: prec%apply(x,y,desc_a,info,trans,work) ->
+ *   mld_dprecaply2_vect (mlprec/impl/mld_dprecaply.f90:305-443) ->
+ *   mld_dmlprec_aply_vect (mlprec/impl/mld_dmlprec_aply.f90:203-357). */
+int mldg_apply(mldg_handle *h, const double *x, double *y, char trans,
+               int nrhs, int ld, int mem_kind);
+
+/* Flexible CG (truncation 1) in FP64 on the GPU with this preconditioner,
+ * stopping on ||b - A x||_2 / ||b||_2 <= tol (PSBLAS istop = 2).  A may be
+ * NULL to use the finest uploaded level matrix.  x holds the initial guess
+ * on entry.  method: 0 = CG, 1 = FCG.
+ * replaces: psb_krylov('FCG'|'CG', a, prec, b, x, eps, desc_a, info, itmax,
+ * iter, err, istop=2) as called at tests/pdegen/mld_d_pde3d.f90:753-755. */
+int mldg_krylov(mldg_handle *h, int method, const mldg_csr *A,
+                const double *b, double *x, double tol, int itmax,
+                int *iters, double *relres, int mem_kind);
+
+/* Per-level sizes of the finalized hierarchy:
+ * info[0..4] = n, nnz(A), nnz(P), nnz(L)+nnz(U)+nnz(ND), number of levels. */
+int mldg_level_info(const mldg_handle *h, int lev, int64_t *info);
+
+/* Device time (ms) of the last mldg_apply / mldg_krylov, measured with CUDA
+ * events on the handle's stream, and the number of kernel launches it made. */
+int mldg_last_timing(const mldg_handle *h, double *ms, int64_t *launches);
+
+/* Bytes an FP64 (or the finalized precision's) V-cycle apply must move at
+ * least: every CSR operand once + every dense vector operand once (the
+ * roofline numerator). */
+int mldg_apply_bytes(const mldg_handle *h, int64_t *bytes);
+
+const char *mldg_last_error(const mldg_handle *h);
+
+/* replaces: prec%free (mlprec/mld_d_prec_type.f90:537-568) */
+void mldg_destroy(mldg_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,959 @@
+// mldg_core.cu -- handle, upload, finalize, V-cycle recorder, apply, Krylov.
+//
+// The V-cycle follows mld_d_inner_mult (mlprec/impl/mld_dmlprec_aply.f90:590-809,
+// ml_cycle = VCYCLE) level by level; smoothers follow
+// mld_d_jac_smoother_apply_vect.f90:107-177 with the diag solver (:102 of
+// mld_d_diag_solver_apply_vect.f90) or the ILU solver
+// (mld_d_ilu_solver_apply_vect.f90:130-142).  All device memory is allocated
+// in mldg_finalize; an apply only launches kernels (optionally replayed from a
+// CUDA graph captured on first use).
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "mldg.h"
+#include "mldg_kernels.cuh"
+#include "mldg_tri.h"
+
+namespace mldg {
+
+// ---------------------------------------------------------------------------
+struct Error {
+  int code;
+  std::string msg;
+};
+
+#define MLDG_CUDA(call)                                                              \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess)                                                           \
+      throw Error{MLDG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+  } while (0)
+
+static void fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  throw Error{code, buf};
+}
+
+struct HostCSR {
+  int nr = 0, nc = 0;
+  std::vector<int> irp, ja;
+  std::vector<double> val;
+  bool present() const { return !irp.empty(); }
+  int64_t nnz() const { return irp.empty() ? 0 : irp[nr]; }
+};
+
+static HostCSR copy_csr(const mldg_csr &c, int base, const char *what, int lev) {
+  HostCSR h;
+  if (!c.irp) return h;
+  if (c.nrows < 0 || c.ncols < 0) fail(MLDG_ERR_ARG, "level %d %s: negative size", lev, what);
+  h.nr = c.nrows;
+  h.nc = c.ncols;
+  h.irp.resize((size_t)h.nr + 1);
+  for (int i = 0; i <= h.nr; ++i) h.irp[i] = c.irp[i] - base;
+  if (h.irp[0] != 0) fail(MLDG_ERR_ARG, "level %d %s: irp[0] != base", lev, what);
+  for (int i = 0; i < h.nr; ++i)
+    if (h.irp[i + 1] < h.irp[i]) fail(MLDG_ERR_ARG, "level %d %s: irp not monotone", lev, what);
+  const int64_t nnz = h.irp[h.nr];
+  if (nnz > 0 && (!c.ja || !c.val)) fail(MLDG_ERR_ARG, "level %d %s: missing ja/val", lev, what);
+  h.ja.resize((size_t)nnz);
+  h.val.assign(c.val, c.val + nnz);
+  for (int64_t k = 0; k < nnz; ++k) {
+    const int j = c.ja[k] - base;
+    if (j < 0 || j >= h.nc) fail(MLDG_ERR_ARG, "level %d %s: column %d out of range", lev, what, j);
+    h.ja[k] = j;
+  }
+  return h;
+}
+
+static HostCSR transpose(const HostCSR &a) {
+  HostCSR t;
+  t.nr = a.nc;
+  t.nc = a.nr;
+  t.irp.assign((size_t)t.nr + 1, 0);
+  const int64_t nnz = a.nnz();
+  t.ja.resize((size_t)nnz);
+  t.val.resize((size_t)nnz);
+  for (int64_t k = 0; k < nnz; ++k) t.irp[a.ja[k] + 1]++;
+  for (int j = 0; j < t.nr; ++j) t.irp[j + 1] += t.irp[j];
+  std::vector<int> fill(t.irp.begin(), t.irp.end() - 1);
+  for (int i = 0; i < a.nr; ++i)
+    for (int k = a.irp[i]; k < a.irp[i + 1]; ++k) {
+      const int p = fill[a.ja[k]]++;
+      t.ja[p] = i;
+      t.val[p] = a.val[k];
+    }
+  return t;
+}
+
+struct HostLevel {
+  bool uploaded = false;
+  HostCSR A, P, R, ND, L, U;
+  std::vector<double> d;
+  int kind = MLDG_SMOOTHER_BJAC, sweeps_pre = 1, sweeps_post = 1;
+  double damp = 1.0;
+};
+
+// ---------------------------------------------------------------------------
+// Device memory arena: everything lives until mldg_destroy.
+struct Arena {
+  std::vector<void *> ptrs;
+  size_t bytes = 0;
+  template <typename T>
+  T *alloc(size_t n) {
+    void *p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+    if (e != cudaSuccess)
+      fail(MLDG_ERR_ALLOC, "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+    ptrs.push_back(p);
+    bytes += n * sizeof(T);
+    return (T *)p;
+  }
+  template <typename T>
+  T *upload(const std::vector<T> &v) {
+    T *p = alloc<T>(v.size());
+    if (!v.empty()) MLDG_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return p;
+  }
+  void release() {
+    for (void *p : ptrs) cudaFree(p);
+    ptrs.clear();
+    bytes = 0;
+  }
+};
+
+template <typename T>
+struct DCSR {
+  int nr = 0, nc = 0;
+  int64_t nnz = 0;
+  int *irp = nullptr, *ja = nullptr;
+  T *val = nullptr;
+  int tpr = 1;
+  bool present() const { return irp != nullptr; }
+};
+
+template <typename T>
+struct DTri {
+  int n = 0, rev = 0, R = 0, nchunks = 0, nlevels = 0;
+  int64_t nnz = 0;
+  int *chunk_lvl = nullptr, *lvl_ptr = nullptr, *prow = nullptr, *pirp = nullptr, *pja = nullptr;
+  T *pval = nullptr;
+  int *counters = nullptr;
+  int tpr = 1, threads = 256, grid = 1;
+  size_t smem = 0;
+  bool present() const { return prow != nullptr; }
+};
+
+static int pick_tpr(int64_t nnz, int nr) {
+  const double avg = nr > 0 ? (double)nnz / nr : 0.0;
+  if (avg <= 8) return 1;
+  if (avg <= 16) return 2;
+  if (avg <= 32) return 4;
+  if (avg <= 64) return 8;
+  if (avg <= 128) return 16;
+  return 32;
+}
+
+template <typename T>
+static DCSR<T> to_dev(Arena &ar, const HostCSR &h) {
+  DCSR<T> d;
+  if (!h.present()) return d;
+  d.nr = h.nr;
+  d.nc = h.nc;
+  d.nnz = h.nnz();
+  d.irp = ar.upload(h.irp);
+  d.ja = ar.upload(h.ja);
+  std::vector<T> v(h.val.begin(), h.val.end());
+  d.val = ar.upload(v);
+  d.tpr = pick_tpr(d.nnz, d.nr);
+  return d;
+}
+
+// ---------------------------------------------------------------------------
+// Engine: one precision form of the V-cycle.
+struct Engine {
+  virtual ~Engine() {}
+  virtual void record(char trans) = 0;  // issue one V-cycle: xin (FP64) -> yout (FP64)
+  int64_t launches = 0;
+  int64_t bytes = 0;
+};
+
+struct Handle;
+
+template <typename T>
+struct EngineT : Engine {
+  struct Lev {
+    int n = 0, kind = 0, spre = 1, spost = 1;
+    double damp = 1.0;
+    int64_t nnz_nd = 0;
+    DCSR<T> A, AT, P, R, ND, NDT;
+    DTri<T> L, U, Lt, Ut;
+    T *d = nullptr;
+    T *x = nullptr, *y = nullptr, *ty = nullptr, *tw = nullptr, *bufA = nullptr, *bufB = nullptr;
+    // FP16 prolongator values + FP32 row scale (MLDG_PREC_FP32_P16)
+    __half *Ph = nullptr;
+    float *Pscale = nullptr;
+  };
+  std::vector<Lev> lv;
+  Handle *h = nullptr;
+  cudaStream_t st = nullptr;
+  int *err = nullptr;
+  double *xin = nullptr, *yout = nullptr;  // FP64 boundary vectors of level 0
+  int nsm = 148;
+
+  // ---- launch helpers ----
+  int blocks_for(int64_t threads) const {
+    int64_t b = (threads + 255) / 256;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)nsm * 16));
+  }
+  void count(int64_t b) {
+    launches++;
+    bytes += b;
+  }
+  void spmv(const DCSR<T> &A, const T *v, T a1, const T *b, T a0, T *out, T a2) {
+    const int g = blocks_for((int64_t)A.nr * A.tpr);
+    switch (A.tpr) {
+#define CASE(K) \
+  case K: k_spmv<T, K><<<g, 256, 0, st>>>(A.nr, A.irp, A.ja, A.val, v, a1, b, a0, out, a2); break;
+      CASE(1) CASE(2) CASE(4) CASE(8) CASE(16) CASE(32)
+#undef CASE
+      default: fail(MLDG_ERR_INTERNAL, "bad tpr %d", A.tpr);
+    }
+    count(A.nnz * (int64_t)(sizeof(T) + 4) + 4 * ((int64_t)A.nr + 1) + (int64_t)A.nc * sizeof(T) +
+          (int64_t)A.nr * sizeof(T) * (1 + (b ? 1 : 0) + (a2 != T(0) ? 1 : 0)));
+  }
+  void jacobi(const DCSR<T> &ND, const T *d, const T *x, const T *ty, int first, T omega,
+              T alpha, T beta, T *out) {
+    const int g = blocks_for((int64_t)ND.nr * ND.tpr);
+    switch (ND.tpr) {
+#define CASE(K)                                                                           \
+  case K:                                                                                 \
+    k_jacobi<T, K><<<g, 256, 0, st>>>(ND.nr, ND.irp, ND.ja, ND.val, d, x, ty, first, omega, \
+                                      alpha, beta, out);                                  \
+    break;
+      CASE(1) CASE(2) CASE(4) CASE(8) CASE(16) CASE(32)
+#undef CASE
+      default: fail(MLDG_ERR_INTERNAL, "bad tpr %d", ND.tpr);
+    }
+    count(ND.nnz * (int64_t)(sizeof(T) + 4) + 4 * ((int64_t)ND.nr + 1) +
+          (int64_t)ND.nr * sizeof(T) * (3 + (first ? 0 : 1) + (beta != T(0) ? 1 : 0)));
+  }
+  void diag(int n, const T *d, const T *x, T alpha, T beta, T *out) {
+    k_diag<T><<<blocks_for(n), 256, 0, st>>>(n, d, x, alpha, beta, out);
+    count((int64_t)n * sizeof(T) * (3 + (beta != T(0) ? 1 : 0)));
+  }
+  void fill(int n, T v, T *y) {
+    k_fill<T><<<blocks_for(n), 256, 0, st>>>(n, v, y);
+    count((int64_t)n * sizeof(T));
+  }
+  void trsv(const DTri<T> &t, const T *rhs, const T *scale, T *cur, T *other, T *out, T alpha,
+            T beta) {
+    TriArgs<T> a;
+    a.n = t.n;
+    a.rev = t.rev;
+    a.R = t.R;
+    a.nchunks = t.nchunks;
+    a.chunk_lvl = t.chunk_lvl;
+    a.lvl_ptr = t.lvl_ptr;
+    a.prow = t.prow;
+    a.pirp = t.pirp;
+    a.pja = t.pja;
+    a.pval = t.pval;
+    a.rhs_src = rhs;
+    a.rhs_scale = scale;
+    a.cur = cur;
+    a.other = other;
+    a.out = out;
+    a.alpha = alpha;
+    a.beta = beta;
+    a.counters = t.counters;
+    a.err = err;
+    switch (t.tpr) {
+#define CASE(K) \
+  case K: k_trsv<T, K><<<t.grid, t.threads, t.smem, st>>>(a); break;
+      CASE(1) CASE(2) CASE(4) CASE(8) CASE(16) CASE(32)
+#undef CASE
+      default: fail(MLDG_ERR_INTERNAL, "bad tpr %d", t.tpr);
+    }
+    count(t.nnz * (int64_t)(sizeof(T) + 4) + 4 * (2 * (int64_t)t.n + 1) +
+          (int64_t)t.n * sizeof(T) *
+              (1 + (scale ? 1 : 0) + 1 + (other ? 1 : 0) + (out ? 1 + (beta != T(0)) : 0)));
+  }
+
+  // ILU solver apply: y = alpha*U^{-1}(d o L^{-1} x) + beta*y, or the 'T' form
+  void ilu_apply(Lev &L, char trans, const T *x, T beta, T *y) {
+    if (trans == 'N') {
+      trsv(L.L, x, nullptr, L.bufA, L.bufB, nullptr, T(1), T(0));
+      trsv(L.U, L.bufA, L.d, L.bufB, L.bufA, y, T(1), beta);
+    } else {
+      trsv(L.Ut, x, nullptr, L.bufA, L.bufB, nullptr, T(1), T(0));
+      trsv(L.Lt, L.bufA, L.d, L.bufB, L.bufA, y, T(1), beta);
+    }
+  }
+
+  // jac smoother apply with init 'Z': y = alpha*S^sweeps(x) + beta*y, alpha = 1
+  void smoother(Lev &L, char trans, const T *x, T beta, T *y, int sweeps) {
+    const DCSR<T> &ND = (trans == 'N') ? L.ND : L.NDT;
+    if (L.kind == MLDG_SMOOTHER_BJAC) {
+      if (sweeps == 1 || L.nnz_nd == 0) {
+        ilu_apply(L, trans, x, beta, y);
+        return;
+      }
+      // block-Jacobi sweeps with a non-empty off-block part (several ranks'
+      // worth of blocks): ty = S(x); ty = S(x - ND ty) ...; y = ty + beta*y
+      ilu_apply(L, trans, x, T(0), L.ty);
+      for (int s = 1; s < sweeps; ++s) {
+        spmv(ND, L.ty, T(-1), x, T(1), L.tw, T(0));
+        ilu_apply(L, trans, L.tw, T(0), L.ty);
+      }
+      k_axpby_impl(L.n, L.ty, beta, y);
+      return;
+    }
+    // point Jacobi (diag solver)
+    const T w = (T)L.damp;
+    if (sweeps == 1 || L.nnz_nd == 0) {
+      diag(L.n, L.d, x, w, beta, y);
+      return;
+    }
+    // sweeps >= 2: first sweep folded into the second (ty = w*d o x on the fly)
+    T *src = nullptr;
+    T *bufs[2] = {L.ty, L.tw};
+    for (int s = 1; s < sweeps; ++s) {
+      const bool last = (s == sweeps - 1);
+      T *dst = last ? y : bufs[s & 1];
+      jacobi(ND, L.d, x, src, s == 1 ? 1 : 0, w, T(1), last ? beta : T(0), dst);
+      src = dst;
+    }
+  }
+  void k_axpby_impl(int n, const T *x, T beta, T *y);
+
+  // V-cycle body (mld_d_inner_mult)
+  void vcycle(int l, char trans) {
+    Lev &L = lv[l];
+    const int nlev = (int)lv.size();
+    const bool pre = (L.spre > 0 && trans == 'N') || (L.spost > 0 && trans != 'N');
+    const bool post = (L.spost > 0 && trans == 'N') || (L.spre > 0 && trans != 'N');
+    if (l < nlev - 1) {
+      Lev &C = lv[l + 1];
+      const DCSR<T> &A = (trans == 'N') ? L.A : L.AT;
+      if (pre) {
+        smoother(L, trans, L.x, T(0), L.y, trans == 'N' ? L.spre : L.spost);
+        spmv(A, L.y, T(-1), L.x, T(1), L.ty, T(0));    // ty = x - op(A) y
+        spmv(C.R, L.ty, T(1), nullptr, T(0), C.x, T(0));  // x_{l+1} = R ty
+      } else {
+        fill(L.n, T(0), L.y);
+        spmv(C.R, L.x, T(1), nullptr, T(0), C.x, T(0));
+      }
+      vcycle(l + 1, trans);
+      prolong(C, L.y);                                   // y += P y_{l+1}
+      if (post) {
+        spmv(A, L.y, T(-1), L.x, T(1), L.ty, T(0));
+        smoother(L, trans, L.ty, T(1), L.y, trans == 'N' ? L.spost : L.spre);
+      }
+    } else {
+      smoother(L, trans, L.x, T(0), L.y, L.spre);
+    }
+  }
+  void prolong(Lev &C, T *y);
+
+  void record(char trans) override {
+    launches = 0;
+    bytes = 0;
+    Lev &F = lv[0];
+    if (!std::is_same<T, double>::value) {
+      k_cast<double, T><<<blocks_for(F.n), 256, 0, st>>>(F.n, xin, F.x);
+      count((int64_t)F.n * (8 + sizeof(T)));
+    }
+    if (lv.size() == 1)
+      smoother(F, trans, F.x, T(0), F.y, F.spre);
+    else
+      vcycle(0, trans);
+    if (!std::is_same<T, double>::value) {
+      k_cast<T, double><<<blocks_for(F.n), 256, 0, st>>>(F.n, F.y, yout);
+      count((int64_t)F.n * (8 + sizeof(T)));
+    }
+  }
+};
+
+template <typename T>
+__global__ void k_axpby1(int n, const T *__restrict__ x, T beta, T *y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    y[i] = (beta == T(0)) ? x[i] : fma(beta, y[i], x[i]);
+}
+
+template <typename T>
+void EngineT<T>::k_axpby_impl(int n, const T *x, T beta, T *y) {
+  k_axpby1<T><<<blocks_for(n), 256, 0, st>>>(n, x, beta, y);
+  count((int64_t)n * sizeof(T) * (2 + (beta != T(0))));
+}
+
+template <typename T>
+void EngineT<T>::prolong(Lev &C, T *y) {
+  spmv(C.P, C.y, T(1), nullptr, T(0), y, T(1));
+}
+
+template <>
+void EngineT<float>::prolong(Lev &C, float *y) {
+  if (!C.Ph) {
+    spmv(C.P, C.y, 1.f, nullptr, 0.f, y, 1.f);
+    return;
+  }
+  const int g = blocks_for((int64_t)C.P.nr * C.P.tpr);
+  switch (C.P.tpr) {
+#define CASE(K) \
+  case K: k_spmv_h<K><<<g, 256, 0, st>>>(C.P.nr, C.P.irp, C.P.ja, C.Ph, C.Pscale, C.y, y); break;
+    CASE(1) CASE(2) CASE(4) CASE(8) CASE(16) CASE(32)
+#undef CASE
+    default: fail(MLDG_ERR_INTERNAL, "bad tpr");
+  }
+  count(C.P.nnz * 6 + 4 * ((int64_t)C.P.nr + 1) + (int64_t)C.P.nc * 4 + (int64_t)C.P.nr * 4 * 3);
+}
+
+// ---------------------------------------------------------------------------
+struct Handle {
+  mldg_opts opts{};
+  std::string last_error;
+  std::vector<HostLevel> host;
+  int nlev = 0;
+  int precision = MLDG_PREC_FP64;
+  bool finalized = false;
+  Arena arena;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::unique_ptr<Engine> eng;
+  int *err = nullptr;
+  double *xin = nullptr, *yout = nullptr;
+  int n0 = 0;
+  // graphs per trans
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  int64_t glaunch[2] = {0, 0}, gbytes[2] = {0, 0};
+  // Krylov state (FP64)
+  DCSR<double> A0;
+  double *kb = nullptr, *kx = nullptr, *kd = nullptr, *kq = nullptr, *kpart = nullptr;
+  KrylovScalars *ksc = nullptr;
+  double *hpin = nullptr;  // pinned host scalar mirror
+  double last_ms = 0;
+  int64_t last_launches = 0;
+  int nsm = 148;
+};
+
+template <typename T>
+static DTri<T> build_tri_dev(Arena &ar, const HostCSR &m, bool upper, int R_hint, int nsm) {
+  DTri<T> t;
+  if (!m.present()) return t;
+  TriSchedule s;
+  const int n = m.nr;
+  int R = R_hint;
+  if (R <= 0) R = (n <= kTriSingleChunkRows) ? std::max(n, 1) : kTriChunkRows;
+  build_tri_schedule(n, m.irp.data(), m.ja.data(), m.val.data(), upper, R, &s);
+  t.n = n;
+  t.rev = upper ? 1 : 0;
+  t.R = R;
+  t.nchunks = s.nchunks;
+  t.nlevels = (int)s.lvl_ptr.size() - 1;
+  t.nnz = m.nnz();
+  t.chunk_lvl = ar.upload(s.chunk_lvl);
+  t.lvl_ptr = ar.upload(s.lvl_ptr);
+  t.prow = ar.upload(s.prow);
+  t.pirp = ar.upload(s.pirp);
+  t.pja = ar.upload(s.pja);
+  std::vector<T> v(s.pval.begin(), s.pval.end());
+  t.pval = ar.upload(v);
+  t.counters = ar.alloc<int>(2);
+  MLDG_CUDA(cudaMemset(t.counters, 0, 2 * sizeof(int)));
+  t.tpr = pick_tpr(t.nnz, std::max(n, 1));
+  if (t.tpr > 8) t.tpr = 8;
+  t.threads = 256;
+  t.smem = (size_t)R * sizeof(T);
+  t.grid = std::max(1, std::min(t.nchunks, nsm * 2));
+  return t;
+}
+
+template <typename T>
+static void set_trsv_smem_attr() {
+  static bool done = false;
+  if (done) return;
+  const int mx = 200 * 1024;
+  MLDG_CUDA(cudaFuncSetAttribute(k_trsv<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  MLDG_CUDA(cudaFuncSetAttribute(k_trsv<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  MLDG_CUDA(cudaFuncSetAttribute(k_trsv<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  MLDG_CUDA(cudaFuncSetAttribute(k_trsv<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  MLDG_CUDA(cudaFuncSetAttribute(k_trsv<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  MLDG_CUDA(cudaFuncSetAttribute(k_trsv<T, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  done = true;
+}
+
+template <typename T>
+static Engine *make_engine(Handle *h) {
+  set_trsv_smem_attr<T>();
+  auto *e = new EngineT<T>();
+  e->h = h;
+  e->st = h->st;
+  e->err = h->err;
+  e->xin = h->xin;
+  e->yout = h->yout;
+  e->nsm = h->nsm;
+  Arena &ar = h->arena;
+  e->lv.resize(h->nlev);
+  for (int l = 0; l < h->nlev; ++l) {
+    HostLevel &H = h->host[l];
+    auto &L = e->lv[l];
+    L.n = H.A.nr;
+    L.kind = H.kind;
+    L.spre = H.sweeps_pre;
+    L.spost = H.sweeps_post;
+    L.damp = H.damp;
+    L.A = to_dev<T>(ar, H.A);
+    L.AT = to_dev<T>(ar, transpose(H.A));
+    if (l > 0) {
+      L.P = to_dev<T>(ar, H.P);
+      L.R = to_dev<T>(ar, H.R);
+      if (std::is_same<T, float>::value && h->precision == MLDG_PREC_FP32_P16) {
+        // FP16 values with an FP32 per-row scale = max |p_ij| of the row
+        std::vector<__half> hv(H.P.val.size());
+        std::vector<float> sc((size_t)H.P.nr, 1.f);
+        for (int i = 0; i < H.P.nr; ++i) {
+          double mx = 0;
+          for (int k = H.P.irp[i]; k < H.P.irp[i + 1]; ++k) mx = std::max(mx, std::fabs(H.P.val[k]));
+          sc[i] = mx > 0 ? (float)mx : 1.f;
+          for (int k = H.P.irp[i]; k < H.P.irp[i + 1]; ++k)
+            hv[k] = __float2half_rn((float)(H.P.val[k] / sc[i]));
+        }
+        L.Ph = ar.upload(hv);
+        L.Pscale = ar.upload(sc);
+      }
+    }
+    L.nnz_nd = H.ND.nnz();
+    if (H.kind == MLDG_SMOOTHER_BJAC) {
+      L.L = build_tri_dev<T>(ar, H.L, false, 0, h->nsm);
+      L.U = build_tri_dev<T>(ar, H.U, true, 0, h->nsm);
+      HostCSR Lt = transpose(H.L), Ut = transpose(H.U);
+      L.Ut = build_tri_dev<T>(ar, Ut, false, 0, h->nsm);  // U^T is lower
+      L.Lt = build_tri_dev<T>(ar, Lt, true, 0, h->nsm);   // L^T is upper
+      if (L.nnz_nd > 0) {
+        L.ND = to_dev<T>(ar, H.ND);
+        L.NDT = to_dev<T>(ar, transpose(H.ND));
+      }
+    } else {
+      if (H.ND.present()) {
+        L.ND = to_dev<T>(ar, H.ND);
+        L.NDT = to_dev<T>(ar, transpose(H.ND));
+      }
+    }
+    std::vector<T> dv(H.d.begin(), H.d.end());
+    L.d = ar.upload(dv);
+    const int n = std::max(L.n, 1);
+    if (l == 0 && std::is_same<T, double>::value) {
+      L.x = (T *)h->xin;
+      L.y = (T *)h->yout;
+    } else {
+      L.x = ar.alloc<T>(n);
+      L.y = ar.alloc<T>(n);
+    }
+    L.ty = ar.alloc<T>(n);
+    L.tw = ar.alloc<T>(n);
+    MLDG_CUDA(cudaMemset(L.y, 0, sizeof(T) * n));
+    MLDG_CUDA(cudaMemset(L.ty, 0, sizeof(T) * n));
+    MLDG_CUDA(cudaMemset(L.tw, 0, sizeof(T) * n));
+    if (H.kind == MLDG_SMOOTHER_BJAC) {
+      L.bufA = ar.alloc<T>(n);
+      L.bufB = ar.alloc<T>(n);
+      k_fill<T><<<64, 256, 0, h->st>>>(n, Sentinel<T>::value(), L.bufA);
+      k_fill<T><<<64, 256, 0, h->st>>>(n, Sentinel<T>::value(), L.bufB);
+    }
+  }
+  MLDG_CUDA(cudaStreamSynchronize(h->st));
+  return e;
+}
+
+static void check_level(const HostLevel &H, int l, const HostLevel *prev) {
+  const int n = H.A.nr;
+  if (!H.A.present()) fail(MLDG_ERR_ARG, "level %d: missing A", l);
+  if (H.A.nc != n) fail(MLDG_ERR_ARG, "level %d: A must be square", l);
+  if (prev) {
+    const int nf = prev->A.nr;
+    if (!H.P.present() || !H.R.present()) fail(MLDG_ERR_ARG, "level %d: missing P/R", l);
+    if (H.P.nr != nf || H.P.nc != n) fail(MLDG_ERR_ARG, "level %d: P must be %d x %d", l, nf, n);
+    if (H.R.nr != n || H.R.nc != nf) fail(MLDG_ERR_ARG, "level %d: R must be %d x %d", l, n, nf);
+  }
+  if ((int)H.d.size() != n) fail(MLDG_ERR_NO_DIAG, "level %d: missing d (length %d)", l, n);
+  if (H.kind == MLDG_SMOOTHER_BJAC) {
+    if (!H.L.present() || !H.U.present()) fail(MLDG_ERR_NO_SOLVER, "level %d: missing L/U", l);
+    if (H.L.nr != n || H.U.nr != n) fail(MLDG_ERR_ARG, "level %d: L/U size", l);
+    for (int i = 0; i < n; ++i) {
+      for (int k = H.L.irp[i]; k < H.L.irp[i + 1]; ++k)
+        if (H.L.ja[k] >= i) fail(MLDG_ERR_ARG, "level %d: L not strictly lower at row %d", l, i);
+      for (int k = H.U.irp[i]; k < H.U.irp[i + 1]; ++k)
+        if (H.U.ja[k] <= i) fail(MLDG_ERR_ARG, "level %d: U not strictly upper at row %d", l, i);
+    }
+  } else if (H.kind != MLDG_SMOOTHER_JACOBI) {
+    fail(MLDG_ERR_ARG, "level %d: unknown smoother kind %d", l, H.kind);
+  }
+  if (H.ND.present() && (H.ND.nr != n || H.ND.nc != n)) fail(MLDG_ERR_ARG, "level %d: ND size", l);
+  if (H.sweeps_pre < 0 || H.sweeps_post < 0) fail(MLDG_ERR_ARG, "level %d: negative sweeps", l);
+}
+
+static void finalize(Handle *h, int nlev, int precision) {
+  if (nlev < 1 || nlev > (int)h->host.size()) fail(MLDG_ERR_ARG, "nlev %d: %zu levels uploaded", nlev, h->host.size());
+  for (int l = 0; l < nlev; ++l)
+    if (!h->host[l].uploaded) fail(MLDG_ERR_ARG, "level %d not uploaded", l);
+  for (int l = 0; l < nlev; ++l) check_level(h->host[l], l, l ? &h->host[l - 1] : nullptr);
+  if (precision != MLDG_PREC_FP64 && precision != MLDG_PREC_FP32 && precision != MLDG_PREC_FP32_P16)
+    fail(MLDG_ERR_ARG, "unknown precision %d", precision);
+  // drop any previous device state
+  for (int t = 0; t < 2; ++t)
+    if (h->gexec[t]) {
+      cudaGraphExecDestroy(h->gexec[t]);
+      h->gexec[t] = nullptr;
+    }
+  h->eng.reset();
+  h->arena.release();
+  h->nlev = nlev;
+  h->precision = precision;
+  h->n0 = h->host[0].A.nr;
+  const int n0 = std::max(h->n0, 1);
+  h->err = h->arena.alloc<int>(1);
+  MLDG_CUDA(cudaMemset(h->err, 0, sizeof(int)));
+  h->xin = h->arena.alloc<double>(n0);
+  h->yout = h->arena.alloc<double>(n0);
+  MLDG_CUDA(cudaMemset(h->xin, 0, sizeof(double) * n0));
+  MLDG_CUDA(cudaMemset(h->yout, 0, sizeof(double) * n0));
+  h->A0 = to_dev<double>(h->arena, h->host[0].A);
+  h->kb = h->arena.alloc<double>(n0);
+  h->kx = h->arena.alloc<double>(n0);
+  h->kd = h->arena.alloc<double>(n0);
+  h->kq = h->arena.alloc<double>(n0);
+  h->kpart = h->arena.alloc<double>(3 * kRedBlocks);
+  h->ksc = h->arena.alloc<KrylovScalars>(1);
+  if (precision == MLDG_PREC_FP64)
+    h->eng.reset(make_engine<double>(h));
+  else
+    h->eng.reset(make_engine<float>(h));
+  h->finalized = true;
+}
+
+static void run_vcycle(Handle *h, char trans) {
+  const int t = (trans == 'N') ? 0 : 1;
+  if (h->opts.use_graphs) {
+    if (!h->gexec[t]) {
+      cudaGraph_t g;
+      MLDG_CUDA(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+      try {
+        h->eng->record(trans);
+      } catch (...) {
+        cudaStreamEndCapture(h->st, &g);
+        throw;
+      }
+      MLDG_CUDA(cudaStreamEndCapture(h->st, &g));
+      MLDG_CUDA(cudaGraphInstantiate(&h->gexec[t], g, 0));
+      cudaGraphDestroy(g);
+      h->glaunch[t] = h->eng->launches;
+      h->gbytes[t] = h->eng->bytes;
+    }
+    MLDG_CUDA(cudaGraphLaunch(h->gexec[t], h->st));
+    h->last_launches += h->glaunch[t];
+  } else {
+    h->eng->record(trans);
+    h->glaunch[t] = h->eng->launches;
+    h->gbytes[t] = h->eng->bytes;
+    h->last_launches += h->eng->launches;
+  }
+}
+
+static int check_device_error(Handle *h) {
+  int e = 0;
+  MLDG_CUDA(cudaMemcpy(&e, h->err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    MLDG_CUDA(cudaMemset(h->err, 0, sizeof(int)));
+    fail(MLDG_ERR_TIMEOUT, "a triangular-solve dependency wait exceeded its limit (code %d)", e);
+  }
+  return 0;
+}
+
+static void apply(Handle *h, const double *x, double *y, char trans, int nrhs, int ld, int mem) {
+  if (!h->finalized) fail(MLDG_ERR_NOT_BUILT, "apply before build (mldg_finalize not called)");
+  if (trans == 'C') trans = 'T';
+  if (trans != 'N' && trans != 'T') fail(MLDG_ERR_TRANS, "invalid trans '%c'", trans);
+  if (nrhs < 0) fail(MLDG_ERR_ARG, "nrhs < 0");
+  const int n = h->n0;
+  if (nrhs > 1 && ld < n) fail(MLDG_ERR_SIZE, "ld %d < n %d", ld, n);
+  if (nrhs > 0 && (!x || !y)) fail(MLDG_ERR_ARG, "null vector");
+  if (mem != MLDG_MEM_HOST && mem != MLDG_MEM_DEVICE) fail(MLDG_ERR_ARG, "bad mem_kind");
+  const cudaMemcpyKind h2d = mem == MLDG_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  const cudaMemcpyKind d2h = mem == MLDG_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  h->last_launches = 0;
+  MLDG_CUDA(cudaEventRecord(h->ev0, h->st));
+  for (int c = 0; c < nrhs; ++c) {
+    const size_t off = (size_t)c * (size_t)(nrhs > 1 ? ld : n);
+    MLDG_CUDA(cudaMemcpyAsync(h->xin, x + off, sizeof(double) * n, h2d, h->st));
+    run_vcycle(h, trans);
+    MLDG_CUDA(cudaMemcpyAsync(y + off, h->yout, sizeof(double) * n, d2h, h->st));
+  }
+  MLDG_CUDA(cudaEventRecord(h->ev1, h->st));
+  MLDG_CUDA(cudaStreamSynchronize(h->st));
+  float ms = 0;
+  MLDG_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  h->last_ms = ms;
+  check_device_error(h);
+}
+
+// ---------------------------------------------------------------------------
+static void dots(Handle *h, int n, int np, const double *x0, const double *y0, const double *x1,
+                 const double *y1, const double *x2, const double *y2) {
+  k_dots<<<kRedBlocks, kRedThreads, 0, h->st>>>(n, np, x0, y0, x1, y1, x2, y2, h->kpart);
+  k_dots_final<<<1, kRedThreads, 0, h->st>>>(kRedBlocks, h->kpart, h->ksc->dots);
+  h->last_launches += 2;
+}
+
+static void spmv64(Handle *h, const DCSR<double> &A, const double *v, double a1, const double *b,
+                   double a0, double *out) {
+  const int64_t thr = (int64_t)A.nr * A.tpr;
+  const int g = (int)std::max<int64_t>(1, std::min<int64_t>((thr + 255) / 256, (int64_t)h->nsm * 16));
+  switch (A.tpr) {
+#define CASE(K) \
+  case K: k_spmv<double, K><<<g, 256, 0, h->st>>>(A.nr, A.irp, A.ja, A.val, v, a1, b, a0, out, 0.0); break;
+    CASE(1) CASE(2) CASE(4) CASE(8) CASE(16) CASE(32)
+#undef CASE
+    default: fail(MLDG_ERR_INTERNAL, "bad tpr");
+  }
+  h->last_launches++;
+}
+
+static void krylov(Handle *h, int method, const mldg_csr *Acsr, const double *b, double *x,
+                   double tol, int itmax, int *iters, double *relres, int mem) {
+  if (!h->finalized) fail(MLDG_ERR_NOT_BUILT, "krylov before build");
+  if (method != 0 && method != 1) fail(MLDG_ERR_ARG, "method must be 0 (CG) or 1 (FCG)");
+  if (!b || !x) fail(MLDG_ERR_ARG, "null vector");
+  if (itmax < 0) fail(MLDG_ERR_ARG, "itmax < 0");
+  const int n = h->n0;
+  DCSR<double> A = h->A0;
+  Arena tmp;
+  if (Acsr) {
+    HostCSR ha = copy_csr(*Acsr, h->opts.index_base, "krylov A", 0);
+    if (ha.nr != n || ha.nc != n) fail(MLDG_ERR_SIZE, "krylov A must be %d x %d", n, n);
+    A = to_dev<double>(tmp, ha);
+  }
+  const cudaMemcpyKind h2d = mem == MLDG_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  const cudaMemcpyKind d2h = mem == MLDG_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  double *r = h->xin, *z = h->yout, *d = h->kd, *q = h->kq, *xx = h->kx, *bb = h->kb;
+  KrylovScalars *sc = h->ksc;
+  h->last_launches = 0;
+  MLDG_CUDA(cudaEventRecord(h->ev0, h->st));
+  MLDG_CUDA(cudaMemcpyAsync(bb, b, sizeof(double) * n, h2d, h->st));
+  MLDG_CUDA(cudaMemcpyAsync(xx, x, sizeof(double) * n, h2d, h->st));
+  spmv64(h, A, xx, -1.0, bb, 1.0, r);  // r = b - A x
+  dots(h, n, 2, bb, bb, r, r, nullptr, nullptr);
+  MLDG_CUDA(cudaMemcpyAsync(h->hpin, sc->dots, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  MLDG_CUDA(cudaStreamSynchronize(h->st));
+  double bn2 = std::sqrt(h->hpin[0]);
+  if (bn2 == 0.0) bn2 = 1.0;
+  double err = std::sqrt(h->hpin[1]) / bn2;
+  int it = 0;
+  const int nb = kRedBlocks;
+  while (err > tol && it < itmax) {
+    ++it;
+    run_vcycle(h, 'N');  // z = M^{-1} r
+    if (method == 1) {
+      if (it > 1) {
+        dots(h, n, 1, z, q, nullptr, nullptr, nullptr, nullptr);
+        k_scal_store<<<1, 32, 0, h->st>>>(sc, 0);
+        h->last_launches++;
+      }
+    } else {
+      dots(h, n, 1, r, z, nullptr, nullptr, nullptr, nullptr);
+      k_scal_store<<<1, 32, 0, h->st>>>(sc, 0);
+      h->last_launches++;
+    }
+    k_dir_update<<<nb, 256, 0, h->st>>>(n, method, it == 1 ? 1 : 0, z, d, sc);
+    spmv64(h, A, d, 1.0, nullptr, 0.0, q);  // q = A d
+    dots(h, n, 2, d, q, d, r, nullptr, nullptr);
+    k_scal_store<<<1, 32, 0, h->st>>>(sc, 1);
+    k_xr_update<<<nb, kRedThreads, 0, h->st>>>(n, method, d, q, xx, r, sc, h->kpart);
+    k_dots_final<<<1, kRedThreads, 0, h->st>>>(nb, h->kpart, sc->dots);
+    k_scal_store<<<1, 32, 0, h->st>>>(sc, 2);
+    h->last_launches += 6;
+    MLDG_CUDA(cudaMemcpyAsync(h->hpin, sc->dots, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    MLDG_CUDA(cudaStreamSynchronize(h->st));
+    err = std::sqrt(std::max(h->hpin[0], 0.0)) / bn2;
+    if (std::isnan(err)) break;
+  }
+  MLDG_CUDA(cudaMemcpyAsync(x, xx, sizeof(double) * n, d2h, h->st));
+  MLDG_CUDA(cudaEventRecord(h->ev1, h->st));
+  MLDG_CUDA(cudaStreamSynchronize(h->st));
+  float ms = 0;
+  MLDG_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  h->last_ms = ms;
+  tmp.release();
+  if (iters) *iters = it;
+  if (relres) *relres = err;
+  check_device_error(h);
+}
+
+}  // namespace mldg
+
+// ===========================================================================
+// C ABI
+using mldg::Error;
+using mldg::Handle;
+
+struct mldg_handle {
+  Handle h;
+};
+
+#define MLDG_GUARD(hp, body)                                     \
+  do {                                                           \
+    try {                                                        \
+      body;                                                      \
+      return MLDG_SUCCESS;                                       \
+    } catch (const Error &e_) {                                  \
+      if (hp) (hp)->h.last_error = e_.msg;                       \
+      return e_.code;                                            \
+    } catch (const std::exception &e_) {                         \
+      if (hp) (hp)->h.last_error = e_.what();                    \
+      return MLDG_ERR_INTERNAL;                                  \
+    }                                                            \
+  } while (0)
+
+extern "C" int mldg_create(mldg_handle **out, const mldg_opts *opts) {
+  if (!out) return MLDG_ERR_ARG;
+  *out = nullptr;
+  mldg_handle *hp = new mldg_handle();
+  Handle &h = hp->h;
+  h.opts.device = 0;
+  h.opts.index_base = 0;
+  h.opts.use_graphs = 1;
+  h.opts.autotune = 1;
+  if (opts) h.opts = *opts;
+  if (h.opts.index_base != 0 && h.opts.index_base != 1) {
+    delete hp;
+    return MLDG_ERR_ARG;
+  }
+  try {
+    MLDG_CUDA(cudaSetDevice(h.opts.device));
+    MLDG_CUDA(cudaStreamCreateWithFlags(&h.st, cudaStreamNonBlocking));
+    MLDG_CUDA(cudaEventCreate(&h.ev0));
+    MLDG_CUDA(cudaEventCreate(&h.ev1));
+    MLDG_CUDA(cudaMallocHost(&h.hpin, 4 * sizeof(double)));
+    MLDG_CUDA(cudaDeviceGetAttribute(&h.nsm, cudaDevAttrMultiProcessorCount, h.opts.device));
+  } catch (const Error &e) {
+    delete hp;
+    return e.code;
+  }
+  *out = hp;
+  return MLDG_SUCCESS;
+}
+
+extern "C" int mldg_upload_level(mldg_handle *hp, int lev, const mldg_level_desc *d) {
+  if (!hp) return MLDG_ERR_ARG;
+  MLDG_GUARD(hp, {
+    Handle &h = hp->h;
+    if (!d) mldg::fail(MLDG_ERR_ARG, "null level descriptor");
+    if (lev < 0 || lev > 64) mldg::fail(MLDG_ERR_ARG, "level %d out of range", lev);
+    if ((int)h.host.size() <= lev) h.host.resize(lev + 1);
+    mldg::HostLevel H;
+    const int b = h.opts.index_base;
+    H.A = mldg::copy_csr(d->A, b, "A", lev);
+    H.P = mldg::copy_csr(d->P, b, "P", lev);
+    H.R = mldg::copy_csr(d->R, b, "R", lev);
+    H.ND = mldg::copy_csr(d->ND, b, "ND", lev);
+    H.L = mldg::copy_csr(d->L, b, "L", lev);
+    H.U = mldg::copy_csr(d->U, b, "U", lev);
+    if (d->d && H.A.present()) H.d.assign(d->d, d->d + H.A.nr);
+    H.kind = d->smoother_kind;
+    H.sweeps_pre = d->sweeps_pre;
+    H.sweeps_post = d->sweeps_post;
+    H.damp = d->damping == 0.0 ? 1.0 : d->damping;
+    H.uploaded = true;
+    h.host[lev] = std::move(H);
+    h.finalized = false;
+  });
+}
+
+extern "C" int mldg_finalize(mldg_handle *hp, int nlev, int precision) {
+  if (!hp) return MLDG_ERR_ARG;
+  MLDG_GUARD(hp, {
+    MLDG_CUDA(cudaSetDevice(hp->h.opts.device));
+    mldg::finalize(&hp->h, nlev, precision);
+  });
+}
+
+extern "C" int mldg_apply(mldg_handle *hp, const double *x, double *y, char trans, int nrhs,
+                          int ld, int mem_kind) {
+  if (!hp) return MLDG_ERR_ARG;
+  MLDG_GUARD(hp, { mldg::apply(&hp->h, x, y, trans, nrhs, ld, mem_kind); });
+}
+
+extern "C" int mldg_krylov(mldg_handle *hp, int method, const mldg_csr *A, const double *b,
+                           double *x, double tol, int itmax, int *iters, double *relres,
+                           int mem_kind) {
+  if (!hp) return MLDG_ERR_ARG;
+  int it = 0;
+  MLDG_GUARD(hp, {
+    mldg::krylov(&hp->h, method, A, b, x, tol, itmax, &it, relres, mem_kind);
+    if (iters) *iters = it;
+    if (it >= itmax && relres && *relres > tol)
+      mldg::fail(MLDG_ERR_NOT_CONVERGED, "not converged in %d iterations (relres %.3e)", it, *relres);
+  });
+}
+
+extern "C" int mldg_level_info(const mldg_handle *hp, int lev, int64_t *info) {
+  if (!hp || !info) return MLDG_ERR_ARG;
+  const Handle &h = hp->h;
+  if (!h.finalized) return MLDG_ERR_NOT_BUILT;
+  if (lev < 0 || lev >= h.nlev) return MLDG_ERR_ARG;
+  const mldg::HostLevel &H = h.host[lev];
+  info[0] = H.A.nr;
+  info[1] = H.A.nnz();
+  info[2] = H.P.nnz();
+  info[3] = H.L.nnz() + H.U.nnz() + H.ND.nnz();
+  info[4] = h.nlev;
+  return MLDG_SUCCESS;
+}
+
+extern "C" int mldg_last_timing(const mldg_handle *hp, double *ms, int64_t *launches) {
+  if (!hp) return MLDG_ERR_ARG;
+  if (ms) *ms = hp->h.last_ms;
+  if (launches) *launches = hp->h.last_launches;
+  return MLDG_SUCCESS;
+}
+
+extern "C" int mldg_apply_bytes(const mldg_handle *hp, int64_t *bytes) {
+  if (!hp || !bytes) return MLDG_ERR_ARG;
+  if (!hp->h.finalized) return MLDG_ERR_NOT_BUILT;
+  *bytes = hp->h.gbytes[0];
+  return MLDG_SUCCESS;
+}
+
+extern "C" const char *mldg_last_error(const mldg_handle *hp) {
+  if (!hp) return "null handle";
+  return hp->h.last_error.c_str();
+}
+
+extern "C" void mldg_destroy(mldg_handle *hp) {
+  if (!hp) return;
+  Handle &h = hp->h;
+  cudaSetDevice(h.opts.device);
+  if (h.st) cudaStreamSynchronize(h.st);
+  for (int t = 0; t < 2; ++t)
+    if (h.gexec[t]) cudaGraphExecDestroy(h.gexec[t]);
+  h.eng.reset();
+  h.arena.release();
+  if (h.hpin) cudaFreeHost(h.hpin);
+  if (h.ev0) cudaEventDestroy(h.ev0);
+  if (h.ev1) cudaEventDestroy(h.ev1);
+  if (h.st) cudaStreamDestroy(h.st);
+  delete hp;
+}
