@@ -1,0 +1,351 @@
+"""Benchmark: FCG to relative residual 1e-10 with the GPU V-cycle preconditioner.
+
+Workload (the plain FP64 drop-in at scale): -Lap u + (1/sqrt3)(u_x+u_y+u_z)
+on the unit cube, 7-point FD, h = 1/(idim+1), idim = 160 (4,096,000 rows,
+28,518,400 nnz), b = A*1, x0 = 0.  MLD2P4 'ML' preconditioner: decoupled
+smoothed aggregation (threshold 0.01, omega = 4/(3 ||D^-1 A||_inf)),
+coarsening to <= 2000 rows, V-cycle with 1 pre + 1 post sweep of
+block-Jacobi ILU(0) (or point Jacobi, --smoother JACOBI: 2 sweeps, damping
+0.8), coarsest level 4 sweeps of block-Jacobi ILU(0).  One step = one full
+FCG solve to 1e-10 (istop 2).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Each rank solves its own copy of the system (weak scaling: N independent
+solves, no data-path collective).  value = solves/s over the whole job,
+device-timed with CUDA events (max over ranks).  The reference arm times the
+CPU restatement of the reference's algorithm (the oracle) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "time-to-1e-10 residual (mixed vs FP64 GPU V-cycle); V-cycle apply HBM GB/s"
+S3 = 1.0 / np.sqrt(3.0)
+ISO = (1.0, 1.0, 1.0, S3, S3, S3, 0.0)
+
+
+def load_package():
+    name = "mld2p4_2_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    pkg_dir = os.path.join(ROOT, "mld2p4-2_b200")
+    spec = importlib.util.spec_from_file_location(
+        name, os.path.join(pkg_dir, "__init__.py"), submodule_search_locations=[pkg_dir])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # CPU baseline / reference arm only
+    return oracle
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampler run during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                out, _ = self.p.communicate(timeout=5)
+            except Exception:
+                self.p.kill()
+                out = ""
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": mx or None, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_problem(mld, idim):
+    a = mld.gen_pde3d(idim, 1, ISO)
+    b = a.matvec(np.ones(a.nrows))
+    return a, b
+
+
+def make_prec(mld, a, smoother, precision="FP64", device=0):
+    p = mld.MldPrec(device=device)
+    p.init("ML")
+    p.set("SMOOTHER_TYPE", smoother)
+    if smoother == "JACOBI":
+        p.set("SMOOTHER_SWEEPS", 2)
+        p.set("SMOOTHER_DAMPING", 0.8)
+    else:
+        p.set("SUB_SOLVE", "ILU")
+        p.set("SMOOTHER_SWEEPS", 1)
+    p.set("COARSE_SOLVE", "BJAC")
+    p.set("COARSE_SUBSOLVE", "ILU")
+    p.set("COARSE_SWEEPS", 4)
+    p.set("MIN_COARSE_SIZE", 2000)
+    p.set("AGGR_THRESH", 0.01)
+    p.set("PRECISION", precision)
+    p.build(a)
+    return p
+
+
+def cpu_solve_oracle(orc, a, smoother, eps):
+    sm = orc.BJAC if smoother == "BJAC" else orc.JACOBI
+    par = orc.default_params(smoother=sm, sweeps_pre=2 if smoother == "JACOBI" else 1,
+                             sweeps_post=2 if smoother == "JACOBI" else 1,
+                             jac_damp=0.8 if smoother == "JACOBI" else 1.0,
+                             coarse_solver=orc.BJAC, coarse_sweeps=4, min_coarse_size=2000)
+    ao = orc.CSR(a.irp, a.ja, a.val)
+    op = orc.Prec(par)
+    op.build(ao)
+    return ao, op
+
+
+def run_reference(args, rank, world):
+    """CPU reference arm: the oracle (restated reference algorithm) on host cores."""
+    if rank != 0:
+        return
+    mld = load_package()
+    orc = load_oracle()
+    a, b = build_problem(mld, args.idim)
+    ao, op = cpu_solve_oracle(orc, a, args.smoother, args.eps)
+    for _ in range(args.warmup):
+        orc.krylov("FCG", ao, op, b, eps=args.eps, itmax=500)
+    t0 = time.perf_counter()
+    its = []
+    for _ in range(args.steps):
+        _, it, rr, _ = orc.krylov("FCG", ao, op, b, eps=args.eps, itmax=500)
+        its.append(it)
+    dt = time.perf_counter() - t0
+    value = args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config(args, a, None),
+        "iterations": its[-1] if its else None,
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": orc.num_threads(),
+                         "kind": "port",
+                         "sample": f"{args.steps} full FCG solve(s) to {args.eps:g}, idim={args.idim}"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config(args, a, p):
+    c = {"workload": f"pdegen 3D convection-diffusion idim={args.idim} FP64, "
+                     f"ML V-cycle {args.smoother} smoother, FCG to {args.eps:g}",
+         "idim": args.idim, "rows": a.nrows, "nnz": a.nnz, "smoother": args.smoother,
+         "precision": args.precision, "parallelism": f"replicas x{args.gpus}",
+         "l2": "inputs larger than L2 (hierarchy > 1 GB resident in HBM)"}
+    if p is not None:
+        c["levels"] = [p.level_info(l)["n"] for l in range(p.nlev)]
+    return c
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    mld = load_package()
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_
+        dist = dist_
+    a, b = build_problem(mld, args.idim)
+    p = make_prec(mld, a, args.smoother, args.precision, device=dev)
+    n = a.nrows
+    # dominant kernel: the (kind, level) group with the largest device time
+    bd = torch.tensor(b, dtype=torch.float64, device=f"cuda:{dev}")
+    x0 = torch.zeros(n, dtype=torch.float64, device=f"cuda:{dev}")
+    xs = torch.zeros_like(x0)
+    torch.cuda.synchronize()
+    p.apply(bd, xs)  # first apply captures the graph
+    prof = p.profile("N")
+    groups = {}
+    for e in prof:
+        k = (e["kind_id"], e["level"])
+        g = groups.setdefault(k, [0.0, 0, 0])
+        g[0] += e["ms"]
+        g[1] += 1
+        g[2] += e["bytes"]
+    (dk, dl), (dms, dcnt, dbytes) = max(groups.items(), key=lambda kv: kv[1][0])
+    p.probe_set(dk, dl, 0)
+    apply_ms_prof = sum(e["ms"] for e in prof)
+
+    def solve(x_dev, b_dev):
+        x_dev.copy_(x0)
+        torch.cuda.synchronize()
+        _, it, rr = mld.krylov("FCG", a, p, b_dev, x_dev, eps=args.eps, itmax=500,
+                               use_prec_matrix=True)
+        ms, nl = p.last_timing()
+        return it, rr, ms, nl
+
+    for _ in range(args.warmup):
+        solve(xs, bd)
+    p.probe_read()
+    # timed region: device time from the library's CUDA events, max over ranks
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(dev) as clk:
+        tot_ms, launches, its = 0.0, 0, []
+        for _ in range(args.steps):
+            it, rr, ms, nl = solve(xs, bd)
+            tot_ms += ms
+            launches += nl
+            its.append(it)
+    torch.cuda.synchronize()
+    probe_ms, probe_cnt, probe_bytes = p.probe_read()
+    if dist is not None:
+        t = torch.tensor([tot_ms], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms = float(t.item())
+    err = float(torch.linalg.norm(xs - 1.0) / np.sqrt(n))
+    # end-to-end through the public API with host buffers (pinned)
+    bh = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    bh.copy_(torch.from_numpy(b))
+    xh = torch.zeros(n, dtype=torch.float64, pin_memory=True)
+    e2e_ms = 0.0
+    for s in range(args.steps):
+        xh.zero_()
+        _, it_h, _ = mld.krylov("FCG", a, p, bh, xh, eps=args.eps, itmax=500,
+                                use_prec_matrix=True)
+        e2e_ms += p.last_timing()[0]
+    if dist is not None:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    # apply alone (V-cycle), device-timed, for the HBM GB/s of the whole cycle
+    ap_ms = []
+    for _ in range(5):
+        p.apply(bd, xs)
+        ap_ms.append(p.last_timing()[0])
+    apply_ms = min(ap_ms)
+    apply_bytes = p.apply_bytes()
+    if rank != 0:
+        return
+    peak, peak_kind = peaks()
+    achieved = (probe_bytes * probe_cnt) / (probe_ms * 1e-3) / 1e9 if probe_ms > 0 else None
+    line = {
+        "metric": METRIC, "value": world * args.steps / (tot_ms * 1e-3), "unit": "solves/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "FP64" else "f32/f64",
+        "data": "synthetic", "config": config(args, a, p),
+        "iterations": its[-1], "time_to_1e-10_ms": tot_ms / args.steps,
+        "final_relres": rr, "max_abs_err_vs_ones": err,
+        "apply_ms": apply_ms, "apply_algorithmic_bytes": apply_bytes,
+        "apply_gbs": apply_bytes / (apply_ms * 1e-3) / 1e9,
+        "apply_roofline_frac": apply_bytes / (apply_ms * 1e-3) / 1e9 / peak,
+        "roofline": {"bound": "hbm", "kernel": f"{mld.KERNEL_NAMES[dk]} level {dl}",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if achieved else None, "traffic": None,
+                     "peak_source": peak_kind, "bytes_per_launch": probe_bytes,
+                     "avg_launch_ms": probe_ms / probe_cnt if probe_cnt else None,
+                     "launches_timed": probe_cnt,
+                     "share_of_apply": dms / apply_ms_prof if apply_ms_prof else None},
+        "e2e": {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "solves/s",
+                "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 8 * n},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        orc = load_oracle()
+        ao, op = cpu_solve_oracle(orc, a, args.smoother, args.eps)
+        t0 = time.perf_counter()
+        _, it_c, _, _ = orc.krylov("FCG", ao, op, b, eps=args.eps, itmax=500)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": 1.0 / dt, "unit": "solves/s", "cores": orc.num_threads(),
+                                "kind": "port",
+                                "sample": f"1 full FCG solve to {args.eps:g} ({it_c} iterations), "
+                                          f"idim={args.idim}, oracle (C restatement)"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--idim", type=int, default=160)
+    ap.add_argument("--smoother", default="BJAC", choices=["BJAC", "JACOBI"])
+    ap.add_argument("--precision", default="FP64", choices=["FP64", "FP32", "FP32_P16"])
+    ap.add_argument("--eps", type=float, default=1e-10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        # rank 0 alone times the CPU reference; other ranks exit without work
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    run_ours(args, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

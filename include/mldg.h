@@ -147,6 +147,32 @@ int mldg_last_timing(const mldg_handle *h, double *ms, int64_t *launches);
  * roofline numerator). */
 int mldg_apply_bytes(const mldg_handle *h, int64_t *bytes);
 
+/* ---- diagnostics: per-kernel device time ------------------------------- */
+#define MLDG_KERNEL_TRSV 1    /* sparse unit-triangular solve (ILU factors)   */
+#define MLDG_KERNEL_SPMV 2    /* CSR SpMV family: residual, R, P             */
+#define MLDG_KERNEL_JACOBI 3  /* fused point-Jacobi sweep                    */
+#define MLDG_KERNEL_VEC 4     /* vector kernels (diag, fill, cast, axpby)   */
+
+typedef struct {
+  int kind;       /* MLDG_KERNEL_*                                            */
+  int level;      /* level the launch works on                               */
+  int64_t bytes;  /* algorithmic bytes of the launch                         */
+  double ms;      /* device time between CUDA events around the launch       */
+} mldg_kernel_stat;
+
+/* Brackets, in every later V-cycle (graph replays included), the index-th
+ * launch of kernel class `kind` on level `lev` with two CUDA events on the
+ * launching stream; kind 0 disables the probe.  Takes effect at the next
+ * graph capture (the call drops captured graphs). */
+int mldg_probe_set(mldg_handle *h, int kind, int lev, int index);
+/* Accumulated device time of the probed launch since the last read, the
+ * number of probed launches, and the algorithmic bytes of one of them. */
+int mldg_probe_read(mldg_handle *h, double *total_ms, int64_t *count, int64_t *bytes);
+
+/* Runs one V-cycle (trans 'N'/'T') on the current level-0 input without a
+ * graph, with CUDA events around every launch; writes up to max entries. */
+int mldg_profile(mldg_handle *h, char trans, int max, mldg_kernel_stat *stats, int *n);
+
 const char *mldg_last_error(const mldg_handle *h);
 
 /* replaces: prec%free (mlprec/mld_d_prec_type.f90:537-568) */

@@ -59,6 +59,52 @@ class _LevelDesc(C.Structure):
                 ("sweeps_pre", C.c_int), ("sweeps_post", C.c_int), ("damping", C.c_double)]
 
 
+class _KStat(C.Structure):
+    _fields_ = [("kind", C.c_int), ("level", C.c_int), ("bytes", C.c_int64),
+                ("ms", C.c_double)]
+
+
+KERNEL_TRSV, KERNEL_SPMV, KERNEL_JACOBI, KERNEL_VEC = 1, 2, 3, 4
+KERNEL_NAMES = {1: "trsv", 2: "spmv", 3: "jacobi", 4: "vec"}
+
+
+class _GpuDiag:
+    """Timing diagnostics shared by Hierarchy and MldPrec (needs self._gpu())."""
+
+    def probe_set(self, kind: int, lev: int, index: int = 0):
+        rc = lib().mldg_probe_set(self._gpu(), kind, lev, index)
+        if rc:
+            raise MldError(rc, "probe_set")
+
+    def probe_read(self):
+        ms = C.c_double(0)
+        cnt = C.c_int64(0)
+        b = C.c_int64(0)
+        lib().mldg_probe_read(self._gpu(), C.byref(ms), C.byref(cnt), C.byref(b))
+        return ms.value, cnt.value, b.value
+
+    def profile(self, trans: str = "N"):
+        """One un-graphed V-cycle with events around every launch."""
+        stats = (_KStat * 4096)()
+        n = C.c_int(0)
+        rc = lib().mldg_profile(self._gpu(), trans.encode(), 4096, stats, C.byref(n))
+        if rc:
+            raise MldError(rc, "profile")
+        return [{"kind": KERNEL_NAMES.get(s.kind, "?"), "kind_id": s.kind, "level": s.level,
+                 "bytes": s.bytes, "ms": s.ms} for s in stats[: min(n.value, 4096)]]
+
+    def last_timing(self):
+        ms = C.c_double(0)
+        nl = C.c_int64(0)
+        lib().mldg_last_timing(self._gpu(), C.byref(ms), C.byref(nl))
+        return ms.value, nl.value
+
+    def apply_bytes(self) -> int:
+        b = C.c_int64(0)
+        lib().mldg_apply_bytes(self._gpu(), C.byref(b))
+        return b.value
+
+
 def lib():
     """Load libmldgpu.so (built by build.py); raise if it is missing."""
     global _lib
@@ -77,6 +123,11 @@ def lib():
         L.mldg_level_info.argtypes = [vp, C.c_int, C.POINTER(C.c_int64)]
         L.mldg_last_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
         L.mldg_apply_bytes.argtypes = [vp, C.POINTER(C.c_int64)]
+        L.mldg_probe_set.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+        L.mldg_probe_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64),
+                                      C.POINTER(C.c_int64)]
+        L.mldg_profile.argtypes = [vp, C.c_char, C.c_int, C.POINTER(_KStat),
+                                   C.POINTER(C.c_int)]
         L.mldg_last_error.argtypes = [vp]
         L.mldg_last_error.restype = C.c_char_p
         L.mldg_destroy.argtypes = [vp]
@@ -137,10 +188,8 @@ class CSR:
 
     def matvec(self, x):
         x = np.asarray(x, dtype=np.float64)
-        y = np.zeros(self.nrows)
         rows = np.repeat(np.arange(self.nrows), np.diff(self.irp))
-        np.add.at(y, rows, self.val * x[self.ja])
-        return y
+        return np.bincount(rows, weights=self.val * x[self.ja], minlength=self.nrows)
 
 
 def gen_pde3d(idim: int, hden: int = 1, coef=(1.0, 1.0, 1.0, 0.0, 0.0, 0.0, 0.0)) -> CSR:
@@ -188,8 +237,11 @@ def _vec_args(x, y):
     return C.c_void_p(x.ctypes.data), C.c_void_p(y.ctypes.data), MEM_HOST
 
 
-class Hierarchy:
+class Hierarchy(_GpuDiag):
     """The drop-in boundary: upload levels, finalize, apply on the GPU."""
+
+    def _gpu(self):
+        return self._h
 
     def __init__(self, device: int = 0, use_graphs: bool = True, index_base: int = 0):
         self._h = C.c_void_p()
@@ -244,17 +296,6 @@ class Hierarchy:
             self._check(rc)
         return x, it.value, err.value
 
-    def last_timing(self):
-        ms = C.c_double(0)
-        nl = C.c_int64(0)
-        lib().mldg_last_timing(self._h, C.byref(ms), C.byref(nl))
-        return ms.value, nl.value
-
-    def apply_bytes(self) -> int:
-        b = C.c_int64(0)
-        self._check(lib().mldg_apply_bytes(self._h, C.byref(b)))
-        return b.value
-
     def level_info(self, lev: int):
         info = (C.c_int64 * 5)()
         self._check(lib().mldg_level_info(self._h, lev, info))
@@ -273,8 +314,11 @@ class Hierarchy:
             pass
 
 
-class MldPrec:
+class MldPrec(_GpuDiag):
     """Mirror of type(mld_dprec_type): init / set / build / apply / descr / free."""
+
+    def _gpu(self):
+        return lib().mldp_gpu(self._p)
 
     def __init__(self, device: int = 0):
         self._p = C.c_void_p()
@@ -371,19 +415,6 @@ class MldPrec:
         buf = C.create_string_buffer(8192)
         self._check(lib().mldp_descr(self._p, buf, 8192))
         return buf.value.decode()
-
-    def gpu_timing(self):
-        h = lib().mldp_gpu(self._p)
-        ms = C.c_double(0)
-        nl = C.c_int64(0)
-        lib().mldg_last_timing(h, C.byref(ms), C.byref(nl))
-        return ms.value, nl.value
-
-    def apply_bytes(self) -> int:
-        h = lib().mldp_gpu(self._p)
-        b = C.c_int64(0)
-        lib().mldg_apply_bytes(h, C.byref(b))
-        return b.value
 
     def free(self):
         if getattr(self, "_p", None) and self._p.value:

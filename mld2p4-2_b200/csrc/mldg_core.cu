@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -147,12 +148,19 @@ struct DCSR {
 
 template <typename T>
 struct DTri {
-  int n = 0, rev = 0, R = 0, nchunks = 0, nlevels = 0;
+  int n = 0, rev = 0, nlevels = 0;
   int64_t nnz = 0;
-  int *chunk_lvl = nullptr, *lvl_ptr = nullptr, *prow = nullptr, *pirp = nullptr, *pja = nullptr;
+  int *lvl_ptr = nullptr, *prow = nullptr, *pirp = nullptr, *pja = nullptr;
   T *pval = nullptr;
   int *counters = nullptr;
-  int tpr = 1, threads = 256, grid = 1;
+  int nblk = 0;
+  int2 *blk = nullptr;
+  int tpr = 1, e = 4;
+  int mode = 0;     // 0: staged single CTA, 1: single CTA, 2: sync-free
+  StageCfg stg{};
+  int4 *desc = nullptr;
+  bool cta = true;  // single-CTA kernel (solution in shared memory) vs sync-free
+  int threads = 512, grid = 1;
   size_t smem = 0;
   bool present() const { return prow != nullptr; }
 };
@@ -189,6 +197,58 @@ struct Engine {
   virtual void record(char trans) = 0;  // issue one V-cycle: xin (FP64) -> yout (FP64)
   int64_t launches = 0;
   int64_t bytes = 0;
+  cudaStream_t st = nullptr;
+  // ---- launch accounting, probe and profile hooks ----
+  int cur_lev = 0;
+  int probe_kind = 0, probe_lev = 0, probe_idx = 0;
+  bool probe_armed = false, pmatch = false;
+  int64_t probe_bytes = 0;
+  cudaEvent_t pev0 = nullptr, pev1 = nullptr;
+  int seen[8][64];
+  struct Prof {
+    int kind, lev;
+    int64_t bytes;
+    cudaEvent_t e0, e1;
+  };
+  std::vector<Prof> *prof = nullptr;
+  bool capturing = false;  // inside stream capture: probe events become graph nodes
+  void rec(cudaEvent_t e) {
+    if (capturing)
+      MLDG_CUDA(cudaEventRecordWithFlags(e, st, cudaEventRecordExternal));
+    else
+      MLDG_CUDA(cudaEventRecord(e, st));
+  }
+  void begin(int kind) {
+    pmatch = false;
+    const int lv_ = std::min(cur_lev, 63);
+    int &c = seen[kind][lv_];
+    if (probe_kind == kind && probe_lev == cur_lev && c == probe_idx) {
+      pmatch = true;
+      rec(pev0);
+    }
+    ++c;
+    if (prof) {
+      Prof e{kind, cur_lev, 0, nullptr, nullptr};
+      MLDG_CUDA(cudaEventCreate(&e.e0));
+      MLDG_CUDA(cudaEventCreate(&e.e1));
+      MLDG_CUDA(cudaEventRecord(e.e0, st));
+      prof->push_back(e);
+    }
+  }
+  void end(int64_t b) {
+    launches++;
+    bytes += b;
+    if (pmatch) {
+      rec(pev1);
+      probe_bytes = b;
+      probe_armed = true;
+      pmatch = false;
+    }
+    if (prof) {
+      prof->back().bytes = b;
+      MLDG_CUDA(cudaEventRecord(prof->back().e1, st));
+    }
+  }
 };
 
 struct Handle;
@@ -209,7 +269,6 @@ struct EngineT : Engine {
   };
   std::vector<Lev> lv;
   Handle *h = nullptr;
-  cudaStream_t st = nullptr;
   int *err = nullptr;
   double *xin = nullptr, *yout = nullptr;  // FP64 boundary vectors of level 0
   int nsm = 148;
@@ -219,12 +278,9 @@ struct EngineT : Engine {
     int64_t b = (threads + 255) / 256;
     return (int)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)nsm * 16));
   }
-  void count(int64_t b) {
-    launches++;
-    bytes += b;
-  }
   void spmv(const DCSR<T> &A, const T *v, T a1, const T *b, T a0, T *out, T a2) {
     const int g = blocks_for((int64_t)A.nr * A.tpr);
+    begin(MLDG_KERNEL_SPMV);
     switch (A.tpr) {
 #define CASE(K) \
   case K: k_spmv<T, K><<<g, 256, 0, st>>>(A.nr, A.irp, A.ja, A.val, v, a1, b, a0, out, a2); break;
@@ -232,12 +288,13 @@ struct EngineT : Engine {
 #undef CASE
       default: fail(MLDG_ERR_INTERNAL, "bad tpr %d", A.tpr);
     }
-    count(A.nnz * (int64_t)(sizeof(T) + 4) + 4 * ((int64_t)A.nr + 1) + (int64_t)A.nc * sizeof(T) +
-          (int64_t)A.nr * sizeof(T) * (1 + (b ? 1 : 0) + (a2 != T(0) ? 1 : 0)));
+    end(A.nnz * (int64_t)(sizeof(T) + 4) + 4 * ((int64_t)A.nr + 1) + (int64_t)A.nc * sizeof(T) +
+        (int64_t)A.nr * sizeof(T) * (1 + (b ? 1 : 0) + (a2 != T(0) ? 1 : 0)));
   }
   void jacobi(const DCSR<T> &ND, const T *d, const T *x, const T *ty, int first, T omega,
               T alpha, T beta, T *out) {
     const int g = blocks_for((int64_t)ND.nr * ND.tpr);
+    begin(MLDG_KERNEL_JACOBI);
     switch (ND.tpr) {
 #define CASE(K)                                                                           \
   case K:                                                                                 \
@@ -248,25 +305,25 @@ struct EngineT : Engine {
 #undef CASE
       default: fail(MLDG_ERR_INTERNAL, "bad tpr %d", ND.tpr);
     }
-    count(ND.nnz * (int64_t)(sizeof(T) + 4) + 4 * ((int64_t)ND.nr + 1) +
-          (int64_t)ND.nr * sizeof(T) * (3 + (first ? 0 : 1) + (beta != T(0) ? 1 : 0)));
+    end(ND.nnz * (int64_t)(sizeof(T) + 4) + 4 * ((int64_t)ND.nr + 1) +
+        (int64_t)ND.nr * sizeof(T) * (3 + (first ? 0 : 1) + (beta != T(0) ? 1 : 0)));
   }
   void diag(int n, const T *d, const T *x, T alpha, T beta, T *out) {
+    begin(MLDG_KERNEL_VEC);
     k_diag<T><<<blocks_for(n), 256, 0, st>>>(n, d, x, alpha, beta, out);
-    count((int64_t)n * sizeof(T) * (3 + (beta != T(0) ? 1 : 0)));
+    end((int64_t)n * sizeof(T) * (3 + (beta != T(0) ? 1 : 0)));
   }
   void fill(int n, T v, T *y) {
+    begin(MLDG_KERNEL_VEC);
     k_fill<T><<<blocks_for(n), 256, 0, st>>>(n, v, y);
-    count((int64_t)n * sizeof(T));
+    end((int64_t)n * sizeof(T));
   }
   void trsv(const DTri<T> &t, const T *rhs, const T *scale, T *cur, T *other, T *out, T alpha,
             T beta) {
     TriArgs<T> a;
     a.n = t.n;
     a.rev = t.rev;
-    a.R = t.R;
-    a.nchunks = t.nchunks;
-    a.chunk_lvl = t.chunk_lvl;
+    a.nlevels = t.nlevels;
     a.lvl_ptr = t.lvl_ptr;
     a.prow = t.prow;
     a.pirp = t.pirp;
@@ -281,16 +338,13 @@ struct EngineT : Engine {
     a.beta = beta;
     a.counters = t.counters;
     a.err = err;
-    switch (t.tpr) {
-#define CASE(K) \
-  case K: k_trsv<T, K><<<t.grid, t.threads, t.smem, st>>>(a); break;
-      CASE(1) CASE(2) CASE(4) CASE(8) CASE(16) CASE(32)
-#undef CASE
-      default: fail(MLDG_ERR_INTERNAL, "bad tpr %d", t.tpr);
-    }
-    count(t.nnz * (int64_t)(sizeof(T) + 4) + 4 * (2 * (int64_t)t.n + 1) +
-          (int64_t)t.n * sizeof(T) *
-              (1 + (scale ? 1 : 0) + 1 + (other ? 1 : 0) + (out ? 1 + (beta != T(0)) : 0)));
+    a.nblk = t.nblk;
+    a.blk = t.blk;
+    begin(MLDG_KERNEL_TRSV);
+    launch_trsv(t, a, st);
+    end(t.nnz * (int64_t)(sizeof(T) + 4) + 4 * (2 * (int64_t)t.n + 1) +
+        (int64_t)t.n * sizeof(T) *
+            (1 + (scale ? 1 : 0) + 1 + (other ? 1 : 0) + (out ? 1 + (beta != T(0)) : 0)));
   }
 
   // ILU solver apply: y = alpha*U^{-1}(d o L^{-1} x) + beta*y, or the 'T' form
@@ -342,6 +396,7 @@ struct EngineT : Engine {
 
   // V-cycle body (mld_d_inner_mult)
   void vcycle(int l, char trans) {
+    cur_lev = l;
     Lev &L = lv[l];
     const int nlev = (int)lv.size();
     const bool pre = (L.spre > 0 && trans == 'N') || (L.spost > 0 && trans != 'N');
@@ -358,6 +413,7 @@ struct EngineT : Engine {
         spmv(C.R, L.x, T(1), nullptr, T(0), C.x, T(0));
       }
       vcycle(l + 1, trans);
+      cur_lev = l;
       prolong(C, L.y);                                   // y += P y_{l+1}
       if (post) {
         spmv(A, L.y, T(-1), L.x, T(1), L.ty, T(0));
@@ -372,18 +428,24 @@ struct EngineT : Engine {
   void record(char trans) override {
     launches = 0;
     bytes = 0;
+    cur_lev = 0;
+    probe_armed = false;
+    std::memset(seen, 0, sizeof seen);
     Lev &F = lv[0];
     if (!std::is_same<T, double>::value) {
+      begin(MLDG_KERNEL_VEC);
       k_cast<double, T><<<blocks_for(F.n), 256, 0, st>>>(F.n, xin, F.x);
-      count((int64_t)F.n * (8 + sizeof(T)));
+      end((int64_t)F.n * (8 + sizeof(T)));
     }
     if (lv.size() == 1)
       smoother(F, trans, F.x, T(0), F.y, F.spre);
     else
       vcycle(0, trans);
     if (!std::is_same<T, double>::value) {
+      cur_lev = 0;
+      begin(MLDG_KERNEL_VEC);
       k_cast<T, double><<<blocks_for(F.n), 256, 0, st>>>(F.n, F.y, yout);
-      count((int64_t)F.n * (8 + sizeof(T)));
+      end((int64_t)F.n * (8 + sizeof(T)));
     }
   }
 };
@@ -396,8 +458,9 @@ __global__ void k_axpby1(int n, const T *__restrict__ x, T beta, T *y) {
 
 template <typename T>
 void EngineT<T>::k_axpby_impl(int n, const T *x, T beta, T *y) {
+  begin(MLDG_KERNEL_VEC);
   k_axpby1<T><<<blocks_for(n), 256, 0, st>>>(n, x, beta, y);
-  count((int64_t)n * sizeof(T) * (2 + (beta != T(0))));
+  end((int64_t)n * sizeof(T) * (2 + (beta != T(0))));
 }
 
 template <typename T>
@@ -412,6 +475,7 @@ void EngineT<float>::prolong(Lev &C, float *y) {
     return;
   }
   const int g = blocks_for((int64_t)C.P.nr * C.P.tpr);
+  begin(MLDG_KERNEL_SPMV);
   switch (C.P.tpr) {
 #define CASE(K) \
   case K: k_spmv_h<K><<<g, 256, 0, st>>>(C.P.nr, C.P.irp, C.P.ja, C.Ph, C.Pscale, C.y, y); break;
@@ -419,7 +483,7 @@ void EngineT<float>::prolong(Lev &C, float *y) {
 #undef CASE
     default: fail(MLDG_ERR_INTERNAL, "bad tpr");
   }
-  count(C.P.nnz * 6 + 4 * ((int64_t)C.P.nr + 1) + (int64_t)C.P.nc * 4 + (int64_t)C.P.nr * 4 * 3);
+  end(C.P.nnz * 6 + 4 * ((int64_t)C.P.nr + 1) + (int64_t)C.P.nc * 4 + (int64_t)C.P.nr * 4 * 3);
 }
 
 // ---------------------------------------------------------------------------
@@ -448,24 +512,67 @@ struct Handle {
   double last_ms = 0;
   int64_t last_launches = 0;
   int nsm = 148;
+  // probe (see mldg_probe_set)
+  int probe_kind = 0, probe_lev = 0, probe_idx = 0;
+  cudaEvent_t pev0 = nullptr, pev1 = nullptr;
+  bool gprobe[2] = {false, false};
+  bool pending = false;  // a probed launch was issued and not yet read
+  double probe_ms = 0;
+  int64_t probe_count = 0, probe_bytes = 0;
 };
 
+// dispatch over (kernel, lanes per row, prefetched entries per lane)
+template <typename T, int TPR, int E>
+static void launch_trsv_te(const DTri<T> &t, const TriArgs<T> &a, cudaStream_t st) {
+  if (t.cta)
+    k_trsv_cta<T, TPR, E><<<1, t.threads, t.smem, st>>>(a);
+  else
+    k_trsv_sf<T, TPR, E><<<t.grid, t.threads, 0, st>>>(a);
+}
+template <typename T, int TPR>
+static void launch_trsv_t(const DTri<T> &t, const TriArgs<T> &a, cudaStream_t st) {
+  if (t.mode == 0) {
+    if (t.stg.D == 3)
+      k_trsv_stg<T, TPR, 3><<<1, t.threads, t.smem, st>>>(a, t.stg, t.desc);
+    else
+      k_trsv_stg<T, TPR, 4><<<1, t.threads, t.smem, st>>>(a, t.stg, t.desc);
+    return;
+  }
+  if (t.e <= 4)
+    launch_trsv_te<T, TPR, 4>(t, a, st);
+  else
+    launch_trsv_te<T, TPR, 8>(t, a, st);
+}
 template <typename T>
-static DTri<T> build_tri_dev(Arena &ar, const HostCSR &m, bool upper, int R_hint, int nsm) {
+static void launch_trsv(const DTri<T> &t, const TriArgs<T> &a, cudaStream_t st) {
+  switch (t.tpr) {
+    case 1: launch_trsv_t<T, 1>(t, a, st); break;
+    case 2: launch_trsv_t<T, 2>(t, a, st); break;
+    case 4: launch_trsv_t<T, 4>(t, a, st); break;
+    case 8: launch_trsv_t<T, 8>(t, a, st); break;
+    case 16: launch_trsv_t<T, 16>(t, a, st); break;
+    default: launch_trsv_t<T, 32>(t, a, st); break;
+  }
+}
+
+// Levels with at most this many rows use the single-CTA kernel (the whole
+// solution vector in shared memory: 128 KB).
+template <typename T>
+constexpr int tri_cta_rows() {
+  return (int)(128 * 1024 / sizeof(T));
+}
+
+template <typename T>
+static DTri<T> build_tri_dev(Arena &ar, const HostCSR &m, bool upper, int nsm) {
   DTri<T> t;
   if (!m.present()) return t;
   TriSchedule s;
   const int n = m.nr;
-  int R = R_hint;
-  if (R <= 0) R = (n <= kTriSingleChunkRows) ? std::max(n, 1) : kTriChunkRows;
-  build_tri_schedule(n, m.irp.data(), m.ja.data(), m.val.data(), upper, R, &s);
+  build_tri_schedule(n, m.irp.data(), m.ja.data(), m.val.data(), upper, std::max(n, 1), &s);
   t.n = n;
   t.rev = upper ? 1 : 0;
-  t.R = R;
-  t.nchunks = s.nchunks;
   t.nlevels = (int)s.lvl_ptr.size() - 1;
   t.nnz = m.nnz();
-  t.chunk_lvl = ar.upload(s.chunk_lvl);
   t.lvl_ptr = ar.upload(s.lvl_ptr);
   t.prow = ar.upload(s.prow);
   t.pirp = ar.upload(s.pirp);
@@ -474,25 +581,89 @@ static DTri<T> build_tri_dev(Arena &ar, const HostCSR &m, bool upper, int R_hint
   t.pval = ar.upload(v);
   t.counters = ar.alloc<int>(2);
   MLDG_CUDA(cudaMemset(t.counters, 0, 2 * sizeof(int)));
-  t.tpr = pick_tpr(t.nnz, std::max(n, 1));
-  if (t.tpr > 8) t.tpr = 8;
-  t.threads = 256;
-  t.smem = (size_t)R * sizeof(T);
-  t.grid = std::max(1, std::min(t.nchunks, nsm * 2));
+  // lanes per row: smallest power of two with <= 8 entries per lane
+  const double avg = n > 0 ? (double)t.nnz / n : 0.0;
+  t.tpr = 1;
+  while (t.tpr < 32 && avg / t.tpr > 8.0) t.tpr *= 2;
+  t.e = (avg / t.tpr <= 4.0) ? 4 : 8;
+  t.cta = n <= tri_cta_rows<T>();
+  // staged single-CTA plan: solution + level descriptors + D ring stages
+  {
+    int maxr = 0, maxe = 0;
+    std::vector<int4> desc((size_t)t.nlevels);
+    for (int L = 0; L < t.nlevels; ++L) {
+      const int p0 = s.lvl_ptr[L], p1 = s.lvl_ptr[L + 1];
+      desc[L] = make_int4(p0, p1, s.pirp[p0], s.pirp[p1]);
+      maxr = std::max(maxr, p1 - p0);
+      maxe = std::max(maxe, s.pirp[p1] - s.pirp[p0]);
+    }
+    StageCfg c{};
+    c.capR = maxr;
+    c.capE = std::max(maxe, 1);
+    c.bytes = (int)(((((size_t)(2 * c.capR + 1 + c.capE) * 4 + 15) & ~(size_t)15) +
+                     (size_t)c.capE * sizeof(T) + 15) & ~(size_t)15);
+    c.off_y = 0;
+    c.off_desc = (int)(((size_t)std::max(n, 1) * sizeof(T) + 15) & ~(size_t)15);
+    c.off_ring = c.off_desc + (int)(((size_t)t.nlevels * 16 + 15) & ~(size_t)15);
+    const size_t budget = 220 * 1024;
+    for (int D = 4; D >= 3; --D) {
+      c.D = D;
+      if ((size_t)c.off_ring + (size_t)D * c.bytes <= budget) break;
+      c.D = 0;
+    }
+    if (c.D >= 3) {
+      t.mode = 0;
+      t.stg = c;
+      t.desc = ar.upload(desc);
+      t.threads = 512;
+      t.grid = 1;
+      t.smem = (size_t)c.off_ring + (size_t)c.D * c.bytes;
+      return t;
+    }
+  }
+  if (t.cta) {
+    t.mode = 1;
+    t.threads = 512;
+    t.grid = 1;
+    t.smem = (size_t)std::max(n, 1) * sizeof(T);
+  } else {
+    t.mode = 2;
+    const int rpw = 32 / t.tpr;
+    std::vector<int2> blk;
+    blk.reserve((size_t)n / rpw + (size_t)t.nlevels + 1);
+    for (int L = 0; L < t.nlevels; ++L)
+      for (int p = s.lvl_ptr[L]; p < s.lvl_ptr[L + 1]; p += rpw)
+        blk.push_back(make_int2(p, std::min(p + rpw, s.lvl_ptr[L + 1])));
+    t.nblk = (int)blk.size();
+    t.blk = ar.upload(blk);
+    // Warps in flight: a few dependency levels' worth of blocks.  More only
+    // adds spinning lanes whose polls compete with real traffic in L2.
+    const int per_level = (t.nblk + t.nlevels - 1) / std::max(t.nlevels, 1);
+    const int warps = std::max(32, std::min(4 * per_level, nsm * 32));
+    t.threads = 256;
+    t.grid = (warps + 7) / 8;
+  }
   return t;
 }
 
+template <typename T, int TPR>
+static void set_attr_t() {
+  const int mx = 224 * 1024;
+  MLDG_CUDA(cudaFuncSetAttribute(k_trsv_stg<T, TPR, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  MLDG_CUDA(cudaFuncSetAttribute(k_trsv_stg<T, TPR, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  MLDG_CUDA(cudaFuncSetAttribute(k_trsv_cta<T, TPR, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  MLDG_CUDA(cudaFuncSetAttribute(k_trsv_cta<T, TPR, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+}
 template <typename T>
 static void set_trsv_smem_attr() {
   static bool done = false;
   if (done) return;
-  const int mx = 200 * 1024;
-  MLDG_CUDA(cudaFuncSetAttribute(k_trsv<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  MLDG_CUDA(cudaFuncSetAttribute(k_trsv<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  MLDG_CUDA(cudaFuncSetAttribute(k_trsv<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  MLDG_CUDA(cudaFuncSetAttribute(k_trsv<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  MLDG_CUDA(cudaFuncSetAttribute(k_trsv<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  MLDG_CUDA(cudaFuncSetAttribute(k_trsv<T, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  set_attr_t<T, 1>();
+  set_attr_t<T, 2>();
+  set_attr_t<T, 4>();
+  set_attr_t<T, 8>();
+  set_attr_t<T, 16>();
+  set_attr_t<T, 32>();
   done = true;
 }
 
@@ -502,6 +673,11 @@ static Engine *make_engine(Handle *h) {
   auto *e = new EngineT<T>();
   e->h = h;
   e->st = h->st;
+  e->pev0 = h->pev0;
+  e->pev1 = h->pev1;
+  e->probe_kind = h->probe_kind;
+  e->probe_lev = h->probe_lev;
+  e->probe_idx = h->probe_idx;
   e->err = h->err;
   e->xin = h->xin;
   e->yout = h->yout;
@@ -538,14 +714,25 @@ static Engine *make_engine(Handle *h) {
     }
     L.nnz_nd = H.ND.nnz();
     if (H.kind == MLDG_SMOOTHER_BJAC) {
-      L.L = build_tri_dev<T>(ar, H.L, false, 0, h->nsm);
-      L.U = build_tri_dev<T>(ar, H.U, true, 0, h->nsm);
+      L.L = build_tri_dev<T>(ar, H.L, false, h->nsm);
+      L.U = build_tri_dev<T>(ar, H.U, true, h->nsm);
       HostCSR Lt = transpose(H.L), Ut = transpose(H.U);
-      L.Ut = build_tri_dev<T>(ar, Ut, false, 0, h->nsm);  // U^T is lower
-      L.Lt = build_tri_dev<T>(ar, Lt, true, 0, h->nsm);   // L^T is upper
+      L.Ut = build_tri_dev<T>(ar, Ut, false, h->nsm);  // U^T is lower
+      L.Lt = build_tri_dev<T>(ar, Lt, true, h->nsm);   // L^T is upper
       if (L.nnz_nd > 0) {
         L.ND = to_dev<T>(ar, H.ND);
         L.NDT = to_dev<T>(ar, transpose(H.ND));
+      }
+      if (std::getenv("MLDG_VERBOSE")) {
+        const DTri<T> *ts[4] = {&L.L, &L.U, &L.Ut, &L.Lt};
+        const char *nm[4] = {"L", "U", "Ut", "Lt"};
+        for (int q = 0; q < 4; ++q)
+          std::fprintf(stderr,
+                       "mldg: level %d %-2s n=%d nnz=%lld levels=%d mode=%d tpr=%d e=%d D=%d "
+                       "capR=%d capE=%d smem=%zu grid=%d\n",
+                       l, nm[q], ts[q]->n, (long long)ts[q]->nnz, ts[q]->nlevels, ts[q]->mode,
+                       ts[q]->tpr, ts[q]->e, ts[q]->stg.D, ts[q]->stg.capR, ts[q]->stg.capE,
+                       ts[q]->smem, ts[q]->grid);
       }
     } else {
       if (H.ND.present()) {
@@ -651,26 +838,44 @@ static void run_vcycle(Handle *h, char trans) {
     if (!h->gexec[t]) {
       cudaGraph_t g;
       MLDG_CUDA(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+      h->eng->capturing = true;
       try {
         h->eng->record(trans);
       } catch (...) {
+        h->eng->capturing = false;
         cudaStreamEndCapture(h->st, &g);
         throw;
       }
+      h->eng->capturing = false;
       MLDG_CUDA(cudaStreamEndCapture(h->st, &g));
       MLDG_CUDA(cudaGraphInstantiate(&h->gexec[t], g, 0));
       cudaGraphDestroy(g);
       h->glaunch[t] = h->eng->launches;
       h->gbytes[t] = h->eng->bytes;
+      h->gprobe[t] = h->eng->probe_armed;
+      if (h->eng->probe_armed) h->probe_bytes = h->eng->probe_bytes;
     }
     MLDG_CUDA(cudaGraphLaunch(h->gexec[t], h->st));
     h->last_launches += h->glaunch[t];
+    h->pending = h->gprobe[t];
   } else {
     h->eng->record(trans);
     h->glaunch[t] = h->eng->launches;
     h->gbytes[t] = h->eng->bytes;
     h->last_launches += h->eng->launches;
+    h->pending = h->eng->probe_armed;
+    if (h->eng->probe_armed) h->probe_bytes = h->eng->probe_bytes;
   }
+}
+
+// after a stream synchronisation: account the probed launch, if any
+static void probe_collect(Handle *h) {
+  if (!h->pending) return;
+  float ms = 0;
+  MLDG_CUDA(cudaEventElapsedTime(&ms, h->pev0, h->pev1));
+  h->probe_ms += ms;
+  h->probe_count += 1;
+  h->pending = false;
 }
 
 static int check_device_error(Handle *h) {
@@ -701,6 +906,10 @@ static void apply(Handle *h, const double *x, double *y, char trans, int nrhs, i
     MLDG_CUDA(cudaMemcpyAsync(h->xin, x + off, sizeof(double) * n, h2d, h->st));
     run_vcycle(h, trans);
     MLDG_CUDA(cudaMemcpyAsync(y + off, h->yout, sizeof(double) * n, d2h, h->st));
+    if (h->pending) {
+      MLDG_CUDA(cudaStreamSynchronize(h->st));
+      probe_collect(h);
+    }
   }
   MLDG_CUDA(cudaEventRecord(h->ev1, h->st));
   MLDG_CUDA(cudaStreamSynchronize(h->st));
@@ -787,6 +996,7 @@ static void krylov(Handle *h, int method, const mldg_csr *Acsr, const double *b,
     h->last_launches += 6;
     MLDG_CUDA(cudaMemcpyAsync(h->hpin, sc->dots, sizeof(double), cudaMemcpyDeviceToHost, h->st));
     MLDG_CUDA(cudaStreamSynchronize(h->st));
+    probe_collect(h);
     err = std::sqrt(std::max(h->hpin[0], 0.0)) / bn2;
     if (std::isnan(err)) break;
   }
@@ -846,6 +1056,8 @@ extern "C" int mldg_create(mldg_handle **out, const mldg_opts *opts) {
     MLDG_CUDA(cudaStreamCreateWithFlags(&h.st, cudaStreamNonBlocking));
     MLDG_CUDA(cudaEventCreate(&h.ev0));
     MLDG_CUDA(cudaEventCreate(&h.ev1));
+    MLDG_CUDA(cudaEventCreate(&h.pev0));
+    MLDG_CUDA(cudaEventCreate(&h.pev1));
     MLDG_CUDA(cudaMallocHost(&h.hpin, 4 * sizeof(double)));
     MLDG_CUDA(cudaDeviceGetAttribute(&h.nsm, cudaDevAttrMultiProcessorCount, h.opts.device));
   } catch (const Error &e) {
@@ -937,6 +1149,82 @@ extern "C" int mldg_apply_bytes(const mldg_handle *hp, int64_t *bytes) {
   return MLDG_SUCCESS;
 }
 
+extern "C" int mldg_probe_set(mldg_handle *hp, int kind, int lev, int index) {
+  if (!hp) return MLDG_ERR_ARG;
+  MLDG_GUARD(hp, {
+    Handle &h = hp->h;
+    if (kind < 0 || kind > MLDG_KERNEL_VEC || lev < 0 || index < 0)
+      mldg::fail(MLDG_ERR_ARG, "bad probe (%d, %d, %d)", kind, lev, index);
+    h.probe_kind = kind;
+    h.probe_lev = lev;
+    h.probe_idx = index;
+    for (int t = 0; t < 2; ++t)
+      if (h.gexec[t]) {
+        cudaGraphExecDestroy(h.gexec[t]);
+        h.gexec[t] = nullptr;
+      }
+    if (h.eng) {
+      h.eng->probe_kind = kind;
+      h.eng->probe_lev = lev;
+      h.eng->probe_idx = index;
+    }
+    h.probe_ms = 0;
+    h.probe_count = 0;
+    h.pending = false;
+  });
+}
+
+extern "C" int mldg_probe_read(mldg_handle *hp, double *total_ms, int64_t *count, int64_t *bytes) {
+  if (!hp) return MLDG_ERR_ARG;
+  Handle &h = hp->h;
+  if (total_ms) *total_ms = h.probe_ms;
+  if (count) *count = h.probe_count;
+  if (bytes) *bytes = h.probe_bytes;
+  h.probe_ms = 0;
+  h.probe_count = 0;
+  return MLDG_SUCCESS;
+}
+
+extern "C" int mldg_profile(mldg_handle *hp, char trans, int max, mldg_kernel_stat *stats, int *n) {
+  if (!hp) return MLDG_ERR_ARG;
+  MLDG_GUARD(hp, {
+    Handle &h = hp->h;
+    if (!h.finalized) mldg::fail(MLDG_ERR_NOT_BUILT, "profile before build");
+    if (trans == 'C') trans = 'T';
+    if (trans != 'N' && trans != 'T') mldg::fail(MLDG_ERR_TRANS, "invalid trans");
+    std::vector<mldg::Engine::Prof> prof;
+    h.eng->prof = &prof;
+    const int pk = h.eng->probe_kind;
+    h.eng->probe_kind = 0;
+    try {
+      h.eng->record(trans);
+    } catch (...) {
+      h.eng->prof = nullptr;
+      h.eng->probe_kind = pk;
+      throw;
+    }
+    h.eng->prof = nullptr;
+    h.eng->probe_kind = pk;
+    MLDG_CUDA(cudaStreamSynchronize(h.st));
+    int k = 0;
+    for (auto &e : prof) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e.e0, e.e1);
+      if (k < max && stats) {
+        stats[k].kind = e.kind;
+        stats[k].level = e.lev;
+        stats[k].bytes = e.bytes;
+        stats[k].ms = ms;
+      }
+      ++k;
+      cudaEventDestroy(e.e0);
+      cudaEventDestroy(e.e1);
+    }
+    if (n) *n = k;
+    mldg::check_device_error(&h);
+  });
+}
+
 extern "C" const char *mldg_last_error(const mldg_handle *hp) {
   if (!hp) return "null handle";
   return hp->h.last_error.c_str();
@@ -954,6 +1242,8 @@ extern "C" void mldg_destroy(mldg_handle *hp) {
   if (h.hpin) cudaFreeHost(h.hpin);
   if (h.ev0) cudaEventDestroy(h.ev0);
   if (h.ev1) cudaEventDestroy(h.ev1);
+  if (h.pev0) cudaEventDestroy(h.pev0);
+  if (h.pev1) cudaEventDestroy(h.pev1);
   if (h.st) cudaStreamDestroy(h.st);
   delete hp;
 }

@@ -236,20 +236,25 @@ __global__ void k_fill(int n, T v, T *__restrict__ y) {
 }
 
 // ---------------------------------------------------------------------------
-// Sparse unit-triangular solve, chunked and level-scheduled.
+// Sparse unit-triangular solve, level-scheduled.
 //
 // The factor is stored "lower in internal numbering": for an upper factor the
 // rows are reversed (internal i' = n-1-i), so every dependency j' < i'.  Rows
-// are cut into chunks of R consecutive internal rows; inside a chunk they are
-// permuted by dependency level (intra-chunk edges only) and stored in that
-// order (prow/pirp/pja/pval).  A CTA takes chunks in increasing order from a
-// ticket counter; it walks the chunk level by level with the chunk's partial
-// solution in shared memory and one __syncthreads per level.  Dependencies on
-// earlier chunks are read from the exchange buffer `cur`, whose entries hold
-// the sentinel until produced (no flags, no fences: the value is the flag).
-// Chunks only wait on earlier chunks, which were claimed earlier by CTAs that
-// are running or finished, so the scheme cannot deadlock; every wait is
-// bounded (wait_value).
+// are sorted by dependency level (the longest chain of dependencies leading
+// to them) and stored in that order (prow/pirp/pja/pval), so all rows of a
+// level are independent and every dependency of a row sits at a smaller
+// position.  Two kernels walk that order:
+//   k_trsv_cta : one CTA, the whole solution in shared memory, one
+//                __syncthreads per level, the next level's entries loaded
+//                into registers while the current level is computed
+//                (small levels).
+//   k_trsv_sf  : all SMs, no barriers; warps claim consecutive blocks of
+//                positions from a ticket counter, load their rows' entries,
+//                then wait for each dependency on the exchange buffer `cur`,
+//                whose entries hold a sentinel until produced (the value is
+//                the flag).  Blocks are claimed in position order and every
+//                dependency lies at an earlier position, so the waits always
+//                end; each wait is bounded anyway (wait_value).
 //
 // rhs_i = rhs_src[o] * (rhs_scale ? rhs_scale[o] : 1), o = original row.
 // After the solve row o holds t_o in cur[o]; `other[o]` is reset to the
@@ -262,10 +267,8 @@ template <typename T>
 struct TriArgs {
   int n;
   int rev;
-  int R;
-  int nchunks;
-  const int *chunk_lvl;
-  const int *lvl_ptr;
+  int nlevels;
+  const int *lvl_ptr;  // nlevels + 1 positions
   const int *prow;
   const int *pirp;
   const int *pja;
@@ -277,75 +280,304 @@ struct TriArgs {
   T *out;
   T alpha;
   T beta;
-  int *counters;  // [0] = chunk ticket, [1] = finished CTAs (self-resetting)
+  int *counters;  // [0] = block ticket, [1] = finished warps (self-resetting)
   int *err;
+  // k_trsv_sf: warp blocks never straddle a level, so the rows of a block
+  // are independent of one another (no lane waits on its own warp)
+  int nblk;
+  const int2 *blk;  // [first position, end position) per block
 };
 
-template <typename T, int TPR>
-__global__ void __launch_bounds__(256) k_trsv(TriArgs<T> a) {
+template <typename T>
+__device__ __forceinline__ void tri_store(const TriArgs<T> &a, int o, T t) {
+  Bits<T>::store(a.cur + o, t);
+  if (a.other) a.other[o] = Sentinel<T>::value();
+  if (a.out) {
+    T w = a.alpha * t;
+    if (a.beta != T(0)) w = fma(a.beta, a.out[o], w);
+    a.out[o] = w;
+  }
+}
+
+// One row's prefetched state: up to E entries per lane held in registers.
+template <typename T, int E>
+struct RowRegs {
+  int i, o, k0, k1;  // internal row, original row, entry range of this lane
+  T rhs;
+  int j[E];
+  T v[E];
+};
+
+template <typename T, int TPR, int E>
+__device__ __forceinline__ void load_row(const TriArgs<T> &a, int p, int sub, RowRegs<T, E> &r) {
+  r.i = a.prow[p];
+  r.o = a.rev ? (a.n - 1 - r.i) : r.i;
+  r.k0 = a.pirp[p] + sub;
+  r.k1 = a.pirp[p + 1];
+  r.rhs = a.rhs_src[r.o];
+  if (a.rhs_scale) r.rhs = r.rhs * a.rhs_scale[r.o];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int k = r.k0 + e * TPR;
+    if (k < r.k1) {
+      r.j[e] = a.pja[k];
+      r.v[e] = a.pval[k];
+    } else {
+      r.j[e] = 0;
+      r.v[e] = T(0);
+    }
+  }
+}
+
+template <typename T, int TPR, int E>
+__global__ void __launch_bounds__(512) k_trsv_cta(TriArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *ysm = reinterpret_cast<T *>(smem_raw);
-  __shared__ int s_chunk;
+  constexpr int RPW = 32 / TPR;
+  const int lane = threadIdx.x & 31;
+  const int sub = lane % TPR;
+  const int slot = (threadIdx.x >> 5) * RPW + lane / TPR;  // row slot within a pass
+  const int nslots = (blockDim.x >> 5) * RPW;
+  RowRegs<T, E> cur, nxt;
+  bool have = false, have_n = false;
+  if (a.nlevels > 0) {
+    const int p = a.lvl_ptr[0] + slot;
+    have = p < a.lvl_ptr[1];
+    if (have) load_row<T, TPR, E>(a, p, sub, cur);
+  }
+  for (int L = 0; L < a.nlevels; ++L) {
+    const int p0 = a.lvl_ptr[L], p1 = a.lvl_ptr[L + 1];
+    // prefetch the first pass of the next level
+    if (L + 1 < a.nlevels) {
+      const int pn = p1 + slot;
+      have_n = pn < a.lvl_ptr[L + 2];
+      if (have_n) load_row<T, TPR, E>(a, pn, sub, nxt);
+    } else {
+      have_n = false;
+    }
+    // first pass from registers
+    {
+      T acc = T(0);
+      if (have) {
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+          if (cur.k0 + e * TPR < cur.k1) acc = fma(cur.v[e], ysm[cur.j[e]], acc);
+        for (int k = cur.k0 + E * TPR; k < cur.k1; k += TPR) acc = fma(a.pval[k], ysm[a.pja[k]], acc);
+      }
+#pragma unroll
+      for (int o = TPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, TPR);
+      if (have && sub == 0) {
+        const T t = Bits<T>::canon(cur.rhs - acc);
+        ysm[cur.i] = t;
+        tri_store(a, cur.o, t);
+      }
+    }
+    // further passes of a wide level (not prefetched)
+    for (int q0 = p0 + nslots; q0 < p1; q0 += nslots) {
+      const int p = q0 + slot;
+      T acc = T(0);
+      RowRegs<T, 1> r;
+      const bool ok = p < p1;
+      if (ok) {
+        load_row<T, TPR, 1>(a, p, sub, r);
+        for (int k = r.k0; k < r.k1; k += TPR) acc = fma(a.pval[k], ysm[a.pja[k]], acc);
+      }
+#pragma unroll
+      for (int o = TPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, TPR);
+      if (ok && sub == 0) {
+        const T t = Bits<T>::canon(r.rhs - acc);
+        ysm[r.i] = t;
+        tri_store(a, r.o, t);
+      }
+    }
+    __syncthreads();
+    cur = nxt;
+    have = have_n;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Staged single-CTA solve (small levels).  The right-hand side is loaded once
+// into the shared solution vector, which is then updated in place level by
+// level; each level's rows and entries stream through a ring of D shared
+// stages filled by cp.async D-1 levels ahead, so the only per-level costs
+// are one barrier and the row arithmetic.  Results are written out
+// (coalesced) at the end.
+struct StageCfg {
+  int D;       // ring depth
+  int capR;    // rows per stage
+  int capE;    // entries per stage
+  int bytes;   // bytes per stage
+  int off_y, off_desc, off_ring;  // byte offsets in dynamic shared memory
+};
+
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <typename T>
+__device__ __forceinline__ void stage_issue(const TriArgs<T> &a, const StageCfg &c, unsigned char *ring,
+                                            const int4 *desc, int l) {
+  if (l >= a.nlevels) return;
+  unsigned char *st = ring + (size_t)(l % c.D) * c.bytes;
+  int *prow_s = reinterpret_cast<int *>(st);
+  int *pirp_s = prow_s + c.capR;
+  int *pja_s = pirp_s + c.capR + 1;
+  T *pval_s = reinterpret_cast<T *>(st + (((size_t)(2 * c.capR + 1 + c.capE) * 4 + 15) & ~(size_t)15));
+  const int4 d = desc[l];  // p0, p1, e0, e1
+  const int nr = d.y - d.x, ne = d.w - d.z;
+  for (int r = threadIdx.x; r < nr; r += blockDim.x) cp_async4(prow_s + r, a.prow + d.x + r);
+  for (int r = threadIdx.x; r <= nr; r += blockDim.x) cp_async4(pirp_s + r, a.pirp + d.x + r);
+  for (int k = threadIdx.x; k < ne; k += blockDim.x) {
+    cp_async4(pja_s + k, a.pja + d.z + k);
+    if (sizeof(T) == 8)
+      cp_async8(pval_s + k, a.pval + d.z + k);
+    else
+      cp_async4(pval_s + k, a.pval + d.z + k);
+  }
+}
+
+template <typename T, int TPR, int D>
+__global__ void __launch_bounds__(512) k_trsv_stg(TriArgs<T> a, StageCfg c, const int4 *gdesc) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *ysm = reinterpret_cast<T *>(smem_raw + c.off_y);
+  int4 *desc = reinterpret_cast<int4 *>(smem_raw + c.off_desc);
+  unsigned char *ring = smem_raw + c.off_ring;
+  constexpr int RPW = 32 / TPR;
+  const int lane = threadIdx.x & 31;
+  const int sub = lane % TPR;
+  const int slot = (threadIdx.x >> 5) * RPW + lane / TPR;
+  const int nslots = (blockDim.x >> 5) * RPW;
+  const T sent = Sentinel<T>::value();
+  for (int l = threadIdx.x; l < a.nlevels; l += blockDim.x) desc[l] = gdesc[l];
+  for (int i = threadIdx.x; i < a.n; i += blockDim.x) {
+    const int o = a.rev ? (a.n - 1 - i) : i;
+    T r = a.rhs_src[o];
+    if (a.rhs_scale) r = r * a.rhs_scale[o];
+    ysm[i] = r;
+    if (a.other) a.other[o] = sent;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int l = 0; l < D - 1; ++l) {
+    stage_issue(a, c, ring, desc, l);
+    cp_async_commit();
+  }
+  for (int L = 0; L < a.nlevels; ++L) {
+    cp_async_wait<D - 2>();
+    __syncthreads();  // level L staged; level L-1 finished (its stage is free)
+    stage_issue(a, c, ring, desc, L + D - 1);
+    cp_async_commit();
+    const unsigned char *st = ring + (size_t)(L % D) * c.bytes;
+    const int *prow_s = reinterpret_cast<const int *>(st);
+    const int *pirp_s = prow_s + c.capR;
+    const int *pja_s = pirp_s + c.capR + 1;
+    const T *pval_s =
+        reinterpret_cast<const T *>(st + (((size_t)(2 * c.capR + 1 + c.capE) * 4 + 15) & ~(size_t)15));
+    const int4 d = desc[L];
+    const int nr = d.y - d.x;
+    for (int r0 = 0; r0 < nr; r0 += nslots) {
+      const int r = r0 + slot;
+      T acc = T(0);
+      int i = 0;
+      if (r < nr) {
+        i = prow_s[r];
+        const int kb = pirp_s[r] - d.z, ke = pirp_s[r + 1] - d.z;
+        for (int k = kb + sub; k < ke; k += TPR) acc = fma(pval_s[k], ysm[pja_s[k]], acc);
+      }
+#pragma unroll
+      for (int o = TPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, TPR);
+      if (r < nr && sub == 0) ysm[i] = Bits<T>::canon(ysm[i] - acc);
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  for (int i = threadIdx.x; i < a.n; i += blockDim.x) {
+    const int o = a.rev ? (a.n - 1 - i) : i;
+    const T t = ysm[i];
+    a.cur[o] = t;
+    if (a.out) {
+      T w = a.alpha * t;
+      if (a.beta != T(0)) w = fma(a.beta, a.out[o], w);
+      a.out[o] = w;
+    }
+  }
+}
+
+template <typename T, int TPR, int E>
+__global__ void __launch_bounds__(256) k_trsv_sf(TriArgs<T> a) {
   constexpr int RPW = 32 / TPR;
   const int lane = threadIdx.x & 31;
   const int sub = lane % TPR;
   const int grp = lane / TPR;
-  const int warp = threadIdx.x >> 5;
-  const int nwarps = blockDim.x >> 5;
-  const T sent = Sentinel<T>::value();
   for (;;) {
-    if (threadIdx.x == 0) s_chunk = atomicAdd(&a.counters[0], 1);
-    __syncthreads();
-    const int c = s_chunk;
-    __syncthreads();
-    if (c >= a.nchunks) break;
-    const int s = c * a.R;
-    const int l0 = a.chunk_lvl[c], l1 = a.chunk_lvl[c + 1];
-    for (int L = l0; L < l1; ++L) {
-      const int p0 = a.lvl_ptr[L], p1 = a.lvl_ptr[L + 1];
-      for (int q0 = p0 + warp * RPW; q0 < p1; q0 += nwarps * RPW) {
-        const int p = q0 + grp;
-        T acc = T(0);
-        int i = 0;
-        if (p < p1) {
-          i = a.prow[p];
-          const int e = a.pirp[p + 1];
-          for (int k = a.pirp[p] + sub; k < e; k += TPR) {
-            const int j = a.pja[k];
-            T yj;
-            if (j >= s) {
-              yj = ysm[j - s];
-            } else {
-              const int oj = a.rev ? (a.n - 1 - j) : j;
-              yj = wait_value<T>(a.cur + oj, a.err);
-            }
-            acc = fma(a.pval[k], yj, acc);
-          }
+    int b = 0;
+    if (lane == 0) b = atomicAdd(&a.counters[0], 1);
+    b = __shfl_sync(0xffffffffu, b, 0);
+    if (b >= a.nblk) break;
+    const int2 be = a.blk[b];
+    const int p = be.x + grp;
+    const bool ok = p < be.y;
+    RowRegs<T, E> r;
+    T acc = T(0);
+    if (ok) {
+      load_row<T, TPR, E>(a, p, sub, r);
+      // all dependency loads in flight at once; re-poll only the missing ones
+      typedef typename Bits<T>::U U;
+      const U sent = (U)Sentinel<T>::bits;
+      U raw[E];
+      const T *src[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const bool has = r.k0 + e * TPR < r.k1;
+        src[e] = a.cur + (a.rev ? (a.n - 1 - r.j[e]) : r.j[e]);
+        raw[e] = has ? Bits<T>::load(src[e]) : (U)0;
+      }
+      for (int it = 0;; ++it) {
+        bool missing = false;
+#pragma unroll
+        for (int e = 0; e < E; ++e) missing |= (raw[e] == sent);
+        if (!missing) break;
+        if (it >= kSpinLimit) {
+          atomicExch(a.err, kErrTimeout);
+          break;
+        }
+        if ((it % kSpinCheck) == kSpinCheck - 1) {
+          if (ld_relaxed_u32(a.err) != 0u) break;
+          __nanosleep(32);
         }
 #pragma unroll
-        for (int o = TPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, TPR);
-        if (p < p1 && sub == 0) {
-          const int o = a.rev ? (a.n - 1 - i) : i;
-          T r = a.rhs_src[o];
-          if (a.rhs_scale) r = r * a.rhs_scale[o];
-          const T t = Bits<T>::canon(r - acc);
-          ysm[i - s] = t;
-          Bits<T>::store(a.cur + o, t);
-          if (a.other) a.other[o] = sent;
-          if (a.out) {
-            T w = a.alpha * t;
-            if (a.beta != T(0)) w = fma(a.beta, a.out[o], w);
-            a.out[o] = w;
-          }
-        }
+        for (int e = 0; e < E; ++e)
+          if (raw[e] == sent) raw[e] = Bits<T>::load(src[e]);
       }
-      __syncthreads();
+#pragma unroll
+      for (int e = 0; e < E; ++e)
+        if (r.k0 + e * TPR < r.k1) acc = fma(r.v[e], Bits<T>::from(raw[e] == sent ? (U)0 : raw[e]), acc);
+      for (int k = r.k0 + E * TPR; k < r.k1; k += TPR) {
+        const int j = a.pja[k];
+        const int oj = a.rev ? (a.n - 1 - j) : j;
+        acc = fma(a.pval[k], wait_value<T>(a.cur + oj, a.err), acc);
+      }
     }
+#pragma unroll
+    for (int o = TPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, TPR);
+    if (ok && sub == 0) tri_store(a, r.o, Bits<T>::canon(r.rhs - acc));
   }
-  // the last CTA to leave resets the counters for the next launch
-  if (threadIdx.x == 0) {
+  // the last warp to leave resets the counters for the next launch
+  if (lane == 0) {
+    const int nw = (int)(gridDim.x * (blockDim.x >> 5));
     const int done = atomicAdd(&a.counters[1], 1);
-    if (done == (int)gridDim.x - 1) {
+    if (done == nw - 1) {
       a.counters[0] = 0;
       a.counters[1] = 0;
     }

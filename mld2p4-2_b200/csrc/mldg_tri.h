@@ -5,11 +5,6 @@
 
 namespace mldg {
 
-// Levels of at most this many rows are solved by a single CTA (one chunk,
-// partial solution in shared memory); larger ones are cut into chunks.
-constexpr int kTriSingleChunkRows = 16384;
-constexpr int kTriChunkRows = 2048;
-
 struct TriSchedule {
   int n = 0, R = 0, nchunks = 0;
   std::vector<int> chunk_lvl;  // nchunks + 1 : first level index of each chunk

@@ -95,3 +95,18 @@ def test_errors(mld, orc):
     with pytest.raises(mld.MldError) as e:
         h.apply(np.zeros(a.nrows), trans="X")
     assert e.value.code == 40
+
+
+def test_apply_large_coarse_level(mld, orc):
+    """idim=60: level 1 has ~27k rows and ~15 entries per triangular row, so
+    its solves run the multi-CTA sync-free kernel with several lanes per row
+    (warp blocks aligned to dependency levels)."""
+    a = orc.gen_pde3d(60, 1, ISO)
+    op = orc.Prec(oracle_params(orc, "BJAC", mcs=2000))
+    op.build(a)
+    assert op.level_info(1)["n"] > 16384
+    h = upload_oracle_hierarchy(mld, orc, op)
+    rng = np.random.default_rng(60)
+    for trans in ("N", "T"):
+        x = rng.uniform(-1, 1, a.nrows)
+        assert _rel(h.apply(x, trans=trans), op.apply(x, trans)) <= TOL_FP64
