@@ -23,6 +23,7 @@
 #include "mldg.h"
 #include "mldg_kernels.cuh"
 #include "mldg_tri.h"
+#include "mldg_trsv_win.cuh"
 
 namespace mldg {
 
@@ -165,6 +166,24 @@ struct DTri {
   bool present() const { return prow != nullptr; }
 };
 
+// Plan of the windowed cluster solve (k_trsv_win) for one triangular factor.
+template <typename T>
+struct DWin {
+  int n = 0, nsteps = 0, W = 0, wshift = 0, C = 1, D = 4, capR = 0, capE = 0, tpr = 1;
+  int off_win = 0, off_desc = 0, off_bar = 0, off_ring = 0, stage_bytes = 0;
+  size_t smem = 0;
+  int64_t nnz = 0;
+  WinDesc *desc = nullptr;
+  int *orig = nullptr, *pirp = nullptr, *pja = nullptr;
+  T *pval = nullptr;
+  int *nextpos = nullptr;  // feed of the following solve of the pair
+  T *nextscale = nullptr;
+  unsigned long long *trace = nullptr;  // MLDG_WIN_TRACE: per-phase cycle counters
+  std::vector<int> h_orig, h_pos;  // position -> original row, original row -> position
+  std::vector<WinDesc> h_desc;
+  bool ok = false;
+};
+
 static int pick_tpr(int64_t nnz, int nr) {
   const double avg = nr > 0 ? (double)nnz / nr : 0.0;
   if (avg <= 8) return 1;
@@ -195,6 +214,7 @@ static DCSR<T> to_dev(Arena &ar, const HostCSR &h) {
 struct Engine {
   virtual ~Engine() {}
   virtual void record(char trans) = 0;  // issue one V-cycle: xin (FP64) -> yout (FP64)
+  virtual void dump_trace() {}
   int64_t launches = 0;
   int64_t bytes = 0;
   cudaStream_t st = nullptr;
@@ -263,6 +283,10 @@ struct EngineT : Engine {
     DTri<T> L, U, Lt, Ut;
     T *d = nullptr;
     T *x = nullptr, *y = nullptr, *ty = nullptr, *tw = nullptr, *bufA = nullptr, *bufB = nullptr;
+    // windowed cluster solves (k_trsv_win) for both factors of each pair
+    bool win = false;
+    DWin<T> wL, wU, wUt, wLt;
+    T *rp0 = nullptr, *rp1 = nullptr;  // right-hand sides in position order
     // FP16 prolongator values + FP32 row scale (MLDG_PREC_FP32_P16)
     __half *Ph = nullptr;
     float *Pscale = nullptr;
@@ -347,8 +371,61 @@ struct EngineT : Engine {
             (1 + (scale ? 1 : 0) + 1 + (other ? 1 : 0) + (out ? 1 + (beta != T(0)) : 0)));
   }
 
+  void gather(const DWin<T> &w, const T *src, T *dst) {
+    begin(MLDG_KERNEL_VEC);
+    k_gather<T><<<blocks_for(w.n), 256, 0, st>>>(w.n, w.orig, src, (const T *)nullptr, dst);
+    end((int64_t)w.n * (4 + 2 * sizeof(T)));
+  }
+  void wsolve(const DWin<T> &w, const T *rhs, T *next, T *out, T beta, T *tpos = nullptr) {
+    WinArgs<T> a;
+    a.n = w.n;
+    a.nsteps = w.nsteps;
+    a.W = w.W;
+    a.wshift = w.wshift;
+    a.capR = w.capR;
+    a.capE = w.capE;
+    a.D = w.D;
+    a.stage_bytes = w.stage_bytes;
+    a.off_win = w.off_win;
+    a.off_desc = w.off_desc;
+    a.off_bar = w.off_bar;
+    a.off_ring = w.off_ring;
+    a.desc = w.desc;
+    a.orig = w.orig;
+    a.pirp = w.pirp;
+    a.pja = w.pja;
+    a.pval = w.pval;
+    a.rhs = rhs;
+    a.nextpos = w.nextpos;
+    a.nextscale = w.nextscale;
+    a.next = next;
+    a.out = (beta == T(0)) ? out : nullptr;
+    a.tpos = (out && beta != T(0)) ? tpos : nullptr;
+    a.alpha = T(1);
+    a.beta = T(0);
+    a.err = err;
+    a.trace = w.trace;
+    begin(MLDG_KERNEL_TRSV);
+    launch_win(w, a, st);
+    end(w.nnz * (int64_t)(sizeof(T) + 4) + 4 * (2 * (int64_t)w.n + 1) +
+        (int64_t)w.n * sizeof(T) * (1 + (next ? 2 : 0) + (out ? 1 : 0)) + (next ? 4 * (int64_t)w.n : 0));
+    if (out && beta != T(0)) {
+      begin(MLDG_KERNEL_VEC);
+      k_combine<T><<<blocks_for(w.n), 256, 0, st>>>(w.n, w.orig, tpos, T(1), beta, out);
+      end((int64_t)w.n * (4 + 3 * sizeof(T)));
+    }
+  }
+
   // ILU solver apply: y = alpha*U^{-1}(d o L^{-1} x) + beta*y, or the 'T' form
   void ilu_apply(Lev &L, char trans, const T *x, T beta, T *y) {
+    if (L.win) {
+      const DWin<T> &f = (trans == 'N') ? L.wL : L.wUt;
+      const DWin<T> &g = (trans == 'N') ? L.wU : L.wLt;
+      gather(f, x, L.rp0);
+      wsolve(f, L.rp0, L.rp1, nullptr, T(0));
+      wsolve(g, L.rp1, nullptr, y, beta, L.rp0);  // rp0 is free again: results in position order
+      return;
+    }
     if (trans == 'N') {
       trsv(L.L, x, nullptr, L.bufA, L.bufB, nullptr, T(1), T(0));
       trsv(L.U, L.bufA, L.d, L.bufB, L.bufA, y, T(1), beta);
@@ -424,6 +501,20 @@ struct EngineT : Engine {
     }
   }
   void prolong(Lev &C, T *y);
+  void dump_trace() override {
+    for (size_t l = 0; l < lv.size(); ++l) {
+      if (!lv[l].win) continue;
+      const DWin<T> *ws[4] = {&lv[l].wL, &lv[l].wU, &lv[l].wUt, &lv[l].wLt};
+      for (int q = 0; q < 4; ++q) {
+        if (!ws[q]->trace) continue;
+        unsigned long long t[8];
+        cudaMemcpy(t, ws[q]->trace, sizeof t, cudaMemcpyDeviceToHost);
+        if (!t[4]) continue;
+        std::fprintf(stderr, "mldg trace: level %zu win%d C=%d steps %llu: cycles/step wait %.0f compute %.0f barrier %.0f\n",
+                     l, q, ws[q]->C, t[4], (double)t[0] / t[4], (double)t[1] / t[4], (double)t[2] / t[4]);
+      }
+    }
+  }
 
   void record(char trans) override {
     launches = 0;
@@ -534,8 +625,10 @@ static void launch_trsv_t(const DTri<T> &t, const TriArgs<T> &a, cudaStream_t st
   if (t.mode == 0) {
     if (t.stg.D == 3)
       k_trsv_stg<T, TPR, 3><<<1, t.threads, t.smem, st>>>(a, t.stg, t.desc);
-    else
+    else if (t.stg.D == 4)
       k_trsv_stg<T, TPR, 4><<<1, t.threads, t.smem, st>>>(a, t.stg, t.desc);
+    else
+      k_trsv_stg<T, TPR, 6><<<1, t.threads, t.smem, st>>>(a, t.stg, t.desc);
     return;
   }
   if (t.e <= 4)
@@ -560,6 +653,241 @@ static void launch_trsv(const DTri<T> &t, const TriArgs<T> &a, cudaStream_t st) 
 template <typename T>
 constexpr int tri_cta_rows() {
   return (int)(128 * 1024 / sizeof(T));
+}
+
+// dynamic shared memory of k_trsv_win: 227 KB per block minus its static part
+constexpr int kWinSmemMax = 227 * 1024 - 1024;
+
+// Builds the step plan of k_trsv_win for a cluster of C CTAs; returns a plan
+// with ok == false when the window cannot hold every dependency or the shared
+// memory budget cannot fit the stages.
+template <typename T>
+static DWin<T> build_win_plan(const HostCSR &m, bool upper, int C) {
+  DWin<T> w;
+  const int n = m.nr;
+  if (n <= 0) return w;
+  TriSchedule s;
+  build_tri_schedule(n, m.irp.data(), m.ja.data(), m.val.data(), upper, n, &s);
+  const int nlev = (int)s.lvl_ptr.size() - 1;
+  std::vector<int> posof((size_t)n);
+  for (int p = 0; p < n; ++p) posof[s.prow[p]] = p;
+  w.n = n;
+  w.C = C;
+  w.nnz = m.nnz();
+  w.h_orig.resize((size_t)n);
+  w.h_pos.resize((size_t)n);
+  for (int p = 0; p < n; ++p) {
+    w.h_orig[p] = upper ? n - 1 - s.prow[p] : s.prow[p];
+    w.h_pos[w.h_orig[p]] = p;
+  }
+  // window: every dependency q of a row in step [sp0, sp1) needs q >= sp1 - W;
+  // steps end no later than their level, so the level end bounds the span
+  int span = 1;
+  for (int L = 0; L < nlev; ++L) {
+    const int p1 = s.lvl_ptr[L + 1];
+    for (int p = s.lvl_ptr[L]; p < p1; ++p)
+      for (int k = s.pirp[p]; k < s.pirp[p + 1]; ++k) span = std::max(span, p1 - posof[s.pja[k]]);
+  }
+  int W = 32 * C;
+  while (W < span + 1) W <<= 1;
+  const size_t budget = kWinSmemMax;
+  const size_t win_bytes = (size_t)(W / C) * sizeof(T);
+  if (win_bytes + 32 * 1024 > budget) return w;
+  // capacities: the largest CTA slice of any level with one part per level
+  int maxr = 0, maxe = 0;
+  for (int L = 0; L < nlev; ++L) {
+    const int p0 = s.lvl_ptr[L], p1 = s.lvl_ptr[L + 1], nr = p1 - p0;
+    for (int cc = 0; cc < C; ++cc) {
+      const int a = p0 + (int)((int64_t)nr * cc / C), b = p0 + (int)((int64_t)nr * (cc + 1) / C);
+      maxr = std::max(maxr, b - a);
+      maxe = std::max(maxe, s.pirp[b] - s.pirp[a]);
+    }
+  }
+  int capR = std::max(maxr, 1), capE = std::max(maxe, 1);
+  int D = 0;
+  std::vector<WinDesc> desc;
+  std::vector<int> stepends;
+  for (int attempt = 0; attempt < 12; ++attempt) {
+    // steps: split each level into parts whose CTA slices fit (capR, capE)
+    desc.clear();
+    stepends.clear();
+    bool fits = true;
+    for (int L = 0; L < nlev && fits; ++L) {
+      const int p0 = s.lvl_ptr[L], p1 = s.lvl_ptr[L + 1], nr = p1 - p0;
+      const int ne = s.pirp[p1] - s.pirp[p0];
+      int k = std::max(1, std::max((nr + C * capR - 1) / (C * capR), (ne + C * capE - 1) / (C * capE)));
+      for (;; ++k) {
+        bool good = true;
+        for (int j = 0; j < k && good; ++j) {
+          const int a0 = p0 + (int)((int64_t)nr * j / k), b0 = p0 + (int)((int64_t)nr * (j + 1) / k);
+          for (int cc = 0; cc < C && good; ++cc) {
+            const int a = a0 + (int)((int64_t)(b0 - a0) * cc / C), b = a0 + (int)((int64_t)(b0 - a0) * (cc + 1) / C);
+            good = (b - a) <= capR && (s.pirp[b] - s.pirp[a]) <= capE;
+          }
+        }
+        if (good) break;
+        if (k > nr) {
+          fits = false;
+          break;
+        }
+      }
+      if (!fits) break;
+      for (int j = 0; j < k; ++j) {
+        const int a0 = p0 + (int)((int64_t)nr * j / k), b0 = p0 + (int)((int64_t)nr * (j + 1) / k);
+        for (int cc = 0; cc < C; ++cc) {
+          const int a = a0 + (int)((int64_t)(b0 - a0) * cc / C), b = a0 + (int)((int64_t)(b0 - a0) * (cc + 1) / C);
+          desc.push_back(WinDesc{a, b, s.pirp[a], s.pirp[b]});
+        }
+        stepends.push_back(b0);
+      }
+    }
+    const int nsteps = (int)stepends.size();
+    const StageLayout lay = stage_layout<T>(capR, capE);
+    const size_t fixed = (size_t)al16((int)win_bytes) + (size_t)al16(nsteps * 16) + 64;
+    D = 0;
+    if (fits)
+      for (int d : {4, 3})
+        if (fixed + (size_t)d * lay.bytes <= budget) {
+          D = d;
+          break;
+        }
+    if (D) break;
+    capR = std::max(1, capR / 2);
+    capE = std::max(1, capE / 2);
+  }
+  if (!D) return w;
+  // window check
+  {
+    int st = 0;
+    for (int p = 0; p < n; ++p) {
+      while (stepends[st] <= p) ++st;
+      const int lim = stepends[st] - W;
+      for (int k = s.pirp[p]; k < s.pirp[p + 1]; ++k)
+        if (posof[s.pja[k]] < lim) return w;
+    }
+  }
+  w.nsteps = (int)stepends.size();
+  w.W = W;
+  int ws = 0;
+  while ((1 << ws) < W / C) ++ws;
+  w.wshift = ws;
+  w.D = D;
+  w.capR = capR;
+  w.capE = capE;
+  const StageLayout lay = stage_layout<T>(capR, capE);
+  w.stage_bytes = lay.bytes;
+  w.off_win = 0;
+  w.off_desc = al16((int)win_bytes);
+  w.off_bar = w.off_desc + al16(w.nsteps * 16);
+  w.off_ring = w.off_bar + 64;
+  w.smem = (size_t)w.off_ring + (size_t)D * lay.bytes;
+  // lanes per row: few entries per lane (latency), but enough rows per pass
+  const double avg = (double)w.nnz / n;
+  const double rows_per_slice = (double)n / std::max(1, w.nsteps * C);
+  w.tpr = 1;
+  while (w.tpr < 32 && avg / w.tpr > 3.0) w.tpr *= 2;
+  while (w.tpr > 1 && rows_per_slice * w.tpr > 960) w.tpr /= 2;
+  w.h_desc = std::move(desc);
+  w.ok = true;
+  return w;
+}
+
+template <typename T>
+static void upload_win(Arena &ar, DWin<T> &w, const HostCSR &m, bool upper) {
+  // rebuild the schedule arrays (cheap) and upload with tail padding
+  TriSchedule s;
+  build_tri_schedule(w.n, m.irp.data(), m.ja.data(), m.val.data(), upper, w.n, &s);
+  std::vector<int> posof((size_t)w.n);
+  for (int p = 0; p < w.n; ++p) posof[s.prow[p]] = p;
+  std::vector<int> orig(w.h_orig);
+  orig.resize((size_t)w.n + 4, 0);
+  std::vector<int> pirp(s.pirp);
+  pirp.resize((size_t)w.n + 1 + 4, (int)w.nnz);
+  std::vector<int> pja((size_t)w.nnz + 4, 0);
+  for (int64_t k = 0; k < w.nnz; ++k) pja[k] = posof[s.pja[k]];
+  std::vector<T> pval((size_t)w.nnz + 4, T(0));
+  for (int64_t k = 0; k < w.nnz; ++k) pval[k] = (T)s.pval[k];
+  w.orig = ar.upload(orig);
+  w.pirp = ar.upload(pirp);
+  w.pja = ar.upload(pja);
+  w.pval = ar.upload(pval);
+  w.desc = ar.upload(w.h_desc);
+  if (std::getenv("MLDG_WIN_TRACE")) {
+    w.trace = ar.alloc<unsigned long long>(8);
+    MLDG_CUDA(cudaMemset(w.trace, 0, 8 * sizeof(unsigned long long)));
+  }
+}
+
+// the first solve of a pair writes the second one's right-hand side:
+// next[pos2(orig)] = d[orig] * t
+template <typename T>
+static void link_pair(Arena &ar, DWin<T> &first, const DWin<T> &second, const std::vector<double> &d) {
+  std::vector<int> np((size_t)first.n + 4, 0);
+  std::vector<T> ns((size_t)first.n + 4, T(0));
+  for (int p = 0; p < first.n; ++p) {
+    const int o = first.h_orig[p];
+    np[p] = second.h_pos[o];
+    ns[p] = (T)d[o];
+  }
+  first.nextpos = ar.upload(np);
+  first.nextscale = ar.upload(ns);
+}
+
+template <typename T, int TPR, int C, int D>
+static void launch_win_3(const DWin<T> &w, const WinArgs<T> &a, cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    MLDG_CUDA(cudaFuncSetAttribute(k_trsv_win<T, TPR, C, D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   kWinSmemMax));
+    if (C > 8)
+      MLDG_CUDA(cudaFuncSetAttribute(k_trsv_win<T, TPR, C, D>,
+                                     cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    attr = true;
+  }
+  if (C == 1) {
+    k_trsv_win<T, TPR, C, D><<<1, 512, w.smem, st>>>(a);
+    return;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  cfg.gridDim = dim3(C);
+  cfg.blockDim = dim3(512);
+  cfg.dynamicSmemBytes = w.smem;
+  cfg.stream = st;
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = C;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  MLDG_CUDA(cudaLaunchKernelEx(&cfg, k_trsv_win<T, TPR, C, D>, a));
+}
+template <typename T, int TPR, int C>
+static void launch_win_2(const DWin<T> &w, const WinArgs<T> &a, cudaStream_t st) {
+  if (w.D == 3)
+    launch_win_3<T, TPR, C, 3>(w, a, st);
+  else
+    launch_win_3<T, TPR, C, 4>(w, a, st);
+}
+template <typename T, int TPR>
+static void launch_win_1(const DWin<T> &w, const WinArgs<T> &a, cudaStream_t st) {
+  if (w.C == 1)
+    launch_win_2<T, TPR, 1>(w, a, st);
+  else if (w.C == 4)
+    launch_win_2<T, TPR, 4>(w, a, st);
+  else
+    launch_win_2<T, TPR, 16>(w, a, st);
+}
+template <typename T>
+static void launch_win(const DWin<T> &w, const WinArgs<T> &a, cudaStream_t st) {
+  switch (w.tpr) {
+    case 1: launch_win_1<T, 1>(w, a, st); break;
+    case 2: launch_win_1<T, 2>(w, a, st); break;
+    case 4: launch_win_1<T, 4>(w, a, st); break;
+    case 8: launch_win_1<T, 8>(w, a, st); break;
+    case 16: launch_win_1<T, 16>(w, a, st); break;
+    default: launch_win_1<T, 32>(w, a, st); break;
+  }
 }
 
 template <typename T>
@@ -587,29 +915,42 @@ static DTri<T> build_tri_dev(Arena &ar, const HostCSR &m, bool upper, int nsm) {
   while (t.tpr < 32 && avg / t.tpr > 8.0) t.tpr *= 2;
   t.e = (avg / t.tpr <= 4.0) ? 4 : 8;
   t.cta = n <= tri_cta_rows<T>();
-  // staged single-CTA plan: solution + level descriptors + D ring stages
-  {
-    int maxr = 0, maxe = 0;
+  // staged single-CTA plan: solution + level descriptors + D ring stages.
+  // Stages are sized for the 95th-percentile level; larger levels are read
+  // straight from global memory.  Latency-bound, so few entries per lane.
+  if (n <= tri_cta_rows<T>()) {
     std::vector<int4> desc((size_t)t.nlevels);
+    std::vector<int> rs, es;
     for (int L = 0; L < t.nlevels; ++L) {
       const int p0 = s.lvl_ptr[L], p1 = s.lvl_ptr[L + 1];
       desc[L] = make_int4(p0, p1, s.pirp[p0], s.pirp[p1]);
-      maxr = std::max(maxr, p1 - p0);
-      maxe = std::max(maxe, s.pirp[p1] - s.pirp[p0]);
+      rs.push_back(p1 - p0);
+      es.push_back(s.pirp[p1] - s.pirp[p0]);
     }
+    auto pct = [](std::vector<int> v, double q) {
+      std::sort(v.begin(), v.end());
+      return v.empty() ? 1 : std::max(1, v[(size_t)(q * (v.size() - 1))]);
+    };
     StageCfg c{};
-    c.capR = maxr;
-    c.capE = std::max(maxe, 1);
-    c.bytes = (int)(((((size_t)(2 * c.capR + 1 + c.capE) * 4 + 15) & ~(size_t)15) +
-                     (size_t)c.capE * sizeof(T) + 15) & ~(size_t)15);
+    c.capR = pct(rs, 0.95);
+    c.capE = pct(es, 0.95);
     c.off_y = 0;
     c.off_desc = (int)(((size_t)std::max(n, 1) * sizeof(T) + 15) & ~(size_t)15);
     c.off_ring = c.off_desc + (int)(((size_t)t.nlevels * 16 + 15) & ~(size_t)15);
     const size_t budget = 220 * 1024;
-    for (int D = 4; D >= 3; --D) {
-      c.D = D;
-      if ((size_t)c.off_ring + (size_t)D * c.bytes <= budget) break;
-      c.D = 0;
+    c.D = 0;
+    for (int shrink = 0; shrink < 6 && c.D == 0; ++shrink) {
+      c.bytes = (int)(((((size_t)(2 * c.capR + 1 + c.capE) * 4 + 15) & ~(size_t)15) +
+                       (size_t)c.capE * sizeof(T) + 15) & ~(size_t)15);
+      for (int D : {6, 4, 3})  // ring depths compiled into k_trsv_stg
+        if ((size_t)c.off_ring + (size_t)D * c.bytes <= budget) {
+          c.D = D;
+          break;
+        }
+      if (c.D == 0) {
+        c.capE = std::max(1, c.capE / 2);
+        c.capR = std::max(1, c.capR / 2);
+      }
     }
     if (c.D >= 3) {
       t.mode = 0;
@@ -618,6 +959,8 @@ static DTri<T> build_tri_dev(Arena &ar, const HostCSR &m, bool upper, int nsm) {
       t.threads = 512;
       t.grid = 1;
       t.smem = (size_t)c.off_ring + (size_t)c.D * c.bytes;
+      t.tpr = 1;
+      while (t.tpr < 32 && avg / t.tpr > 2.0) t.tpr *= 2;
       return t;
     }
   }
@@ -639,7 +982,9 @@ static DTri<T> build_tri_dev(Arena &ar, const HostCSR &m, bool upper, int nsm) {
     // Warps in flight: a few dependency levels' worth of blocks.  More only
     // adds spinning lanes whose polls compete with real traffic in L2.
     const int per_level = (t.nblk + t.nlevels - 1) / std::max(t.nlevels, 1);
-    const int warps = std::max(32, std::min(4 * per_level, nsm * 32));
+    int mult = 4;
+    if (const char *e = std::getenv("MLDG_SF_MULT")) mult = std::max(1, std::atoi(e));
+    const int warps = std::max(32, std::min(mult * per_level, nsm * 32));
     t.threads = 256;
     t.grid = (warps + 7) / 8;
   }
@@ -651,6 +996,7 @@ static void set_attr_t() {
   const int mx = 224 * 1024;
   MLDG_CUDA(cudaFuncSetAttribute(k_trsv_stg<T, TPR, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   MLDG_CUDA(cudaFuncSetAttribute(k_trsv_stg<T, TPR, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  MLDG_CUDA(cudaFuncSetAttribute(k_trsv_stg<T, TPR, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   MLDG_CUDA(cudaFuncSetAttribute(k_trsv_cta<T, TPR, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   MLDG_CUDA(cudaFuncSetAttribute(k_trsv_cta<T, TPR, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
 }
@@ -713,7 +1059,41 @@ static Engine *make_engine(Handle *h) {
       }
     }
     L.nnz_nd = H.ND.nnz();
-    if (H.kind == MLDG_SMOOTHER_BJAC) {
+    if (H.kind == MLDG_SMOOTHER_BJAC && !std::getenv("MLDG_NO_WIN")) {
+      const int n = H.A.nr;
+      // Single-CTA windows win on small levels; large levels stay on the
+      // sync-free solve unless MLDG_WIN_ALL asks for clusters everywhere.
+      const int C = n > 1000000 ? 16 : (n > 65536 ? 4 : 1);
+      const bool try_win = C == 1 || std::getenv("MLDG_WIN_ALL");
+      HostCSR Lt = transpose(H.L), Ut = transpose(H.U);
+      if (try_win) {
+        L.wL = build_win_plan<T>(H.L, false, C);
+        L.wU = build_win_plan<T>(H.U, true, C);
+        L.wUt = build_win_plan<T>(Ut, false, C);
+        L.wLt = build_win_plan<T>(Lt, true, C);
+      }
+      if (try_win && L.wL.ok && L.wU.ok && L.wUt.ok && L.wLt.ok) {
+        L.win = true;
+        upload_win(ar, L.wL, H.L, false);
+        upload_win(ar, L.wU, H.U, true);
+        upload_win(ar, L.wUt, Ut, false);
+        upload_win(ar, L.wLt, Lt, true);
+        link_pair(ar, L.wL, L.wU, H.d);
+        link_pair(ar, L.wUt, L.wLt, H.d);
+        L.rp0 = ar.alloc<T>((size_t)n + 8);
+        L.rp1 = ar.alloc<T>((size_t)n + 8);
+        MLDG_CUDA(cudaMemset(L.rp0, 0, sizeof(T) * ((size_t)n + 8)));
+        MLDG_CUDA(cudaMemset(L.rp1, 0, sizeof(T) * ((size_t)n + 8)));
+        if (std::getenv("MLDG_VERBOSE")) {
+          const DWin<T> *ws[4] = {&L.wL, &L.wU, &L.wUt, &L.wLt};
+          for (int q = 0; q < 4; ++q)
+            std::fprintf(stderr, "mldg: level %d win%d n=%d C=%d W=%d steps=%d D=%d capR=%d capE=%d tpr=%d smem=%zu\n",
+                         l, q, ws[q]->n, ws[q]->C, ws[q]->W, ws[q]->nsteps, ws[q]->D, ws[q]->capR,
+                         ws[q]->capE, ws[q]->tpr, ws[q]->smem);
+        }
+      }
+    }
+    if (H.kind == MLDG_SMOOTHER_BJAC && !L.win) {
       L.L = build_tri_dev<T>(ar, H.L, false, h->nsm);
       L.U = build_tri_dev<T>(ar, H.U, true, h->nsm);
       HostCSR Lt = transpose(H.L), Ut = transpose(H.U);
@@ -1235,6 +1615,7 @@ extern "C" void mldg_destroy(mldg_handle *hp) {
   Handle &h = hp->h;
   cudaSetDevice(h.opts.device);
   if (h.st) cudaStreamSynchronize(h.st);
+  if (h.eng && std::getenv("MLDG_WIN_TRACE")) h.eng->dump_trace();
   for (int t = 0; t < 2; ++t)
     if (h.gexec[t]) cudaGraphExecDestroy(h.gexec[t]);
   h.eng.reset();

@@ -436,6 +436,7 @@ __device__ __forceinline__ void stage_issue(const TriArgs<T> &a, const StageCfg 
   T *pval_s = reinterpret_cast<T *>(st + (((size_t)(2 * c.capR + 1 + c.capE) * 4 + 15) & ~(size_t)15));
   const int4 d = desc[l];  // p0, p1, e0, e1
   const int nr = d.y - d.x, ne = d.w - d.z;
+  if (nr > c.capR || ne > c.capE) return;  // oversized level: read from global at compute time
   for (int r = threadIdx.x; r < nr; r += blockDim.x) cp_async4(prow_s + r, a.prow + d.x + r);
   for (int r = threadIdx.x; r <= nr; r += blockDim.x) cp_async4(pirp_s + r, a.pirp + d.x + r);
   for (int k = threadIdx.x; k < ne; k += blockDim.x) {
@@ -486,6 +487,13 @@ __global__ void __launch_bounds__(512) k_trsv_stg(TriArgs<T> a, StageCfg c, cons
         reinterpret_cast<const T *>(st + (((size_t)(2 * c.capR + 1 + c.capE) * 4 + 15) & ~(size_t)15));
     const int4 d = desc[L];
     const int nr = d.y - d.x;
+    const bool staged = nr <= c.capR && (d.w - d.z) <= c.capE;
+    if (!staged) {
+      prow_s = a.prow + d.x;
+      pirp_s = a.pirp + d.x;
+      pja_s = a.pja + d.z;
+      pval_s = a.pval + d.z;
+    }
     for (int r0 = 0; r0 < nr; r0 += nslots) {
       const int r = r0 + slot;
       T acc = T(0);
