@@ -54,6 +54,19 @@ def load_oracle():
     return oracle
 
 
+def profiled_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "roofline_traffic.json")) as f:
+            k = json.load(f)["kernels"].get(kernel)
+        if k:
+            t = k["traffic_bytes_per_launch"]
+            return sum(t) / len(t)
+    except Exception:
+        pass
+    return None
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -291,7 +304,9 @@ def run_ours(args, rank, world, local_rank):
         "apply_roofline_frac": apply_bytes / (apply_ms * 1e-3) / 1e9 / peak,
         "roofline": {"bound": "hbm", "kernel": f"{mld.KERNEL_NAMES[dk]} level {dl}",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak if achieved else None, "traffic": None,
+                     "frac": achieved / peak if achieved else None,
+                     "traffic": profiled_traffic(f"{mld.KERNEL_NAMES[dk]} level {dl}")
+                     if args.idim == 160 and args.precision == "FP64" else None,
                      "peak_source": peak_kind, "bytes_per_launch": probe_bytes,
                      "avg_launch_ms": probe_ms / probe_cnt if probe_cnt else None,
                      "launches_timed": probe_cnt,

@@ -744,7 +744,9 @@ int orc_prec_build(orc_prec *p, int n, const int *irp, const int *ja,
   csr_copy(&lv[0].A, n, n, irp, ja, val);
   int nlev = 1;
   int newsz = 0;
-  for (int i = 1; i < nplevs; i++) {
+  /* max_levs == 1: the one-level preconditioner of init('BJAC'/'JACOBI')
+   * (mld_d_hierarchy_bld.f90:159-164 returns at once for one level) */
+  for (int i = 1; i < (par->max_levs == 1 ? 1 : nplevs); i++) {
     const csr *af = &lv[i - 1].A;
     int *ilaggr = (int *)xcalloc((size_t)af->nr, sizeof(int));
     int naggr = 0;

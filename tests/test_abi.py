@@ -1,0 +1,84 @@
+"""CPU: the C-ABI library loads, exports every declared entry point, and
+rejects bad calls on the host side without a GPU."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared(header):
+    txt = open(os.path.join(ROOT, "include", header)).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(mld[gp]_[a-z0-9_]+)\s*\(", txt)))
+
+
+@pytest.mark.parametrize("header", ["mldg.h", "mld_prec.h"])
+def test_library_exports_every_declared_symbol(mld, header):
+    lib = mld.lib()
+    names = _declared(header)
+    assert len(names) >= 8
+    for name in names:
+        assert hasattr(lib, name), f"{name} declared in include/{header} but not exported"
+
+
+def test_null_handle_errors(mld):
+    lib = mld.lib()
+    assert lib.mldg_upload_level(None, 0, None) == 30
+    assert lib.mldg_finalize(None, 1, 0) == 30
+    assert lib.mldg_apply(None, None, None, b"N", 1, 0, 0) == 30
+    assert lib.mldg_last_error(None) == b"null handle"
+    lib.mldg_destroy(None)  # no-op
+
+
+def test_host_mirror_set_and_build_errors(mld):
+    p = mld.MldPrec()
+    with pytest.raises(mld.MldError) as e:
+        p.set("SMOOTHER_TYPE", "BJAC")          # set before init
+    assert e.value.code == 3111
+    p.init("ML")
+    with pytest.raises(mld.MldError):
+        p.set("NO_SUCH_KEY", 1)
+    a = mld.gen_pde3d(6, 1)
+    # the reference's ML default smoother (FBGS) has no GPU apply
+    with pytest.raises(mld.MldError) as e:
+        p.hierarchy_build(a)
+    assert "FBGS" in str(e.value)
+    p.set("SMOOTHER_TYPE", "BJAC")
+    p.set("ML_CYCLE", "WCYCLE")
+    with pytest.raises(mld.MldError) as e:
+        p.hierarchy_build(a)
+    assert "ML_CYCLE" in str(e.value)
+    with pytest.raises(mld.MldError) as e:
+        p.apply(np.zeros(a.nrows))
+    assert e.value.code == mld.ERR_NOT_BUILT
+
+
+def test_host_mirror_descr_and_levels(mld):
+    p = mld.MldPrec()
+    p.init("ML")
+    p.set("SMOOTHER_TYPE", "JACOBI")
+    p.set("SMOOTHER_SWEEPS", 2)
+    p.set("SMOOTHER_DAMPING", 0.8)
+    p.set("MIN_COARSE_SIZE", 100)
+    p.hierarchy_build(mld.gen_pde3d(12, 1))
+    assert p.nlev >= 2
+    info = p.level_info(1)
+    assert info["n"] == info["naggr"] and info["nnzP"] == info["nnzR"]
+
+
+def test_kappa_generator_is_symmetric_and_matches_constant_case(mld):
+    idim = 6
+    k = np.ones(idim ** 3)
+    a = mld.gen_kappa3d(idim, k)
+    b = mld.gen_pde3d(idim, 1, (1, 1, 1, 0, 0, 0, 0))
+    assert np.array_equal(a.irp, b.irp) and np.array_equal(a.ja, b.ja)
+    assert np.allclose(a.val, b.val, rtol=1e-14)
+    rng = np.random.default_rng(0)
+    a2 = mld.gen_kappa3d(idim, np.exp(rng.normal(size=idim ** 3)))
+    import scipy.sparse as sp
+    m = sp.csr_matrix((a2.val, a2.ja, a2.irp))
+    assert abs(m - m.T).max() <= 1e-9 * abs(m).max()
