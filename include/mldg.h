@@ -173,6 +173,28 @@ int mldg_probe_read(mldg_handle *h, double *total_ms, int64_t *count, int64_t *b
  * graph, with CUDA events around every launch; writes up to max entries. */
 int mldg_profile(mldg_handle *h, char trans, int max, mldg_kernel_stat *stats, int *n);
 
+/* ---- allocation-free relative residual --------------------------------- */
+/* No counterpart in the reference.  For callers that must not allocate
+ * device memory: code that runs while a CUDA graph is being captured (where
+ * cudaMalloc is not allowed), applications whose memory pool owns every
+ * device byte, and convergence checks in tight loops where cudaMalloc /
+ * cudaFree would synchronise the device.
+ *
+ * Computes *relres = ||b - A x||_2 / ||b||_2 (1 when ||b|| = 0).  A's arrays
+ * and x, b are DEVICE pointers, 0-based CSR, nrows == ncols == n.  The
+ * residual vector and the reduction partials live in one file-scope device
+ * array of MLDG_NOALLOC_MAX_N + 1024 doubles (about 4 MiB) that every GPU
+ * loading the library keeps until exit; n > MLDG_NOALLOC_MAX_N is rejected
+ * with MLDG_ERR_SIZE.  Nothing is allocated: the first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress) once, so make that
+ * first call before any stream capture.  All calls share the array and it
+ * keeps the last call's contents; calls that overlap on the GPU (other
+ * streams, other threads) race on it.  Runs on the handle's stream and
+ * returns after the result is on the host. */
+#define MLDG_NOALLOC_MAX_N 524288
+int mldg_relres_noalloc(mldg_handle *h, const mldg_csr *A, const double *x, const double *b,
+                        double *relres);
+
 const char *mldg_last_error(const mldg_handle *h);
 
 /* replaces: prec%free (mlprec/mld_d_prec_type.f90:537-568) */

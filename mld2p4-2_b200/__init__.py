@@ -128,6 +128,8 @@ def lib():
                                       C.POINTER(C.c_int64)]
         L.mldg_profile.argtypes = [vp, C.c_char, C.c_int, C.POINTER(_KStat),
                                    C.POINTER(C.c_int)]
+        L.mldg_relres_noalloc.argtypes = [vp, C.POINTER(_CSR), C.c_void_p, C.c_void_p,
+                                          C.POINTER(C.c_double)]
         L.mldg_last_error.argtypes = [vp]
         L.mldg_last_error.restype = C.c_char_p
         L.mldg_destroy.argtypes = [vp]

@@ -17,6 +17,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1603,6 +1604,90 @@ extern "C" int mldg_profile(mldg_handle *hp, char trans, int max, mldg_kernel_st
     if (n) *n = k;
     mldg::check_device_error(&h);
   });
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free relative residual (see mldg.h).  The scratch of this entry
+// point is a file-scope device array: [0, MAX_N) holds the residual r,
+// [MAX_N, MAX_N + 3*kRedBlocks) the per-block partials of the two-pass
+// reduction, the next 3 doubles its result.  Nothing there needs to start at
+// zero: every call overwrites r, every partial and the result before reading
+// them.
+static __device__ __align__(256) double g_noalloc_scratch[MLDG_NOALLOC_MAX_N + 1024];
+static_assert(3 * mldg::kRedBlocks + 3 <= 1024, "scratch tail too small for the partials");
+
+namespace {
+std::mutex g_noalloc_mu;
+double *g_noalloc_ptr[128] = {nullptr};  // device address of the array, per device
+
+// once per device, with that device current
+double *noalloc_scratch(int device) {
+  if (device < 0 || device >= 128) mldg::fail(MLDG_ERR_ARG, "device %d out of range", device);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      mldg::fail(MLDG_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+    g_noalloc_ptr[device] = (double *)p;
+  }
+  return g_noalloc_ptr[device];
+}
+}  // namespace
+
+static void relres_noalloc(Handle &h, const mldg_csr *A, const double *x, const double *b,
+                           double *relres) {
+  {
+    if (!A || !x || !b || !relres) mldg::fail(MLDG_ERR_ARG, "null argument");
+    const int n = A->nrows;
+    if (n < 0 || A->ncols != n) mldg::fail(MLDG_ERR_ARG, "A must be square (%d x %d)", n, A->ncols);
+    if (n > MLDG_NOALLOC_MAX_N)
+      mldg::fail(MLDG_ERR_SIZE, "n = %d exceeds the allocation-free limit MLDG_NOALLOC_MAX_N = %d", n,
+                 MLDG_NOALLOC_MAX_N);
+    if (n > 0 && (!A->irp || !A->ja || !A->val)) mldg::fail(MLDG_ERR_ARG, "null CSR array");
+    MLDG_CUDA(cudaSetDevice(h.opts.device));
+    double *scratch = noalloc_scratch(h.opts.device);
+    double *r = scratch;
+    double *partial = scratch + MLDG_NOALLOC_MAX_N;
+    double *res = partial + 3 * mldg::kRedBlocks;
+    if (n == 0) {
+      *relres = 1.0;
+      return;
+    }
+    // r = b - A x with the row length of A choosing the lanes per row
+    int64_t nnz = 0;
+    MLDG_CUDA(cudaMemcpyAsync(&nnz, A->irp + n, sizeof(int32_t), cudaMemcpyDeviceToHost, h.st));
+    MLDG_CUDA(cudaStreamSynchronize(h.st));
+    nnz = (int64_t)(int32_t)nnz;
+    const int tpr = mldg::pick_tpr(nnz, n);
+    const int64_t thr = (int64_t)n * tpr;
+    const int g = (int)std::max<int64_t>(1, std::min<int64_t>((thr + 255) / 256, (int64_t)h.nsm * 16));
+    switch (tpr) {
+#define CASE(K)                                                                                 \
+  case K:                                                                                       \
+    mldg::k_spmv<double, K><<<g, 256, 0, h.st>>>(n, A->irp, A->ja, A->val, x, -1.0, b, 1.0, r, 0.0); \
+    break;
+      CASE(1) CASE(2) CASE(4) CASE(8) CASE(16) CASE(32)
+#undef CASE
+      default: mldg::fail(MLDG_ERR_INTERNAL, "bad tpr");
+    }
+    // ||b||^2, ||r||^2: per-block partials, then one block in a fixed order
+    mldg::k_dots<<<mldg::kRedBlocks, mldg::kRedThreads, 0, h.st>>>(n, 2, b, b, r, r, nullptr, nullptr,
+                                                                     partial);
+    mldg::k_dots_final<<<1, mldg::kRedThreads, 0, h.st>>>(mldg::kRedBlocks, partial, res);
+    double out[3] = {0, 0, 0};
+    MLDG_CUDA(cudaMemcpyAsync(out, res, 3 * sizeof(double), cudaMemcpyDeviceToHost, h.st));
+    MLDG_CUDA(cudaStreamSynchronize(h.st));
+    MLDG_CUDA(cudaGetLastError());
+    const double bn = std::sqrt(out[0]);
+    *relres = bn == 0.0 ? 1.0 : std::sqrt(out[1]) / bn;
+  }
+}
+
+extern "C" int mldg_relres_noalloc(mldg_handle *hp, const mldg_csr *A, const double *x,
+                                   const double *b, double *relres) {
+  if (!hp) return MLDG_ERR_ARG;
+  MLDG_GUARD(hp, { relres_noalloc(hp->h, A, x, b, relres); });
 }
 
 extern "C" const char *mldg_last_error(const mldg_handle *hp) {
