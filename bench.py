@@ -207,6 +207,68 @@ def config(args, a, p):
     return c
 
 
+def time_variant(mld, a, b, smoother, precision, args, dev, torch, probe=False, dist=None):
+    """Build one preconditioner form and time K FCG solves (device events)."""
+    p = make_prec(mld, a, smoother, precision, device=dev)
+    n = a.nrows
+    bd = torch.tensor(b, dtype=torch.float64, device=f"cuda:{dev}")
+    x0 = torch.zeros(n, dtype=torch.float64, device=f"cuda:{dev}")
+    xs = torch.zeros_like(x0)
+    torch.cuda.synchronize()
+    p.apply(bd, xs)  # first apply captures the graph
+    res = {"p": p, "bd": bd, "xs": xs}
+    if probe:
+        # dominant kernel: the (kind, level) group with the largest device time
+        prof = p.profile("N")
+        groups = {}
+        for e in prof:
+            g = groups.setdefault((e["kind_id"], e["level"]), [0.0, 0, 0])
+            g[0] += e["ms"]
+            g[1] += 1
+            g[2] += e["bytes"]
+        (dk, dl), (dms, _, _) = max(groups.items(), key=lambda kv: kv[1][0])
+        p.probe_set(dk, dl, 0)
+        res.update(dk=dk, dl=dl, share=dms / sum(e["ms"] for e in prof))
+
+    def solve():
+        xs.copy_(x0)
+        torch.cuda.synchronize()
+        _, it, rr = mld.krylov("FCG", a, p, bd, xs, eps=args.eps, itmax=500, use_prec_matrix=True)
+        ms, nl = p.last_timing()
+        return it, rr, ms, nl
+
+    for _ in range(args.warmup):
+        solve()
+    p.probe_read()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    tot, launches, its, rr = 0.0, 0, [], None
+    for _ in range(args.steps):
+        it, rr, ms, nl = solve()
+        tot += ms
+        launches += nl
+        its.append(it)
+    torch.cuda.synchronize()
+    res["probe"] = p.probe_read()
+    if dist is not None:
+        t = torch.tensor([tot], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot = float(t.item())
+    ap = []
+    for _ in range(5):
+        p.apply(bd, xs)
+        ap.append(p.last_timing()[0])
+    res.update(tot_ms=tot, launches=launches, iters=its[-1], relres=rr,
+               apply_ms=min(ap), apply_bytes=p.apply_bytes())
+    # solution error of the last timed solve
+    xs.copy_(x0)
+    torch.cuda.synchronize()
+    mld.krylov("FCG", a, p, bd, xs, eps=args.eps, itmax=500, use_prec_matrix=True)
+    res["err"] = float(torch.max(torch.abs(xs - 1.0)))
+    return res
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     mld = load_package()
@@ -217,55 +279,20 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist_
         dist = dist_
     a, b = build_problem(mld, args.idim)
-    p = make_prec(mld, a, args.smoother, args.precision, device=dev)
     n = a.nrows
-    # dominant kernel: the (kind, level) group with the largest device time
-    bd = torch.tensor(b, dtype=torch.float64, device=f"cuda:{dev}")
-    x0 = torch.zeros(n, dtype=torch.float64, device=f"cuda:{dev}")
-    xs = torch.zeros_like(x0)
-    torch.cuda.synchronize()
-    p.apply(bd, xs)  # first apply captures the graph
-    prof = p.profile("N")
-    groups = {}
-    for e in prof:
-        k = (e["kind_id"], e["level"])
-        g = groups.setdefault(k, [0.0, 0, 0])
-        g[0] += e["ms"]
-        g[1] += 1
-        g[2] += e["bytes"]
-    (dk, dl), (dms, dcnt, dbytes) = max(groups.items(), key=lambda kv: kv[1][0])
-    p.probe_set(dk, dl, 0)
-    apply_ms_prof = sum(e["ms"] for e in prof)
-
-    def solve(x_dev, b_dev):
-        x_dev.copy_(x0)
-        torch.cuda.synchronize()
-        _, it, rr = mld.krylov("FCG", a, p, b_dev, x_dev, eps=args.eps, itmax=500,
-                               use_prec_matrix=True)
-        ms, nl = p.last_timing()
-        return it, rr, ms, nl
-
-    for _ in range(args.warmup):
-        solve(xs, bd)
-    p.probe_read()
-    # timed region: device time from the library's CUDA events, max over ranks
-    if dist is not None:
-        dist.barrier()
-    torch.cuda.synchronize()
+    peak, peak_kind = peaks()
     with Clocks(dev) as clk:
-        tot_ms, launches, its = 0.0, 0, []
-        for _ in range(args.steps):
-            it, rr, ms, nl = solve(xs, bd)
-            tot_ms += ms
-            launches += nl
-            its.append(it)
-    torch.cuda.synchronize()
-    probe_ms, probe_cnt, probe_bytes = p.probe_read()
-    if dist is not None:
-        t = torch.tensor([tot_ms], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms = float(t.item())
-    err = float(torch.linalg.norm(xs - 1.0) / np.sqrt(n))
+        main = time_variant(mld, a, b, args.smoother, args.precision, args, dev, torch, probe=True,
+                            dist=dist)
+        others = {}
+        if not args.no_variants:
+            for sm, pr in (("JACOBI", "FP64"), ("BJAC", "FP32")):
+                if (sm, pr) == (args.smoother, args.precision):
+                    continue
+                r = time_variant(mld, a, b, sm, pr, args, dev, torch, dist=dist)
+                others[f"{sm.lower()}_{pr.lower()}"] = r
+                r["p"].free()
+    p = main["p"]
     # end-to-end through the public API with host buffers (pinned)
     bh = torch.empty(n, dtype=torch.float64, pin_memory=True)
     bh.copy_(torch.from_numpy(b))
@@ -273,47 +300,52 @@ def run_ours(args, rank, world, local_rank):
     e2e_ms = 0.0
     for s in range(args.steps):
         xh.zero_()
-        _, it_h, _ = mld.krylov("FCG", a, p, bh, xh, eps=args.eps, itmax=500,
-                                use_prec_matrix=True)
+        mld.krylov("FCG", a, p, bh, xh, eps=args.eps, itmax=500, use_prec_matrix=True)
         e2e_ms += p.last_timing()[0]
     if dist is not None:
         t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{dev}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    # apply alone (V-cycle), device-timed, for the HBM GB/s of the whole cycle
-    ap_ms = []
-    for _ in range(5):
-        p.apply(bd, xs)
-        ap_ms.append(p.last_timing()[0])
-    apply_ms = min(ap_ms)
-    apply_bytes = p.apply_bytes()
     if rank != 0:
         return
-    peak, peak_kind = peaks()
+    probe_ms, probe_cnt, probe_bytes = main["probe"]
     achieved = (probe_bytes * probe_cnt) / (probe_ms * 1e-3) / 1e9 if probe_ms > 0 else None
+    kname = f"{mld.KERNEL_NAMES[main['dk']]} level {main['dl']}"
+
+    def summary(r, label):
+        return {"form": label, "time_to_1e-10_ms": r["tot_ms"] / args.steps,
+                "solves_per_s": world * args.steps / (r["tot_ms"] * 1e-3),
+                "iterations": r["iters"], "final_relres": r["relres"],
+                "max_abs_err_vs_ones": r["err"], "apply_ms": r["apply_ms"],
+                "apply_algorithmic_bytes": r["apply_bytes"],
+                "apply_gbs": r["apply_bytes"] / (r["apply_ms"] * 1e-3) / 1e9,
+                "apply_frac_of_peak": r["apply_bytes"] / (r["apply_ms"] * 1e-3) / 1e9 / peak}
+
+    variants = {f"{args.smoother.lower()}_{args.precision.lower()}":
+                summary(main, f"{args.smoother} smoother, {args.precision} V-cycle")}
+    for k, r in others.items():
+        variants[k] = summary(r, k)
     line = {
-        "metric": METRIC, "value": world * args.steps / (tot_ms * 1e-3), "unit": "solves/s",
+        "metric": METRIC, "value": world * args.steps / (main["tot_ms"] * 1e-3), "unit": "solves/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": main["tot_ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if args.precision == "FP64" else "f32/f64",
         "data": "synthetic", "config": config(args, a, p),
-        "iterations": its[-1], "time_to_1e-10_ms": tot_ms / args.steps,
-        "final_relres": rr, "max_abs_err_vs_ones": err,
-        "apply_ms": apply_ms, "apply_algorithmic_bytes": apply_bytes,
-        "apply_gbs": apply_bytes / (apply_ms * 1e-3) / 1e9,
-        "apply_roofline_frac": apply_bytes / (apply_ms * 1e-3) / 1e9 / peak,
-        "roofline": {"bound": "hbm", "kernel": f"{mld.KERNEL_NAMES[dk]} level {dl}",
-                     "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak if achieved else None,
-                     "traffic": profiled_traffic(f"{mld.KERNEL_NAMES[dk]} level {dl}")
+        "iterations": main["iters"], "time_to_1e-10_ms": main["tot_ms"] / args.steps,
+        "final_relres": main["relres"], "max_abs_err_vs_ones": main["err"],
+        "apply_ms": main["apply_ms"], "apply_algorithmic_bytes": main["apply_bytes"],
+        "apply_gbs": main["apply_bytes"] / (main["apply_ms"] * 1e-3) / 1e9,
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                     "traffic": profiled_traffic(kname)
                      if args.idim == 160 and args.precision == "FP64" else None,
                      "peak_source": peak_kind, "bytes_per_launch": probe_bytes,
                      "avg_launch_ms": probe_ms / probe_cnt if probe_cnt else None,
-                     "launches_timed": probe_cnt,
-                     "share_of_apply": dms / apply_ms_prof if apply_ms_prof else None},
+                     "launches_timed": probe_cnt, "share_of_apply": main["share"]},
+        "variants": variants,
         "e2e": {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "solves/s",
                 "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 8 * n},
-        "gpu_launches": launches,
+        "gpu_launches": main["launches"],
         "clocks": clk.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:
@@ -325,7 +357,7 @@ def run_ours(args, rank, world, local_rank):
         line["cpu_baseline"] = {"value": 1.0 / dt, "unit": "solves/s", "cores": orc.num_threads(),
                                 "kind": "port",
                                 "sample": f"1 full FCG solve to {args.eps:g} ({it_c} iterations), "
-                                          f"idim={args.idim}, oracle (C restatement)"}
+                                          f"idim={args.idim}, {args.smoother} smoother, oracle (C restatement)"}
     print(json.dumps(line), flush=True)
 
 
@@ -340,6 +372,8 @@ def main():
     ap.add_argument("--precision", default="FP64", choices=["FP64", "FP32", "FP32_P16"])
     ap.add_argument("--eps", type=float, default=1e-10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-variants", action="store_true",
+                    help="time only the selected smoother/precision form")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

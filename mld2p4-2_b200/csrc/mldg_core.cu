@@ -287,6 +287,8 @@ struct EngineT : Engine {
     // windowed cluster solves (k_trsv_win) for both factors of each pair
     bool win = false;
     DWin<T> wL, wU, wUt, wLt;
+    // coarsest level: explicit inverse of its ILU(0) factorisation (and its transpose)
+    T *minv = nullptr, *minvT = nullptr;
     T *rp0 = nullptr, *rp1 = nullptr;  // right-hand sides in position order
     // FP16 prolongator values + FP32 row scale (MLDG_PREC_FP32_P16)
     __half *Ph = nullptr;
@@ -419,6 +421,13 @@ struct EngineT : Engine {
 
   // ILU solver apply: y = alpha*U^{-1}(d o L^{-1} x) + beta*y, or the 'T' form
   void ilu_apply(Lev &L, char trans, const T *x, T beta, T *y) {
+    if (L.minv) {
+      const T *M = (trans == 'N') ? L.minv : L.minvT;
+      begin(MLDG_KERNEL_VEC);
+      k_gemv<T><<<blocks_for((int64_t)L.n * 32), 256, 0, st>>>(L.n, M, x, T(1), beta, y);
+      end((int64_t)L.n * L.n * sizeof(T) + (int64_t)L.n * sizeof(T) * (2 + (beta != T(0))));
+      return;
+    }
     if (L.win) {
       const DWin<T> &f = (trans == 'N') ? L.wL : L.wUt;
       const DWin<T> &g = (trans == 'N') ? L.wU : L.wLt;
@@ -502,17 +511,66 @@ struct EngineT : Engine {
     }
   }
   void prolong(Lev &C, T *y);
+  // Lanes-per-row autotuner: times k_spmv with every TPR on each level's
+  // operators (A, A^T, P, R, ND, ND^T) and keeps the fastest.
+  void autotune_spmv(int reps) {
+    cudaEvent_t e0, e1;
+    MLDG_CUDA(cudaEventCreate(&e0));
+    MLDG_CUDA(cudaEventCreate(&e1));
+    for (size_t l = 0; l < lv.size(); ++l) {
+      Lev &L = lv[l];
+      DCSR<T> *ops[6] = {&L.A, &L.AT, &L.P, &L.R, &L.ND, &L.NDT};
+      for (DCSR<T> *op : ops) {
+        if (!op->present() || op->nr == 0) continue;
+        // scratch vectors of this level/its neighbour large enough for nc / nr
+        const int nmax = std::max(op->nr, op->nc);
+        T *v = scratch_for(nmax, 0), *o = scratch_for(nmax, 1);
+        float best = 1e30f;
+        int best_t = op->tpr;
+        for (int t : {1, 2, 4, 8, 16, 32}) {
+          op->tpr = t;
+          spmv(*op, v, T(1), nullptr, T(0), o, T(0));  // warm
+          MLDG_CUDA(cudaEventRecord(e0, st));
+          for (int r = 0; r < reps; ++r) spmv(*op, v, T(1), nullptr, T(0), o, T(0));
+          MLDG_CUDA(cudaEventRecord(e1, st));
+          MLDG_CUDA(cudaEventSynchronize(e1));
+          float ms = 0;
+          MLDG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+          if (ms < best) {
+            best = ms;
+            best_t = t;
+          }
+        }
+        op->tpr = best_t;
+      }
+    }
+    launches = 0;
+    bytes = 0;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  T *tune_buf[2] = {nullptr, nullptr};
+  int tune_n = 0;
+  T *scratch_for(int n, int which) {
+    if (n > tune_n) fail(MLDG_ERR_INTERNAL, "autotune scratch too small");
+    return tune_buf[which];
+  }
+
   void dump_trace() override {
     for (size_t l = 0; l < lv.size(); ++l) {
       if (!lv[l].win) continue;
       const DWin<T> *ws[4] = {&lv[l].wL, &lv[l].wU, &lv[l].wUt, &lv[l].wLt};
       for (int q = 0; q < 4; ++q) {
         if (!ws[q]->trace) continue;
-        unsigned long long t[8];
-        cudaMemcpy(t, ws[q]->trace, sizeof t, cudaMemcpyDeviceToHost);
+        unsigned long long t[16] = {0};
+        cudaMemcpy(t, ws[q]->trace, 16 * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
         if (!t[4]) continue;
-        std::fprintf(stderr, "mldg trace: level %zu win%d C=%d steps %llu: cycles/step wait %.0f compute %.0f barrier %.0f\n",
-                     l, q, ws[q]->C, t[4], (double)t[0] / t[4], (double)t[1] / t[4], (double)t[2] / t[4]);
+        std::fprintf(stderr,
+                     "mldg trace: level %zu win%d C=%d steps %llu: cycles/step wait %.0f compute %.0f barrier %.0f | "
+                     "kernel cycles/step %.0f ns/step %.0f (clock %.0f MHz) loop cycles/step %.0f prologue cycles/step %.0f\n",
+                     l, q, ws[q]->C, t[4], (double)t[0] / t[4], (double)t[1] / t[4], (double)t[2] / t[4],
+                     (double)t[5] / t[4], (double)t[6] / t[4], t[6] ? 1e3 * (double)t[5] / (double)t[6] : 0.0,
+                     (double)t[7] / t[4], (double)t[8] / t[4]);
       }
     }
   }
@@ -814,8 +872,8 @@ static void upload_win(Arena &ar, DWin<T> &w, const HostCSR &m, bool upper) {
   w.pval = ar.upload(pval);
   w.desc = ar.upload(w.h_desc);
   if (std::getenv("MLDG_WIN_TRACE")) {
-    w.trace = ar.alloc<unsigned long long>(8);
-    MLDG_CUDA(cudaMemset(w.trace, 0, 8 * sizeof(unsigned long long)));
+    w.trace = ar.alloc<unsigned long long>(16);
+    MLDG_CUDA(cudaMemset(w.trace, 0, 16 * sizeof(unsigned long long)));
   }
 }
 
@@ -1014,6 +1072,42 @@ static void set_trsv_smem_attr() {
   done = true;
 }
 
+// Coarsest levels up to this size are solved with the explicit inverse of
+// their ILU(0) factorisation: the same operator as the two triangular solves
+// (U^{-1} diag(d) L^{-1}), applied as one bandwidth-bound matrix-vector
+// product instead of a chain of dependency levels.
+constexpr int kDenseCoarseRows = 2048;
+
+// M = U^{-1} diag(d) L^{-1} (row-major) and its transpose, column by column
+static void dense_ilu_inverse(const HostCSR &Lf, const HostCSR &Uf, const std::vector<double> &d,
+                              std::vector<double> &M, std::vector<double> &MT) {
+  const int n = Lf.nr;
+  M.assign((size_t)n * n, 0.0);
+  MT.assign((size_t)n * n, 0.0);
+#pragma omp parallel
+  {
+    std::vector<double> t((size_t)n), z((size_t)n);
+#pragma omp for schedule(dynamic, 8)
+    for (int j = 0; j < n; ++j) {
+      for (int i = 0; i < n; ++i) {  // t = L^{-1} e_j
+        double s = 0.0;
+        for (int k = Lf.irp[i]; k < Lf.irp[i + 1]; ++k) s += Lf.val[k] * t[Lf.ja[k]];
+        t[i] = (i == j ? 1.0 : 0.0) - s;
+      }
+      for (int i = 0; i < n; ++i) t[i] *= d[i];
+      for (int i = n - 1; i >= 0; --i) {  // z = U^{-1} t
+        double s = 0.0;
+        for (int k = Uf.irp[i]; k < Uf.irp[i + 1]; ++k) s += Uf.val[k] * z[Uf.ja[k]];
+        z[i] = t[i] - s;
+      }
+      for (int i = 0; i < n; ++i) {
+        M[(size_t)i * n + j] = z[i];
+        MT[(size_t)j * n + i] = z[i];
+      }
+    }
+  }
+}
+
 template <typename T>
 static Engine *make_engine(Handle *h) {
   set_trsv_smem_attr<T>();
@@ -1121,6 +1215,14 @@ static Engine *make_engine(Handle *h) {
         L.NDT = to_dev<T>(ar, transpose(H.ND));
       }
     }
+    if (H.kind == MLDG_SMOOTHER_BJAC && l == h->nlev - 1 && h->nlev > 1 && L.n <= kDenseCoarseRows &&
+        !std::getenv("MLDG_NO_DENSE_COARSE")) {
+      std::vector<double> M, MT;
+      dense_ilu_inverse(H.L, H.U, H.d, M, MT);
+      std::vector<T> m(M.begin(), M.end()), mt(MT.begin(), MT.end());
+      L.minv = ar.upload(m);
+      L.minvT = ar.upload(mt);
+    }
     std::vector<T> dv(H.d.begin(), H.d.end());
     L.d = ar.upload(dv);
     const int n = std::max(L.n, 1);
@@ -1144,6 +1246,16 @@ static Engine *make_engine(Handle *h) {
     }
   }
   MLDG_CUDA(cudaStreamSynchronize(h->st));
+  if (h->opts.autotune) {
+    int nmax = 1;
+    for (auto &L : e->lv) nmax = std::max(nmax, L.n);
+    e->tune_n = nmax;
+    e->tune_buf[0] = ar.alloc<T>(nmax);
+    e->tune_buf[1] = ar.alloc<T>(nmax);
+    k_fill<T><<<64, 256, 0, h->st>>>(nmax, T(1), e->tune_buf[0]);
+    e->autotune_spmv(5);
+    MLDG_CUDA(cudaStreamSynchronize(h->st));
+  }
   return e;
 }
 

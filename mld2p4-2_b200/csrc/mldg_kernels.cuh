@@ -212,6 +212,29 @@ __global__ void __launch_bounds__(256) k_jacobi(int nr, const int *__restrict__ 
   }
 }
 
+// Dense coarsest-level solve: out = alpha * M x + beta * out with M the
+// explicit inverse of the coarsest ILU(0) factorisation (row-major n x n),
+// one warp per row.
+template <typename T>
+__global__ void __launch_bounds__(256) k_gemv(int n, const T *__restrict__ M, const T *__restrict__ x,
+                                              T alpha, T beta, T *out) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = warp; i < n; i += nwarps) {
+    const T *row = M + (size_t)i * n;
+    T s = T(0);
+    for (int j = lane; j < n; j += 32) s = fma(row[j], __ldg(x + j), s);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+      T r = alpha * s;
+      if (beta != T(0)) r = fma(beta, out[i], r);
+      out[i] = r;
+    }
+  }
+}
+
 // out = alpha * d o x + beta * out     (diag solver apply, :102)
 template <typename T>
 __global__ void k_diag(int n, const T *__restrict__ d, const T *__restrict__ x, T alpha, T beta,

@@ -206,6 +206,11 @@ __global__ void __launch_bounds__(512, 1) k_trsv_win(WinArgs<T> a) {
   WinDesc *desc = reinterpret_cast<WinDesc *>(sm + a.off_desc);
   uint64_t *bar = reinterpret_cast<uint64_t *>(sm + a.off_bar);
   unsigned char *ring = sm + a.off_ring;
+  unsigned long long k_t0 = 0, k_ns0 = 0;
+  if (a.trace && threadIdx.x == 0 && blockIdx.x == 0) {
+    k_t0 = clock64();
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(k_ns0));
+  }
   const StageLayout L = stage_layout<T>(a.capR, a.capE);
   const unsigned win_s = smem_u32(win);
   const unsigned ring_s = smem_u32(ring);
@@ -254,26 +259,39 @@ __global__ void __launch_bounds__(512, 1) k_trsv_win(WinArgs<T> a) {
     mbar_expect_tx(&bar[d], sl.bytes);  // this lane's arrival (+ its bytes)
     if (sl.bytes) tma_bulk_g2s(st + dst, sl.src, sl.bytes, &bar[d]);
   };
-  if (producer)
+  // The producer alone waits for each stage's TMA completion (mbarrier,
+  // acquire) before the step barrier; the barrier then publishes the staged
+  // data to the consumer warps, which never poll the mbarrier themselves.
+  __shared__ int s_fail;  // set by the producer when a stage never completed
+  if (tid == 0) s_fail = 0;
+  __syncthreads();
+  if (producer) {
     for (int s = 0; s < D - 1; ++s) issue(s);
+    if (a.nsteps > 0 && !mbar_wait(&bar[0], 0u) && (tid & 31) == 0) {
+      s_fail = 1;
+      atomicExch(a.err, 4021);
+    }
+  }
+  __syncthreads();
   constexpr int RPW = 32 / TPR;
   const int lane = tid & 31;
   const int sub = lane % TPR;
   const int slot = warp * RPW + lane / TPR;
   const int nslots = ((int)(blockDim.x >> 5) - 1) * RPW;
-  bool ok = true;
   const bool tr = a.trace && rank == 0 && tid == 0;
   unsigned long long c_wait = 0, c_comp = 0, c_bar = 0, t0 = 0, t1 = 0;
+  const unsigned long long loop_t0 = tr ? clock64() : 0ull;
   for (int step = 0; step < a.nsteps; ++step) {
     const int d = step % D;
     if (producer) {
       issue(step + D - 1);  // stage (step-1) % D: its readers passed the last barrier
-    } else {
-      if (tr) t0 = clock64();
-      if (!mbar_wait(&bar[d], (unsigned)((step / D) & 1))) {
-        ok = false;
+      const int nx = step + 1;
+      if (nx < a.nsteps && !mbar_wait(&bar[nx % D], (unsigned)((nx / D) & 1)) && (tid & 31) == 0) {
+        s_fail = 1;
         atomicExch(a.err, 4021);
       }
+    } else {
+      if (tr) t0 = clock64();
       if (tr) {
         t1 = clock64();
         c_wait += t1 - t0;
@@ -291,7 +309,7 @@ __global__ void __launch_bounds__(512, 1) k_trsv_win(WinArgs<T> a) {
       const unsigned a_nsc = st + L.o_nsc + (unsigned)sizeof(T) * o[6];
       const WinDesc w = desc[step];
       const int nr = w.r1 - w.r0;
-      if (ok) {
+      if (!s_fail) {
         for (int r0 = 0; r0 < nr; r0 += nslots) {
           const int r = r0 + slot;
           T acc = T(0);
@@ -362,10 +380,16 @@ __global__ void __launch_bounds__(512, 1) k_trsv_win(WinArgs<T> a) {
     if (tr) c_bar += clock64() - t0;
   }
   if (tr) {
+    unsigned long long ns1;
+    a.trace[7] += clock64() - loop_t0;
+    a.trace[8] += loop_t0 - k_t0;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(ns1));
     a.trace[0] += c_wait;
     a.trace[1] += c_comp;
     a.trace[2] += c_bar;
     a.trace[4] += (unsigned long long)a.nsteps;
+    a.trace[5] += clock64() - k_t0;
+    a.trace[6] += ns1 - k_ns0;
   }
   // keep this CTA's window alive until every peer has finished reading it
   if (C > 1)
