@@ -245,9 +245,10 @@ class Hierarchy(_GpuDiag):
     def _gpu(self):
         return self._h
 
-    def __init__(self, device: int = 0, use_graphs: bool = True, index_base: int = 0):
+    def __init__(self, device: int = 0, use_graphs: bool = True, index_base: int = 0,
+                 autotune: bool = True):
         self._h = C.c_void_p()
-        o = _Opts(device, index_base, 1 if use_graphs else 0, 1)
+        o = _Opts(device, index_base, 1 if use_graphs else 0, 1 if autotune else 0)
         rc = lib().mldg_create(C.byref(self._h), C.byref(o))
         if rc:
             raise MldError(rc, "mldg_create failed (no usable CUDA device?)")

@@ -53,9 +53,9 @@ def oracle_params(orc, smoother="BJAC", sweeps=1, damp=1.0, coarse_sweeps=4, mcs
                               coarse_sweeps=coarse_sweeps, min_coarse_size=mcs)
 
 
-def upload_oracle_hierarchy(mld, orc, oprec, use_graphs=True, precision=0):
+def upload_oracle_hierarchy(mld, orc, oprec, use_graphs=True, precision=0, autotune=True):
     """Upload the oracle's (reference-algorithm) hierarchy through the C ABI."""
-    h = mld.Hierarchy(use_graphs=use_graphs)
+    h = mld.Hierarchy(use_graphs=use_graphs, autotune=autotune)
     for l in range(oprec.nlev):
         info = oprec.level_info(l)
         def conv(m):

@@ -40,13 +40,20 @@ def test_apply_without_graphs_identical(mld, orc):
     a = orc.gen_pde3d(14, 1, ISO)
     op = orc.Prec(oracle_params(orc, "BJAC", mcs=300))
     op.build(a)
-    h1 = upload_oracle_hierarchy(mld, orc, op, use_graphs=True)
-    h2 = upload_oracle_hierarchy(mld, orc, op, use_graphs=False)
+    # launch shapes pinned (no autotuning): graph replay and direct launches
+    # run the same kernels with the same schedules -> identical bits
+    h1 = upload_oracle_hierarchy(mld, orc, op, use_graphs=True, autotune=False)
+    h2 = upload_oracle_hierarchy(mld, orc, op, use_graphs=False, autotune=False)
     x = np.random.default_rng(3).uniform(-1, 1, a.nrows)
     y1, y2 = h1.apply(x), h2.apply(x)
-    # the triangular solves are deterministic: same kernels, same schedule
     assert np.array_equal(y1, y2)
     assert np.array_equal(h1.apply(x), y1)
+    # an autotuned handle may pick other lanes-per-row (summation order), so
+    # it agrees to rounding, and is bitwise repeatable on its own
+    h3 = upload_oracle_hierarchy(mld, orc, op)
+    y3 = h3.apply(x)
+    assert np.linalg.norm(y3 - y1) <= 1e-14 * np.linalg.norm(y1)
+    assert np.array_equal(h3.apply(x), y3)
 
 
 def test_fp32_apply(mld, orc):
