@@ -252,9 +252,8 @@ def time_variant(mld, a, b, smoother, precision, args, dev, torch, probe=False, 
     torch.cuda.synchronize()
     res["probe"] = p.probe_read()
     if dist is not None:
-        t = torch.tensor([tot], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot = float(t.item())
+        from mld2p4_2_b200 import dist as mdist
+        tot = mdist.max_over_ranks(tot, device=f"cuda:{dev}")
     ap = []
     for _ in range(5):
         p.apply(bd, xs)
@@ -303,9 +302,8 @@ def run_ours(args, rank, world, local_rank):
         mld.krylov("FCG", a, p, bh, xh, eps=args.eps, itmax=500, use_prec_matrix=True)
         e2e_ms += p.last_timing()[0]
     if dist is not None:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+        from mld2p4_2_b200 import dist as mdist
+        e2e_ms = mdist.max_over_ranks(e2e_ms, device=f"cuda:{dev}")
     if rank != 0:
         return
     probe_ms, probe_cnt, probe_bytes = main["probe"]
