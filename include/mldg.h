@@ -134,6 +134,26 @@ int mldg_krylov(mldg_handle *h, int method, const mldg_csr *A,
                 const double *b, double *x, double tol, int itmax,
                 int *iters, double *relres, int mem_kind);
 
+/* Adjoint solve A^T lambda = g with flexible CG in FP64, preconditioned by
+ * the transposed V-cycle M^{-T} (the reference's trans='T' apply,
+ * mld_dmlprec_aply.f90:634-656,765-777: smoothers swapped, A^T residuals,
+ * U^T/L^T triangular solves).  lambda holds the initial guess on entry;
+ * stops on ||g - A^T lambda||_2 / ||g||_2 <= tol.  No counterpart as an entry
+ * point in the reference (it composes psb_krylov with trans='T'). */
+int mldg_adjoint(mldg_handle *h, const double *g, double *lambda, double tol, int itmax,
+                 int *iters, double *relres, int mem_kind);
+
+/* dL/dkappa for -div(kappa grad u) = f assembled by the harmonic-mean face
+ * rule on idim^3 cells (h = 1/(idim+1), zero Dirichlet boundary faces taking
+ * the cell's own kappa): given the forward solution x and the adjoint
+ * lambda (A^T lambda = dL/dx),
+ *   grad[c] = -(1/h^2) [ sum_{interior faces (c,s)} 2 kappa_s^2/(kappa_c+kappa_s)^2
+ *                           (lambda_c - lambda_s)(x_c - x_s)
+ *                        + (boundary faces of c) lambda_c x_c ].
+ * One thread per cell, no atomics.  No counterpart in the reference. */
+int mldg_kappa_grad(mldg_handle *h, int idim, const double *kappa, const double *x,
+                    const double *lambda, double *grad, int mem_kind);
+
 /* Per-level sizes of the finalized hierarchy:
  * info[0..4] = n, nnz(A), nnz(P), nnz(L)+nnz(U)+nnz(ND), number of levels. */
 int mldg_level_info(const mldg_handle *h, int lev, int64_t *info);

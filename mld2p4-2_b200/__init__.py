@@ -99,6 +99,29 @@ class _GpuDiag:
         lib().mldg_last_timing(self._gpu(), C.byref(ms), C.byref(nl))
         return ms.value, nl.value
 
+    def adjoint(self, g, lam=None, eps: float = 1e-10, itmax: int = 500):
+        """Solve A^T lam = g (FCG with the transposed V-cycle). Returns (lam, iters, relres)."""
+        if lam is None:
+            lam = np.zeros_like(g) if isinstance(g, np.ndarray) else g.new_zeros(g.shape)
+        lp, gp, mem = _vec_args(lam, g)
+        it = C.c_int(0)
+        rr = C.c_double(0)
+        rc = lib().mldg_adjoint(self._gpu(), gp, lp, eps, itmax, C.byref(it), C.byref(rr), mem)
+        if rc and rc != ERR_NOT_CONVERGED:
+            raise MldError(rc, lib().mldg_last_error(self._gpu()).decode())
+        return lam, it.value, rr.value
+
+    def kappa_grad(self, idim: int, kappa, x, lam, grad=None):
+        """dL/dkappa from the forward solution x and the adjoint lam (harmonic-mean faces)."""
+        if grad is None:
+            grad = np.zeros_like(x) if isinstance(x, np.ndarray) else x.new_zeros(x.shape)
+        kp, xp, mem = _vec_args(kappa, x)
+        lp, gp, _ = _vec_args(lam, grad)
+        rc = lib().mldg_kappa_grad(self._gpu(), idim, kp, xp, lp, gp, mem)
+        if rc:
+            raise MldError(rc, lib().mldg_last_error(self._gpu()).decode())
+        return grad
+
     def apply_bytes(self) -> int:
         b = C.c_int64(0)
         lib().mldg_apply_bytes(self._gpu(), C.byref(b))
@@ -130,6 +153,10 @@ def lib():
                                    C.POINTER(C.c_int)]
         L.mldg_relres_noalloc.argtypes = [vp, C.POINTER(_CSR), C.c_void_p, C.c_void_p,
                                           C.POINTER(C.c_double)]
+        L.mldg_adjoint.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_double, C.c_int,
+                                   C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int]
+        L.mldg_kappa_grad.argtypes = [vp, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_int]
         L.mldg_last_error.argtypes = [vp]
         L.mldg_last_error.restype = C.c_char_p
         L.mldg_destroy.argtypes = [vp]
@@ -223,6 +250,29 @@ def gen_kappa3d(idim: int, kappa: np.ndarray) -> CSR:
     if rc:
         raise MldError(rc, "gen_kappa3d")
     return CSR(irp, ja, val)
+
+
+def grf3d(idim: int, corr_len: float = 0.1, variance: float = 1.0, seed: int = 0) -> np.ndarray:
+    """Smooth Gaussian random field on the idim^3 cells of the unit cube.
+
+    White noise filtered in Fourier space by exp(-(corr_len k)^2 / 4) (its
+    square is the spectrum of the squared-exponential covariance of length
+    corr_len) on a periodic grid padded by 3 correlation lengths, then
+    standardised to mean 0 and the requested variance.  Returned flat in the
+    generator's row order (x slowest, z fastest).
+    """
+    h = 1.0 / (idim + 1)
+    pad = int(np.ceil(3 * corr_len / h))
+    N = idim + pad
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal((N, N, N))
+    k = 2 * np.pi * np.fft.fftfreq(N, d=h)
+    kz = 2 * np.pi * np.fft.rfftfreq(N, d=h)
+    K2 = k[:, None, None] ** 2 + k[None, :, None] ** 2 + kz[None, None, :] ** 2
+    f = np.fft.irfftn(np.fft.rfftn(w) * np.exp(-(corr_len ** 2) * K2 / 4.0), s=(N, N, N))
+    f = f[:idim, :idim, :idim]
+    f = (f - f.mean()) / f.std() * np.sqrt(variance)
+    return np.ascontiguousarray(f.reshape(-1))
 
 
 def _vec_args(x, y):

@@ -655,7 +655,7 @@ struct Handle {
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   int64_t glaunch[2] = {0, 0}, gbytes[2] = {0, 0};
   // Krylov state (FP64)
-  DCSR<double> A0;
+  DCSR<double> A0, A0T;
   double *kb = nullptr, *kx = nullptr, *kd = nullptr, *kq = nullptr, *kpart = nullptr;
   KrylovScalars *ksc = nullptr;
   double *hpin = nullptr;  // pinned host scalar mirror
@@ -1312,6 +1312,7 @@ static void finalize(Handle *h, int nlev, int precision) {
   MLDG_CUDA(cudaMemset(h->xin, 0, sizeof(double) * n0));
   MLDG_CUDA(cudaMemset(h->yout, 0, sizeof(double) * n0));
   h->A0 = to_dev<double>(h->arena, h->host[0].A);
+  h->A0T = DCSR<double>();
   h->kb = h->arena.alloc<double>(n0);
   h->kx = h->arena.alloc<double>(n0);
   h->kd = h->arena.alloc<double>(n0);
@@ -1435,7 +1436,7 @@ static void spmv64(Handle *h, const DCSR<double> &A, const double *v, double a1,
 }
 
 static void krylov(Handle *h, int method, const mldg_csr *Acsr, const double *b, double *x,
-                   double tol, int itmax, int *iters, double *relres, int mem) {
+                   double tol, int itmax, int *iters, double *relres, int mem, char trans = 'N') {
   if (!h->finalized) fail(MLDG_ERR_NOT_BUILT, "krylov before build");
   if (method != 0 && method != 1) fail(MLDG_ERR_ARG, "method must be 0 (CG) or 1 (FCG)");
   if (!b || !x) fail(MLDG_ERR_ARG, "null vector");
@@ -1443,6 +1444,11 @@ static void krylov(Handle *h, int method, const mldg_csr *Acsr, const double *b,
   const int n = h->n0;
   DCSR<double> A = h->A0;
   Arena tmp;
+  if (trans != 'N') {
+    // A^T of the finest level, built on first use
+    if (!h->A0T.present()) h->A0T = to_dev<double>(h->arena, transpose(h->host[0].A));
+    A = h->A0T;
+  }
   if (Acsr) {
     HostCSR ha = copy_csr(*Acsr, h->opts.index_base, "krylov A", 0);
     if (ha.nr != n || ha.nc != n) fail(MLDG_ERR_SIZE, "krylov A must be %d x %d", n, n);
@@ -1467,7 +1473,7 @@ static void krylov(Handle *h, int method, const mldg_csr *Acsr, const double *b,
   const int nb = kRedBlocks;
   while (err > tol && it < itmax) {
     ++it;
-    run_vcycle(h, 'N');  // z = M^{-1} r
+    run_vcycle(h, trans);  // z = M^{-1} r (or M^{-T} r)
     if (method == 1) {
       if (it > 1) {
         dots(h, n, 1, z, q, nullptr, nullptr, nullptr, nullptr);
@@ -1612,6 +1618,50 @@ extern "C" int mldg_krylov(mldg_handle *hp, int method, const mldg_csr *A, const
     if (it >= itmax && relres && *relres > tol)
       mldg::fail(MLDG_ERR_NOT_CONVERGED, "not converged in %d iterations (relres %.3e)", it, *relres);
   });
+}
+
+extern "C" int mldg_adjoint(mldg_handle *hp, const double *g, double *lambda, double tol, int itmax,
+                            int *iters, double *relres, int mem_kind) {
+  if (!hp) return MLDG_ERR_ARG;
+  int it = 0;
+  MLDG_GUARD(hp, {
+    mldg::krylov(&hp->h, 1, nullptr, g, lambda, tol, itmax, &it, relres, mem_kind, 'T');
+    if (iters) *iters = it;
+    if (it >= itmax && relres && *relres > tol)
+      mldg::fail(MLDG_ERR_NOT_CONVERGED, "adjoint not converged in %d iterations (relres %.3e)", it, *relres);
+  });
+}
+
+static void kappa_grad(Handle &h, int idim, const double *kappa, const double *x, const double *lam,
+                       double *grad, int mem) {
+  if (idim <= 0 || !kappa || !x || !lam || !grad) mldg::fail(MLDG_ERR_ARG, "bad kappa_grad arguments");
+  MLDG_CUDA(cudaSetDevice(h.opts.device));
+  const long long n = (long long)idim * idim * idim;
+  const double hh = 1.0 / (double)(idim + 1);
+  const int blocks = (int)std::min<long long>((n + 255) / 256, (long long)h.nsm * 16);
+  if (mem == MLDG_MEM_DEVICE) {
+    mldg::k_kappa_grad<<<blocks, 256, 0, h.st>>>(idim, 1.0 / (hh * hh), kappa, x, lam, grad);
+    MLDG_CUDA(cudaStreamSynchronize(h.st));
+    MLDG_CUDA(cudaGetLastError());
+    return;
+  }
+  if (mem != MLDG_MEM_HOST) mldg::fail(MLDG_ERR_ARG, "bad mem_kind");
+  mldg::Arena tmp;  // host buffers: staged through device copies
+  double *dk = tmp.alloc<double>((size_t)n), *dx = tmp.alloc<double>((size_t)n);
+  double *dl = tmp.alloc<double>((size_t)n), *dg = tmp.alloc<double>((size_t)n);
+  MLDG_CUDA(cudaMemcpyAsync(dk, kappa, sizeof(double) * n, cudaMemcpyHostToDevice, h.st));
+  MLDG_CUDA(cudaMemcpyAsync(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice, h.st));
+  MLDG_CUDA(cudaMemcpyAsync(dl, lam, sizeof(double) * n, cudaMemcpyHostToDevice, h.st));
+  mldg::k_kappa_grad<<<blocks, 256, 0, h.st>>>(idim, 1.0 / (hh * hh), dk, dx, dl, dg);
+  MLDG_CUDA(cudaMemcpyAsync(grad, dg, sizeof(double) * n, cudaMemcpyDeviceToHost, h.st));
+  MLDG_CUDA(cudaStreamSynchronize(h.st));
+  tmp.release();
+}
+
+extern "C" int mldg_kappa_grad(mldg_handle *hp, int idim, const double *kappa, const double *x,
+                               const double *lambda, double *grad, int mem_kind) {
+  if (!hp) return MLDG_ERR_ARG;
+  MLDG_GUARD(hp, { kappa_grad(hp->h, idim, kappa, x, lambda, grad, mem_kind); });
 }
 
 extern "C" int mldg_level_info(const mldg_handle *hp, int lev, int64_t *info) {

@@ -235,6 +235,30 @@ __global__ void __launch_bounds__(256) k_gemv(int n, const T *__restrict__ M, co
   }
 }
 
+// dL/dkappa of -div(kappa grad u) with harmonic-mean faces (see mldg.h)
+__global__ void k_kappa_grad(int idim, double ih2, const double *__restrict__ kappa,
+                             const double *__restrict__ x, const double *__restrict__ lam,
+                             double *__restrict__ grad) {
+  const long long s2 = (long long)idim * idim, n = s2 * idim;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(c / s2), iy = (int)((c / idim) % idim), iz = (int)(c % idim);
+    const double kc = kappa[c], xc = x[c], lc = lam[c];
+    const bool in[6] = {ix > 0, iy > 0, iz > 0, iz < idim - 1, iy < idim - 1, ix < idim - 1};
+    const long long nb[6] = {c - s2, c - idim, c - 1, c + 1, c + idim, c + s2};
+    double g = 0.0;
+    for (int q = 0; q < 6; ++q) {
+      if (in[q]) {
+        const double ks = kappa[nb[q]], den = kc + ks;
+        g += 2.0 * ks * ks / (den * den) * (lc - lam[nb[q]]) * (xc - x[nb[q]]);
+      } else {
+        g += lc * xc;
+      }
+    }
+    grad[c] = -ih2 * g;
+  }
+}
+
 // out = alpha * d o x + beta * out     (diag solver apply, :102)
 template <typename T>
 __global__ void k_diag(int n, const T *__restrict__ d, const T *__restrict__ x, T alpha, T beta,
