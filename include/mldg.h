@@ -118,6 +118,9 @@ int mldg_finalize(mldg_handle *h, int nlev, int precision);
 /* y = M^{-1} x (trans 'N') or y = M^{-T} x (trans 'T'/'C') for nrhs vectors
  * stored column by column with leading dimension ld (ld >= n).
  * mem_kind: MLDG_MEM_HOST or MLDG_MEM_DEVICE for both x and y.
+ * nrhs > 1 runs blocks of up to 32 columns through one multi-vector V-cycle
+ * (every kernel works on all columns of the block at once); the result of
+ * each column is that of nrhs = 1 up to rounding order.
  * replaces: prec%apply(x,y,desc_a,info,trans,work) ->
  *   mld_dprecaply2_vect (mlprec/impl/mld_dprecaply.f90:305-443) ->
  *   mld_dmlprec_aply_vect (mlprec/impl/mld_dmlprec_aply.f90:203-357). */
@@ -133,6 +136,18 @@ int mldg_apply(mldg_handle *h, const double *x, double *y, char trans,
 int mldg_krylov(mldg_handle *h, int method, const mldg_csr *A,
                 const double *b, double *x, double tol, int itmax,
                 int *iters, double *relres, int mem_kind);
+
+/* nrhs independent CG/FCG solves A x_c = b_c sharing this preconditioner,
+ * advanced together in blocks of up to 32 columns (one multi-vector V-cycle
+ * and SpMM per iteration, per-column scalars).  b and x are column-major with
+ * leading dimensions ldb, ldx >= n; x holds the initial guesses.  Each column
+ * stops on its own ||b_c - A x_c||_2 / ||b_c||_2 <= tol and is frozen from
+ * then on; iters[c] and relres[c] report it.  Returns MLDG_ERR_NOT_CONVERGED
+ * if a column reached itmax above tol.  No counterpart in the reference (a
+ * caller there loops psb_krylov over the right-hand sides). */
+int mldg_krylov_multi(mldg_handle *h, int method, const mldg_csr *A, int nrhs,
+                      const double *b, int ldb, double *x, int ldx, double tol,
+                      int itmax, int *iters, double *relres, int mem_kind);
 
 /* Adjoint solve A^T lambda = g with flexible CG in FP64, preconditioned by
  * the transposed V-cycle M^{-T} (the reference's trans='T' apply,

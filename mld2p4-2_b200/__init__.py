@@ -122,6 +122,36 @@ class _GpuDiag:
             raise MldError(rc, lib().mldg_last_error(self._gpu()).decode())
         return grad
 
+    def apply_block(self, X, Y=None, trans: str = "N"):
+        """Y = M^{-1} X for a block of right-hand sides: X has shape (nrhs, n),
+        contiguous (column c of the C-ABI block is X[c]); numpy or torch."""
+        if Y is None:
+            Y = np.zeros_like(X) if isinstance(X, np.ndarray) else X.new_zeros(X.shape)
+        nrhs, ld = X.shape
+        xp, yp, mem = _vec_args(X, Y)
+        rc = lib().mldg_apply(self._gpu(), xp, yp, trans.encode(), nrhs, ld, mem)
+        if rc:
+            raise MldError(rc, lib().mldg_last_error(self._gpu()).decode())
+        return Y
+
+    def krylov_multi(self, method: str, B, X=None, eps: float = 1e-10, itmax: int = 500,
+                     A: "CSR | None" = None):
+        """nrhs independent CG/FCG solves advanced together (mldg_krylov_multi).
+        B has shape (nrhs, n).  Returns (X, iters[nrhs], relres[nrhs])."""
+        m = {"CG": 0, "FCG": 1}[method.upper()]
+        if X is None:
+            X = np.zeros_like(B) if isinstance(B, np.ndarray) else B.new_zeros(B.shape)
+        nrhs, ld = B.shape
+        xp, bp, mem = _vec_args(X, B)
+        it = (C.c_int * max(nrhs, 1))()
+        rr = (C.c_double * max(nrhs, 1))()
+        Ac = A.c() if A is not None else None
+        rc = lib().mldg_krylov_multi(self._gpu(), m, C.byref(Ac) if Ac is not None else None, nrhs,
+                                     bp, ld, xp, X.shape[1], eps, itmax, it, rr, mem)
+        if rc and rc != ERR_NOT_CONVERGED:
+            raise MldError(rc, lib().mldg_last_error(self._gpu()).decode())
+        return X, np.array(it[:nrhs]), np.array(rr[:nrhs])
+
     def apply_bytes(self) -> int:
         b = C.c_int64(0)
         lib().mldg_apply_bytes(self._gpu(), C.byref(b))
@@ -143,6 +173,9 @@ def lib():
         L.mldg_krylov.argtypes = [vp, C.c_int, C.POINTER(_CSR), C.c_void_p, C.c_void_p,
                                   C.c_double, C.c_int, C.POINTER(C.c_int),
                                   C.POINTER(C.c_double), C.c_int]
+        L.mldg_krylov_multi.argtypes = [vp, C.c_int, C.POINTER(_CSR), C.c_int, C.c_void_p, C.c_int,
+                                        C.c_void_p, C.c_int, C.c_double, C.c_int,
+                                        C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int]
         L.mldg_level_info.argtypes = [vp, C.c_int, C.POINTER(C.c_int64)]
         L.mldg_last_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
         L.mldg_apply_bytes.argtypes = [vp, C.POINTER(C.c_int64)]

@@ -19,10 +19,12 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "mldg.h"
 #include "mldg_kernels.cuh"
+#include "mldg_multi.cuh"
 #include "mldg_tri.h"
 #include "mldg_trsv_win.cuh"
 
@@ -164,6 +166,10 @@ struct DTri {
   bool cta = true;  // single-CTA kernel (solution in shared memory) vs sync-free
   int threads = 512, grid = 1;
   size_t smem = 0;
+  std::vector<int> h_lvl;  // level pointers (host copy)
+  // multi-RHS sync-free solve (k_trsv_sf_m): level-aligned blocks of 32/K rows, per log2(K)
+  int2 *blkm[6] = {};
+  int nblkm[6] = {}, gridm[6] = {};
   bool present() const { return prow != nullptr; }
 };
 
@@ -210,11 +216,36 @@ static DCSR<T> to_dev(Arena &ar, const HostCSR &h) {
   return d;
 }
 
+// multi-RHS kernels are compiled for K = 2, 4, 8, 16, 32 columns
+template <typename F>
+static void kdispatch(int K, F &&f) {
+  switch (K) {
+    case 2: f(std::integral_constant<int, 2>()); break;
+    case 4: f(std::integral_constant<int, 4>()); break;
+    case 8: f(std::integral_constant<int, 8>()); break;
+    case 16: f(std::integral_constant<int, 16>()); break;
+    case 32: f(std::integral_constant<int, 32>()); break;
+    default: fail(MLDG_ERR_INTERNAL, "bad multi-vector width %d", K);
+  }
+}
+static int ilog2(int K) {
+  int r = 0;
+  while ((1 << r) < K) ++r;
+  return r;
+}
+
 // ---------------------------------------------------------------------------
 // Engine: one precision form of the V-cycle.
 struct Engine {
   virtual ~Engine() {}
   virtual void record(char trans) = 0;  // issue one V-cycle: xin (FP64) -> yout (FP64)
+  // Multi-RHS V-cycle on K row-interleaved columns: xin_m -> yout_m (FP64,
+  // n0 x K interleaved).  ensure_multi allocates the K-wide buffers (true when
+  // they were reallocated, which invalidates captured multi graphs).
+  virtual bool ensure_multi(int K) = 0;
+  virtual void record_multi(char trans, int K) = 0;
+  double *xin_m = nullptr, *yout_m = nullptr, *col_m = nullptr;
+  int mcap = 0;
   virtual void dump_trace() {}
   int64_t launches = 0;
   int64_t bytes = 0;
@@ -272,6 +303,12 @@ struct Engine {
   }
 };
 
+template <typename T>
+__global__ void k_axpby1(int n, const T *__restrict__ x, T beta, T *y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    y[i] = (beta == T(0)) ? x[i] : fma(beta, y[i], x[i]);
+}
+
 struct Handle;
 
 template <typename T>
@@ -284,6 +321,8 @@ struct EngineT : Engine {
     DTri<T> L, U, Lt, Ut;
     T *d = nullptr;
     T *x = nullptr, *y = nullptr, *ty = nullptr, *tw = nullptr, *bufA = nullptr, *bufB = nullptr;
+    // K-wide (row-interleaved) counterparts for the multi-RHS V-cycle
+    T *xm = nullptr, *ym = nullptr, *tym = nullptr, *twm = nullptr, *bufAm = nullptr, *bufBm = nullptr;
     // windowed cluster solves (k_trsv_win) for both factors of each pair
     bool win = false;
     DWin<T> wL, wU, wUt, wLt;
@@ -556,6 +595,270 @@ struct EngineT : Engine {
     return tune_buf[which];
   }
 
+  // ---- multi-RHS V-cycle: K columns row-interleaved, v[i*K + c] ----
+  int K = 2;
+  Arena marena;  // K-wide buffers and block tables (grown on demand)
+  ~EngineT() override { marena.release(); }
+  int64_t nk(int n) const { return (int64_t)n * K; }
+
+  void build_blk_m(DTri<T> &t, int Kw) {
+    const int ki = ilog2(Kw), rpw = 32 / Kw;
+    const int nl = (int)t.h_lvl.size() - 1;
+    std::vector<int2> blk;
+    blk.reserve((size_t)t.n / rpw + (size_t)std::max(nl, 0) + 1);
+    for (int L = 0; L < nl; ++L)
+      for (int p = t.h_lvl[L]; p < t.h_lvl[L + 1]; p += rpw)
+        blk.push_back(make_int2(p, std::min(p + rpw, t.h_lvl[L + 1])));
+    t.nblkm[ki] = (int)blk.size();
+    t.blkm[ki] = marena.upload(blk);
+    // as for the single-vector solve: a few dependency levels of blocks in flight
+    const int per_level = (t.nblkm[ki] + nl - 1) / std::max(nl, 1);
+    const int warps = std::max(32, std::min(4 * per_level, nsm * 32));
+    t.gridm[ki] = (warps + 7) / 8;
+  }
+  bool ensure_multi(int Kw) override {
+    bool grown = false;
+    if (Kw > mcap) {
+      marena.release();
+      for (auto &L : lv) {
+        L.xm = L.ym = L.tym = L.twm = L.bufAm = L.bufBm = nullptr;
+        for (DTri<T> *t : {&L.L, &L.U, &L.Ut, &L.Lt})
+          for (int q = 0; q < 6; ++q) {
+            t->blkm[q] = nullptr;
+            t->nblkm[q] = t->gridm[q] = 0;
+          }
+      }
+      mcap = Kw;
+      const size_t n0 = (size_t)std::max(lv[0].n, 1);
+      if ((int64_t)n0 * mcap >= (int64_t)INT32_MAX) fail(MLDG_ERR_SIZE, "n * nrhs too large");
+      xin_m = marena.alloc<double>(n0 * mcap);
+      yout_m = marena.alloc<double>(n0 * mcap);
+      col_m = marena.alloc<double>(n0 * mcap);
+      for (size_t l = 0; l < lv.size(); ++l) {
+        Lev &L = lv[l];
+        const size_t n = (size_t)std::max(L.n, 1) * mcap;
+        if (l == 0 && std::is_same<T, double>::value) {
+          L.xm = (T *)xin_m;
+          L.ym = (T *)yout_m;
+        } else {
+          L.xm = marena.alloc<T>(n);
+          L.ym = marena.alloc<T>(n);
+        }
+        L.tym = marena.alloc<T>(n);
+        L.twm = marena.alloc<T>(n);
+        MLDG_CUDA(cudaMemsetAsync(L.ym, 0, sizeof(T) * n, st));
+        MLDG_CUDA(cudaMemsetAsync(L.tym, 0, sizeof(T) * n, st));
+        MLDG_CUDA(cudaMemsetAsync(L.twm, 0, sizeof(T) * n, st));
+        if (L.kind == MLDG_SMOOTHER_BJAC && !L.minv) {
+          // exchange buffers start as all-sentinel (bufAm stays so after every solve pair)
+          L.bufAm = marena.alloc<T>(n);
+          L.bufBm = marena.alloc<T>(n);
+          k_fill<T><<<blocks_for((int64_t)n), 256, 0, st>>>((int)n, Sentinel<T>::value(), L.bufAm);
+          k_fill<T><<<blocks_for((int64_t)n), 256, 0, st>>>((int)n, Sentinel<T>::value(), L.bufBm);
+        }
+      }
+      grown = true;
+    }
+    const int ki = ilog2(Kw);
+    for (auto &L : lv) {
+      if (L.kind != MLDG_SMOOTHER_BJAC || L.minv) continue;
+      for (DTri<T> *t : {&L.L, &L.U, &L.Ut, &L.Lt}) {
+        if (!t->present()) fail(MLDG_ERR_INTERNAL, "multi-RHS solve without a level schedule");
+        if (!t->blkm[ki]) build_blk_m(*t, Kw);
+      }
+    }
+    MLDG_CUDA(cudaStreamSynchronize(st));
+    return grown;
+  }
+
+  void spmm(const DCSR<T> &A, const T *v, T a1, const T *b, T a0, T *out, T a2) {
+    const int g = blocks_for(nk(A.nr));
+    begin(MLDG_KERNEL_SPMV);
+    kdispatch(K, [&](auto kc) {
+      constexpr int KK = decltype(kc)::value;
+      k_spmm<T, KK><<<g, 256, 0, st>>>(A.nr, A.irp, A.ja, A.val, v, a1, b, a0, out, a2);
+    });
+    end(A.nnz * (int64_t)(sizeof(T) + 4) + 4 * ((int64_t)A.nr + 1) + nk(A.nc) * (int64_t)sizeof(T) +
+        nk(A.nr) * (int64_t)sizeof(T) * (1 + (b ? 1 : 0) + (a2 != T(0) ? 1 : 0)));
+  }
+  void jacobi_m(const DCSR<T> &ND, const T *d, const T *x, const T *ty, int first, T omega, T alpha, T beta,
+                T *out) {
+    const int g = blocks_for(nk(ND.nr));
+    begin(MLDG_KERNEL_JACOBI);
+    kdispatch(K, [&](auto kc) {
+      constexpr int KK = decltype(kc)::value;
+      k_jacobi_m<T, KK><<<g, 256, 0, st>>>(ND.nr, ND.irp, ND.ja, ND.val, d, x, ty, first, omega, alpha, beta, out);
+    });
+    end(ND.nnz * (int64_t)(sizeof(T) + 4) + 4 * ((int64_t)ND.nr + 1) + (int64_t)ND.nr * sizeof(T) +
+        nk(ND.nr) * (int64_t)sizeof(T) * (2 + (first ? 0 : 1) + (beta != T(0) ? 1 : 0)));
+  }
+  void diag_m(int n, const T *d, const T *x, T alpha, T beta, T *out) {
+    begin(MLDG_KERNEL_VEC);
+    kdispatch(K, [&](auto kc) {
+      constexpr int KK = decltype(kc)::value;
+      k_diag_m<T, KK><<<blocks_for(nk(n)), 256, 0, st>>>(n, d, x, alpha, beta, out);
+    });
+    end((int64_t)n * sizeof(T) + nk(n) * (int64_t)sizeof(T) * (2 + (beta != T(0) ? 1 : 0)));
+  }
+  void fill_m(int n, T v, T *y) {
+    begin(MLDG_KERNEL_VEC);
+    k_fill<T><<<blocks_for(nk(n)), 256, 0, st>>>((int)nk(n), v, y);
+    end(nk(n) * (int64_t)sizeof(T));
+  }
+  void axpby_m(int n, const T *x, T beta, T *y) {
+    begin(MLDG_KERNEL_VEC);
+    k_axpby1<T><<<blocks_for(nk(n)), 256, 0, st>>>((int)nk(n), x, beta, y);
+    end(nk(n) * (int64_t)sizeof(T) * (2 + (beta != T(0))));
+  }
+  void trsv_m(DTri<T> &t, const T *rhs, const T *scale, T *cur, T *other, T *out, T alpha, T beta) {
+    TriArgs<T> a;
+    a.n = t.n;
+    a.rev = t.rev;
+    a.nlevels = t.nlevels;
+    a.lvl_ptr = t.lvl_ptr;
+    a.prow = t.prow;
+    a.pirp = t.pirp;
+    a.pja = t.pja;
+    a.pval = t.pval;
+    a.rhs_src = rhs;
+    a.rhs_scale = scale;
+    a.cur = cur;
+    a.other = other;
+    a.out = out;
+    a.alpha = alpha;
+    a.beta = beta;
+    a.counters = t.counters;
+    a.err = err;
+    a.nblk = 0;
+    a.blk = nullptr;
+    const int ki = ilog2(K);
+    begin(MLDG_KERNEL_TRSV);
+    kdispatch(K, [&](auto kc) {
+      constexpr int KK = decltype(kc)::value;
+      k_trsv_sf_m<T, KK><<<t.gridm[ki], 256, 0, st>>>(a, t.nblkm[ki], t.blkm[ki]);
+    });
+    end(t.nnz * (int64_t)(sizeof(T) + 4) + 4 * (2 * (int64_t)t.n + 1) + (scale ? (int64_t)t.n * sizeof(T) : 0) +
+        nk(t.n) * (int64_t)sizeof(T) * (1 + 1 + (other ? 1 : 0) + (out ? 1 + (beta != T(0)) : 0)));
+  }
+  void ilu_apply_m(Lev &L, char trans, const T *x, T beta, T *y) {
+    if (L.minv) {
+      const T *M = (trans == 'N') ? L.minv : L.minvT;
+      begin(MLDG_KERNEL_VEC);
+      kdispatch(K, [&](auto kc) {
+        constexpr int KK = decltype(kc)::value;
+        k_gemm_m<T, KK><<<blocks_for(nk(L.n)), 256, 0, st>>>(L.n, M, x, T(1), beta, y);
+      });
+      end((int64_t)L.n * L.n * sizeof(T) + nk(L.n) * (int64_t)sizeof(T) * (2 + (beta != T(0))));
+      return;
+    }
+    if (trans == 'N') {
+      trsv_m(L.L, x, nullptr, L.bufAm, L.bufBm, nullptr, T(1), T(0));
+      trsv_m(L.U, L.bufAm, L.d, L.bufBm, L.bufAm, y, T(1), beta);
+    } else {
+      trsv_m(L.Ut, x, nullptr, L.bufAm, L.bufBm, nullptr, T(1), T(0));
+      trsv_m(L.Lt, L.bufAm, L.d, L.bufBm, L.bufAm, y, T(1), beta);
+    }
+  }
+  // the single-vector smoother() with K-wide kernels
+  void smoother_m(Lev &L, char trans, const T *x, T beta, T *y, int sweeps) {
+    const DCSR<T> &ND = (trans == 'N') ? L.ND : L.NDT;
+    if (L.kind == MLDG_SMOOTHER_BJAC) {
+      if (sweeps == 1 || L.nnz_nd == 0) {
+        ilu_apply_m(L, trans, x, beta, y);
+        return;
+      }
+      ilu_apply_m(L, trans, x, T(0), L.tym);
+      for (int s = 1; s < sweeps; ++s) {
+        spmm(ND, L.tym, T(-1), x, T(1), L.twm, T(0));
+        ilu_apply_m(L, trans, L.twm, T(0), L.tym);
+      }
+      axpby_m(L.n, L.tym, beta, y);
+      return;
+    }
+    const T w = (T)L.damp;
+    if (sweeps == 1 || L.nnz_nd == 0) {
+      diag_m(L.n, L.d, x, w, beta, y);
+      return;
+    }
+    T *src = nullptr;
+    T *bufs[2] = {L.tym, L.twm};
+    for (int s = 1; s < sweeps; ++s) {
+      const bool last = (s == sweeps - 1);
+      T *dst = last ? y : bufs[s & 1];
+      jacobi_m(ND, L.d, x, src, s == 1 ? 1 : 0, w, T(1), last ? beta : T(0), dst);
+      src = dst;
+    }
+  }
+  void prolong_m(Lev &C, T *y) {
+    if constexpr (std::is_same<T, float>::value) {
+      if (C.Ph) {
+        begin(MLDG_KERNEL_SPMV);
+        kdispatch(K, [&](auto kc) {
+          constexpr int KK = decltype(kc)::value;
+          k_spmm_h<KK><<<blocks_for(nk(C.P.nr)), 256, 0, st>>>(C.P.nr, C.P.irp, C.P.ja, C.Ph, C.Pscale, C.ym, y);
+        });
+        end(C.P.nnz * 6 + 4 * ((int64_t)C.P.nr + 1) + (int64_t)C.P.nr * 4 + nk(C.P.nc) * 4 + nk(C.P.nr) * 4 * 2);
+        return;
+      }
+    }
+    spmm(C.P, C.ym, T(1), nullptr, T(0), y, T(1));
+  }
+  // the single-vector vcycle() with K-wide kernels
+  void vcycle_m(int l, char trans) {
+    cur_lev = l;
+    Lev &L = lv[l];
+    const int nlev = (int)lv.size();
+    const bool pre = (L.spre > 0 && trans == 'N') || (L.spost > 0 && trans != 'N');
+    const bool post = (L.spost > 0 && trans == 'N') || (L.spre > 0 && trans != 'N');
+    if (l < nlev - 1) {
+      Lev &C = lv[l + 1];
+      const DCSR<T> &A = (trans == 'N') ? L.A : L.AT;
+      if (pre) {
+        smoother_m(L, trans, L.xm, T(0), L.ym, trans == 'N' ? L.spre : L.spost);
+        spmm(A, L.ym, T(-1), L.xm, T(1), L.tym, T(0));
+        spmm(C.R, L.tym, T(1), nullptr, T(0), C.xm, T(0));
+      } else {
+        fill_m(L.n, T(0), L.ym);
+        spmm(C.R, L.xm, T(1), nullptr, T(0), C.xm, T(0));
+      }
+      vcycle_m(l + 1, trans);
+      cur_lev = l;
+      prolong_m(C, L.ym);
+      if (post) {
+        spmm(A, L.ym, T(-1), L.xm, T(1), L.tym, T(0));
+        smoother_m(L, trans, L.tym, T(1), L.ym, trans == 'N' ? L.spost : L.spre);
+      }
+    } else {
+      smoother_m(L, trans, L.xm, T(0), L.ym, L.spre);
+    }
+  }
+  void record_multi(char trans, int Kw) override {
+    if (Kw > mcap) fail(MLDG_ERR_INTERNAL, "multi buffers not allocated for %d columns", Kw);
+    launches = 0;
+    bytes = 0;
+    cur_lev = 0;
+    probe_armed = false;
+    std::memset(seen, 0, sizeof seen);
+    K = Kw;
+    Lev &F = lv[0];
+    const int64_t n = nk(F.n);
+    if (!std::is_same<T, double>::value) {
+      begin(MLDG_KERNEL_VEC);
+      k_cast<double, T><<<blocks_for(n), 256, 0, st>>>((int)n, xin_m, F.xm);
+      end(n * (8 + (int64_t)sizeof(T)));
+    }
+    if (lv.size() == 1)
+      smoother_m(F, trans, F.xm, T(0), F.ym, F.spre);
+    else
+      vcycle_m(0, trans);
+    if (!std::is_same<T, double>::value) {
+      cur_lev = 0;
+      begin(MLDG_KERNEL_VEC);
+      k_cast<T, double><<<blocks_for(n), 256, 0, st>>>((int)n, F.ym, yout_m);
+      end(n * (8 + (int64_t)sizeof(T)));
+    }
+  }
+
   void dump_trace() override {
     for (size_t l = 0; l < lv.size(); ++l) {
       if (!lv[l].win) continue;
@@ -599,12 +902,6 @@ struct EngineT : Engine {
     }
   }
 };
-
-template <typename T>
-__global__ void k_axpby1(int n, const T *__restrict__ x, T beta, T *y) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    y[i] = (beta == T(0)) ? x[i] : fma(beta, y[i], x[i]);
-}
 
 template <typename T>
 void EngineT<T>::k_axpby_impl(int n, const T *x, T beta, T *y) {
@@ -669,7 +966,24 @@ struct Handle {
   bool pending = false;  // a probed launch was issued and not yet read
   double probe_ms = 0;
   int64_t probe_count = 0, probe_bytes = 0;
+  // multi-RHS V-cycle graphs per (trans, log2 K) and the K-wide FP64 Krylov state
+  cudaGraphExec_t gexec_m[2][6] = {};
+  int64_t glaunch_m[2][6] = {};
+  bool gprobe_m[2][6] = {};
+  Arena karena;
+  int kcap = 0;
+  double *kb_m = nullptr, *kx_m = nullptr, *kd_m = nullptr, *kq_m = nullptr, *kpart_m = nullptr;
+  KrylovM *ksc_m = nullptr, *hksc_m = nullptr;  // device state, pinned host mirror
 };
+
+static void drop_multi_graphs(Handle *h) {
+  for (int t = 0; t < 2; ++t)
+    for (int q = 0; q < 6; ++q)
+      if (h->gexec_m[t][q]) {
+        cudaGraphExecDestroy(h->gexec_m[t][q]);
+        h->gexec_m[t][q] = nullptr;
+      }
+}
 
 // dispatch over (kernel, lanes per row, prefetched entries per lane)
 template <typename T, int TPR, int E>
@@ -959,6 +1273,7 @@ static DTri<T> build_tri_dev(Arena &ar, const HostCSR &m, bool upper, int nsm) {
   t.n = n;
   t.rev = upper ? 1 : 0;
   t.nlevels = (int)s.lvl_ptr.size() - 1;
+  t.h_lvl = s.lvl_ptr;
   t.nnz = m.nnz();
   t.lvl_ptr = ar.upload(s.lvl_ptr);
   t.prow = ar.upload(s.prow);
@@ -1188,17 +1503,15 @@ static Engine *make_engine(Handle *h) {
         }
       }
     }
-    if (H.kind == MLDG_SMOOTHER_BJAC && !L.win) {
+    // level schedules of the four factors: the single-vector solve where no
+    // window plan was taken, and always the multi-RHS solve (k_trsv_sf_m)
+    if (H.kind == MLDG_SMOOTHER_BJAC) {
       L.L = build_tri_dev<T>(ar, H.L, false, h->nsm);
       L.U = build_tri_dev<T>(ar, H.U, true, h->nsm);
       HostCSR Lt = transpose(H.L), Ut = transpose(H.U);
       L.Ut = build_tri_dev<T>(ar, Ut, false, h->nsm);  // U^T is lower
       L.Lt = build_tri_dev<T>(ar, Lt, true, h->nsm);   // L^T is upper
-      if (L.nnz_nd > 0) {
-        L.ND = to_dev<T>(ar, H.ND);
-        L.NDT = to_dev<T>(ar, transpose(H.ND));
-      }
-      if (std::getenv("MLDG_VERBOSE")) {
+      if (std::getenv("MLDG_VERBOSE") && !L.win) {
         const DTri<T> *ts[4] = {&L.L, &L.U, &L.Ut, &L.Lt};
         const char *nm[4] = {"L", "U", "Ut", "Lt"};
         for (int q = 0; q < 4; ++q)
@@ -1209,11 +1522,10 @@ static Engine *make_engine(Handle *h) {
                        ts[q]->tpr, ts[q]->e, ts[q]->stg.D, ts[q]->stg.capR, ts[q]->stg.capE,
                        ts[q]->smem, ts[q]->grid);
       }
-    } else {
-      if (H.ND.present()) {
-        L.ND = to_dev<T>(ar, H.ND);
-        L.NDT = to_dev<T>(ar, transpose(H.ND));
-      }
+    }
+    if (H.ND.present() && L.nnz_nd > 0) {
+      L.ND = to_dev<T>(ar, H.ND);
+      L.NDT = to_dev<T>(ar, transpose(H.ND));
     }
     if (H.kind == MLDG_SMOOTHER_BJAC && l == h->nlev - 1 && h->nlev > 1 && L.n <= kDenseCoarseRows &&
         !std::getenv("MLDG_NO_DENSE_COARSE")) {
@@ -1299,8 +1611,11 @@ static void finalize(Handle *h, int nlev, int precision) {
       cudaGraphExecDestroy(h->gexec[t]);
       h->gexec[t] = nullptr;
     }
+  drop_multi_graphs(h);
   h->eng.reset();
   h->arena.release();
+  h->karena.release();
+  h->kcap = 0;
   h->nlev = nlev;
   h->precision = precision;
   h->n0 = h->host[0].A.nr;
@@ -1382,6 +1697,93 @@ static int check_device_error(Handle *h) {
   return 0;
 }
 
+static void run_vcycle_multi(Handle *h, char trans, int K) {
+  const int t = (trans == 'N') ? 0 : 1, q = ilog2(K);
+  if (h->opts.use_graphs) {
+    if (!h->gexec_m[t][q]) {
+      cudaGraph_t g;
+      MLDG_CUDA(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+      h->eng->capturing = true;
+      try {
+        h->eng->record_multi(trans, K);
+      } catch (...) {
+        h->eng->capturing = false;
+        cudaStreamEndCapture(h->st, &g);
+        throw;
+      }
+      h->eng->capturing = false;
+      MLDG_CUDA(cudaStreamEndCapture(h->st, &g));
+      MLDG_CUDA(cudaGraphInstantiate(&h->gexec_m[t][q], g, 0));
+      cudaGraphDestroy(g);
+      h->glaunch_m[t][q] = h->eng->launches;
+      h->gprobe_m[t][q] = h->eng->probe_armed;
+      if (h->eng->probe_armed) h->probe_bytes = h->eng->probe_bytes;
+    }
+    MLDG_CUDA(cudaGraphLaunch(h->gexec_m[t][q], h->st));
+    h->last_launches += h->glaunch_m[t][q];
+    h->pending = h->gprobe_m[t][q];
+  } else {
+    h->eng->record_multi(trans, K);
+    h->glaunch_m[t][q] = h->eng->launches;
+    h->last_launches += h->eng->launches;
+    h->pending = h->eng->probe_armed;
+    if (h->eng->probe_armed) h->probe_bytes = h->eng->probe_bytes;
+  }
+}
+
+// columns [c0, c0+k) of a column-major (ld) FP64 block, host or device, into
+// the K-wide interleaved device buffer dst (columns >= k zero)
+static void load_block(Handle *h, const double *src, int ld, int k, int K, int mem, double *dst) {
+  const int n = h->n0;
+  int sld = ld;
+  if (mem == MLDG_MEM_HOST) {
+    MLDG_CUDA(cudaMemcpy2DAsync(h->eng->col_m, sizeof(double) * n, src, sizeof(double) * ld, sizeof(double) * n, k,
+                                cudaMemcpyHostToDevice, h->st));
+    src = h->eng->col_m;
+    sld = n;
+  }
+  const int64_t tot = (int64_t)n * K;
+  const int g = (int)std::max<int64_t>(1, std::min<int64_t>((tot + 255) / 256, (int64_t)h->nsm * 16));
+  k_to_interleaved<double><<<g, 256, 0, h->st>>>(n, k, K, sld, src, dst);
+  h->last_launches++;
+}
+static void store_block(Handle *h, const double *src, int k, int K, int mem, double *dst, int ld) {
+  const int n = h->n0;
+  const int64_t tot = (int64_t)n * k;
+  const int g = (int)std::max<int64_t>(1, std::min<int64_t>((tot + 255) / 256, (int64_t)h->nsm * 16));
+  if (mem == MLDG_MEM_HOST) {
+    k_from_interleaved<double><<<g, 256, 0, h->st>>>(n, k, K, n, src, h->eng->col_m);
+    MLDG_CUDA(cudaMemcpy2DAsync(dst, sizeof(double) * ld, h->eng->col_m, sizeof(double) * n, sizeof(double) * n, k,
+                                cudaMemcpyDeviceToHost, h->st));
+  } else {
+    k_from_interleaved<double><<<g, 256, 0, h->st>>>(n, k, K, ld, src, dst);
+  }
+  h->last_launches++;
+}
+static int width_for(int k) {
+  int K = 2;
+  while (K < k) K *= 2;
+  return K;
+}
+static void prepare_multi(Handle *h, int K) {
+  if (h->eng->ensure_multi(K)) drop_multi_graphs(h);
+}
+
+// nrhs > 1: blocks of up to 32 columns through the K-wide V-cycle
+static void apply_multi(Handle *h, const double *x, double *y, char trans, int nrhs, int ld, int mem) {
+  for (int c0 = 0; c0 < nrhs; c0 += 32) {
+    const int k = std::min(32, nrhs - c0), K = width_for(k);
+    prepare_multi(h, K);
+    load_block(h, x + (size_t)c0 * ld, ld, k, K, mem, h->eng->xin_m);
+    run_vcycle_multi(h, trans, K);
+    store_block(h, h->eng->yout_m, k, K, mem, y + (size_t)c0 * ld, ld);
+    if (h->pending) {
+      MLDG_CUDA(cudaStreamSynchronize(h->st));
+      probe_collect(h);
+    }
+  }
+}
+
 static void apply(Handle *h, const double *x, double *y, char trans, int nrhs, int ld, int mem) {
   if (!h->finalized) fail(MLDG_ERR_NOT_BUILT, "apply before build (mldg_finalize not called)");
   if (trans == 'C') trans = 'T';
@@ -1395,7 +1797,10 @@ static void apply(Handle *h, const double *x, double *y, char trans, int nrhs, i
   const cudaMemcpyKind d2h = mem == MLDG_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
   h->last_launches = 0;
   MLDG_CUDA(cudaEventRecord(h->ev0, h->st));
-  for (int c = 0; c < nrhs; ++c) {
+  const char *em = std::getenv("MLDG_MULTI");
+  const bool multi = nrhs > 1 && !(em && em[0] == '0');
+  if (multi) apply_multi(h, x, y, trans, nrhs, ld, mem);
+  for (int c = 0; c < (multi ? 0 : nrhs); ++c) {
     const size_t off = (size_t)c * (size_t)(nrhs > 1 ? ld : n);
     MLDG_CUDA(cudaMemcpyAsync(h->xin, x + off, sizeof(double) * n, h2d, h->st));
     run_vcycle(h, trans);
@@ -1511,6 +1916,150 @@ static void krylov(Handle *h, int method, const mldg_csr *Acsr, const double *b,
   check_device_error(h);
 }
 
+
+// ---------------------------------------------------------------------------
+// nrhs independent CG/FCG solves sharing the preconditioner, advanced
+// together: one K-wide V-cycle, one SpMM and per-column scalars per
+// iteration.  A converged column is frozen (its x and r stop changing), so
+// each column follows the single-vector krylov() iteration for its own system.
+template <int KK>
+static void dots_m_t(Handle *h, int nq, const double *x0, const double *y0, const double *x1, const double *y1) {
+  k_dots_m<KK><<<kRedBlocksM, 256, 0, h->st>>>(h->n0, nq, x0, y0, x1, y1, h->kpart_m);
+  k_dots_m_final<KK><<<1, 2 * KK, 0, h->st>>>(kRedBlocksM, h->kpart_m, h->ksc_m->dots);
+  h->last_launches += 2;
+}
+static void dots_m(Handle *h, int K, int nq, const double *x0, const double *y0, const double *x1,
+                   const double *y1) {
+  kdispatch(K, [&](auto kc) { dots_m_t<decltype(kc)::value>(h, nq, x0, y0, x1, y1); });
+}
+static void scal_m(Handle *h, int K, int what) {
+  kdispatch(K, [&](auto kc) { k_scal_store_m<decltype(kc)::value><<<1, 32, 0, h->st>>>(h->ksc_m, what); });
+  h->last_launches++;
+}
+static void spmm64(Handle *h, int K, const DCSR<double> &A, const double *v, double a1, const double *b, double a0,
+                   double *out) {
+  const int64_t thr = (int64_t)A.nr * K;
+  const int g = (int)std::max<int64_t>(1, std::min<int64_t>((thr + 255) / 256, (int64_t)h->nsm * 16));
+  kdispatch(K, [&](auto kc) {
+    k_spmm<double, decltype(kc)::value><<<g, 256, 0, h->st>>>(A.nr, A.irp, A.ja, A.val, v, a1, b, a0, out, 0.0);
+  });
+  h->last_launches++;
+}
+static void ensure_krylov_m(Handle *h, int K) {
+  if (!h->hksc_m) MLDG_CUDA(cudaMallocHost(&h->hksc_m, sizeof(KrylovM)));
+  if (K <= h->kcap) return;
+  h->karena.release();
+  const size_t nk = (size_t)std::max(h->n0, 1) * K;
+  h->kb_m = h->karena.alloc<double>(nk);
+  h->kx_m = h->karena.alloc<double>(nk);
+  h->kd_m = h->karena.alloc<double>(nk);
+  h->kq_m = h->karena.alloc<double>(nk);
+  h->kpart_m = h->karena.alloc<double>((size_t)2 * 32 * kRedBlocksM);
+  h->ksc_m = h->karena.alloc<KrylovM>(1);
+  h->kcap = K;
+}
+
+static void krylov_multi(Handle *h, int method, const mldg_csr *Acsr, int nrhs, const double *b, int ldb,
+                         double *x, int ldx, double tol, int itmax, int *iters, double *relres, int mem) {
+  if (!h->finalized) fail(MLDG_ERR_NOT_BUILT, "krylov before build");
+  if (method != 0 && method != 1) fail(MLDG_ERR_ARG, "method must be 0 (CG) or 1 (FCG)");
+  if (nrhs < 0) fail(MLDG_ERR_ARG, "nrhs < 0");
+  if (nrhs > 0 && (!b || !x || !iters || !relres)) fail(MLDG_ERR_ARG, "null argument");
+  if (itmax < 0) fail(MLDG_ERR_ARG, "itmax < 0");
+  if (mem != MLDG_MEM_HOST && mem != MLDG_MEM_DEVICE) fail(MLDG_ERR_ARG, "bad mem_kind");
+  const int n = h->n0;
+  if (ldb < n || ldx < n) fail(MLDG_ERR_SIZE, "ldb %d / ldx %d < n %d", ldb, ldx, n);
+  DCSR<double> A = h->A0;
+  Arena tmp;
+  if (Acsr) {
+    HostCSR ha = copy_csr(*Acsr, h->opts.index_base, "krylov A", 0);
+    if (ha.nr != n || ha.nc != n) fail(MLDG_ERR_SIZE, "krylov A must be %d x %d", n, n);
+    A = to_dev<double>(tmp, ha);
+  }
+  h->last_launches = 0;
+  MLDG_CUDA(cudaEventRecord(h->ev0, h->st));
+  for (int c0 = 0; c0 < nrhs; c0 += 32) {
+    const int k = std::min(32, nrhs - c0), K = width_for(k);
+    prepare_multi(h, K);
+    ensure_krylov_m(h, K);
+    Engine &e = *h->eng;
+    double *r = e.xin_m, *z = e.yout_m, *d = h->kd_m, *q = h->kq_m, *xx = h->kx_m, *bb = h->kb_m;
+    KrylovM *hs = h->hksc_m;
+    load_block(h, b + (size_t)c0 * ldb, ldb, k, K, mem, bb);
+    load_block(h, x + (size_t)c0 * ldx, ldx, k, K, mem, xx);
+    spmm64(h, K, A, xx, -1.0, bb, 1.0, r);  // r = b - A x
+    std::memset(hs, 0, sizeof(KrylovM));
+    hs->tol = tol;
+    hs->ncols = k;
+    MLDG_CUDA(cudaMemcpyAsync(h->ksc_m, hs, sizeof(KrylovM), cudaMemcpyHostToDevice, h->st));
+    dots_m(h, K, 2, bb, bb, r, r);
+    scal_m(h, K, 3);
+    MLDG_CUDA(cudaMemcpyAsync(hs, h->ksc_m, sizeof(KrylovM), cudaMemcpyDeviceToHost, h->st));
+    MLDG_CUDA(cudaStreamSynchronize(h->st));
+    int it = 0;
+    std::vector<int> done(k, 0);
+    for (int c = 0; c < k; ++c)
+      if (!hs->active[c]) {
+        done[c] = 1;
+        iters[c0 + c] = 0;
+      }
+    auto any_active = [&]() {
+      for (int c = 0; c < k; ++c)
+        if (hs->active[c]) return true;
+      return false;
+    };
+    while (any_active() && it < itmax) {
+      ++it;
+      run_vcycle_multi(h, 'N', K);  // z = M^{-1} r, all columns
+      if (method == 1) {
+        if (it > 1) {
+          dots_m(h, K, 1, z, q, nullptr, nullptr);
+          scal_m(h, K, 0);
+        }
+      } else {
+        dots_m(h, K, 1, r, z, nullptr, nullptr);
+        scal_m(h, K, 0);
+      }
+      const int64_t tot = (int64_t)n * K;
+      const int g = (int)std::max<int64_t>(1, std::min<int64_t>((tot + 255) / 256, (int64_t)h->nsm * 16));
+      kdispatch(K, [&](auto kc) {
+        constexpr int KK = decltype(kc)::value;
+        k_dir_update_m<KK><<<g, 256, 0, h->st>>>(n, method, it == 1 ? 1 : 0, z, d, h->ksc_m);
+      });
+      spmm64(h, K, A, d, 1.0, nullptr, 0.0, q);  // q = A d
+      dots_m(h, K, 2, d, q, d, r);
+      scal_m(h, K, 1);
+      kdispatch(K, [&](auto kc) {
+        constexpr int KK = decltype(kc)::value;
+        k_xr_update_m<KK><<<g, 256, 0, h->st>>>(n, method, d, q, xx, r, h->ksc_m);
+      });
+      dots_m(h, K, 1, r, r, nullptr, nullptr);
+      scal_m(h, K, 2);
+      h->last_launches += 2;
+      MLDG_CUDA(cudaMemcpyAsync(hs, h->ksc_m, sizeof(KrylovM), cudaMemcpyDeviceToHost, h->st));
+      MLDG_CUDA(cudaStreamSynchronize(h->st));
+      probe_collect(h);
+      for (int c = 0; c < k; ++c)
+        if (!done[c] && !hs->active[c]) {
+          done[c] = 1;
+          iters[c0 + c] = it;
+        }
+    }
+    for (int c = 0; c < k; ++c) {
+      if (!done[c]) iters[c0 + c] = it;
+      relres[c0 + c] = std::sqrt(std::max(hs->rr[c], 0.0)) / hs->bn[c];
+      if (std::isnan(hs->rr[c])) relres[c0 + c] = hs->rr[c];
+    }
+    store_block(h, xx, k, K, mem, x + (size_t)c0 * ldx, ldx);
+  }
+  MLDG_CUDA(cudaEventRecord(h->ev1, h->st));
+  MLDG_CUDA(cudaStreamSynchronize(h->st));
+  float ms = 0;
+  MLDG_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  h->last_ms = ms;
+  tmp.release();
+  check_device_error(h);
+}
 }  // namespace mldg
 
 // ===========================================================================
@@ -1617,6 +2166,19 @@ extern "C" int mldg_krylov(mldg_handle *hp, int method, const mldg_csr *A, const
     if (iters) *iters = it;
     if (it >= itmax && relres && *relres > tol)
       mldg::fail(MLDG_ERR_NOT_CONVERGED, "not converged in %d iterations (relres %.3e)", it, *relres);
+  });
+}
+
+extern "C" int mldg_krylov_multi(mldg_handle *hp, int method, const mldg_csr *A, int nrhs, const double *b,
+                                 int ldb, double *x, int ldx, double tol, int itmax, int *iters, double *relres,
+                                 int mem_kind) {
+  if (!hp) return MLDG_ERR_ARG;
+  MLDG_GUARD(hp, {
+    mldg::krylov_multi(&hp->h, method, A, nrhs, b, ldb, x, ldx, tol, itmax, iters, relres, mem_kind);
+    for (int c = 0; c < nrhs; ++c)
+      if (iters[c] >= itmax && !(relres[c] <= tol))
+        mldg::fail(MLDG_ERR_NOT_CONVERGED, "column %d not converged in %d iterations (relres %.3e)", c, iters[c],
+                   relres[c]);
   });
 }
 
@@ -1865,9 +2427,12 @@ extern "C" void mldg_destroy(mldg_handle *hp) {
   if (h.eng && std::getenv("MLDG_WIN_TRACE")) h.eng->dump_trace();
   for (int t = 0; t < 2; ++t)
     if (h.gexec[t]) cudaGraphExecDestroy(h.gexec[t]);
+  mldg::drop_multi_graphs(&h);
   h.eng.reset();
   h.arena.release();
+  h.karena.release();
   if (h.hpin) cudaFreeHost(h.hpin);
+  if (h.hksc_m) cudaFreeHost(h.hksc_m);
   if (h.ev0) cudaEventDestroy(h.ev0);
   if (h.ev1) cudaEventDestroy(h.ev1);
   if (h.pev0) cudaEventDestroy(h.pev0);
