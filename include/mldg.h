@@ -207,6 +207,10 @@ int mldg_probe_read(mldg_handle *h, double *total_ms, int64_t *count, int64_t *b
 /* Runs one V-cycle (trans 'N'/'T') on the current level-0 input without a
  * graph, with CUDA events around every launch; writes up to max entries. */
 int mldg_profile(mldg_handle *h, char trans, int max, mldg_kernel_stat *stats, int *n);
+/* The same for the multi-vector V-cycle of mldg_apply with nrhs (2..32)
+ * columns (nrhs = 1 is mldg_profile). */
+int mldg_profile_multi(mldg_handle *h, char trans, int nrhs, int max, mldg_kernel_stat *stats,
+                       int *n);
 
 /* ---- allocation-free relative residual --------------------------------- */
 /* No counterpart in the reference.  For callers that must not allocate

@@ -83,11 +83,11 @@ class _GpuDiag:
         lib().mldg_probe_read(self._gpu(), C.byref(ms), C.byref(cnt), C.byref(b))
         return ms.value, cnt.value, b.value
 
-    def profile(self, trans: str = "N"):
-        """One un-graphed V-cycle with events around every launch."""
+    def profile(self, trans: str = "N", nrhs: int = 1):
+        """One un-graphed V-cycle (nrhs columns) with events around every launch."""
         stats = (_KStat * 4096)()
         n = C.c_int(0)
-        rc = lib().mldg_profile(self._gpu(), trans.encode(), 4096, stats, C.byref(n))
+        rc = lib().mldg_profile_multi(self._gpu(), trans.encode(), nrhs, 4096, stats, C.byref(n))
         if rc:
             raise MldError(rc, "profile")
         return [{"kind": KERNEL_NAMES.get(s.kind, "?"), "kind_id": s.kind, "level": s.level,
@@ -184,6 +184,8 @@ def lib():
                                       C.POINTER(C.c_int64)]
         L.mldg_profile.argtypes = [vp, C.c_char, C.c_int, C.POINTER(_KStat),
                                    C.POINTER(C.c_int)]
+        L.mldg_profile_multi.argtypes = [vp, C.c_char, C.c_int, C.c_int, C.POINTER(_KStat),
+                                         C.POINTER(C.c_int)]
         L.mldg_relres_noalloc.argtypes = [vp, C.POINTER(_CSR), C.c_void_p, C.c_void_p,
                                           C.POINTER(C.c_double)]
         L.mldg_adjoint.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_double, C.c_int,

@@ -166,10 +166,19 @@ struct DTri {
   bool cta = true;  // single-CTA kernel (solution in shared memory) vs sync-free
   int threads = 512, grid = 1;
   size_t smem = 0;
-  std::vector<int> h_lvl;  // level pointers (host copy)
+  // host copy of the level schedule (transformed index space)
+  std::vector<int> h_lvl, h_prow, h_pirp, h_pja;
+  std::vector<double> h_pval;
   // multi-RHS sync-free solve (k_trsv_sf_m): level-aligned blocks of 32/K rows, per log2(K)
   int2 *blkm[6] = {};
   int nblkm[6] = {}, gridm[6] = {};
+  // its ELL form (k_trsv_ell), per log2(K); ok = false falls back to k_trsv_sf_m
+  struct Ell {
+    bool ok = false;
+    int ntask = 0, npad = 0, E = 0, S = 1, grid = 0, backoff = 0;
+    int *prow = nullptr, *ej = nullptr, *ovp = nullptr, *ovj = nullptr, *ctr = nullptr;
+    T *ev = nullptr, *ovv = nullptr;
+  } ell[6];
   bool present() const { return prow != nullptr; }
 };
 
@@ -227,6 +236,14 @@ static void kdispatch(int K, F &&f) {
     case 32: f(std::integral_constant<int, 32>()); break;
     default: fail(MLDG_ERR_INTERNAL, "bad multi-vector width %d", K);
   }
+}
+// the ELL triangular solve also serves the single-vector V-cycle (K = 1)
+template <typename F>
+static void kdispatch_ell(int K, F &&f) {
+  if (K == 1)
+    f(std::integral_constant<int, 1>());
+  else
+    kdispatch(K, f);
 }
 static int ilog2(int K) {
   int r = 0;
@@ -325,6 +342,8 @@ struct EngineT : Engine {
     T *xm = nullptr, *ym = nullptr, *tym = nullptr, *twm = nullptr, *bufAm = nullptr, *bufBm = nullptr;
     // windowed cluster solves (k_trsv_win) for both factors of each pair
     bool win = false;
+    // single-vector solves through the ELL kernel (k_trsv_ell, K = 1) instead
+    bool ell1 = false;
     DWin<T> wL, wU, wUt, wLt;
     // coarsest level: explicit inverse of its ILU(0) factorisation (and its transpose)
     T *minv = nullptr, *minvT = nullptr;
@@ -413,6 +432,44 @@ struct EngineT : Engine {
             (1 + (scale ? 1 : 0) + 1 + (other ? 1 : 0) + (out ? 1 + (beta != T(0)) : 0)));
   }
 
+  void trsv_ell1(const DTri<T> &t, const T *rhs, const T *scale, T *cur, T *other, T *out, T alpha, T beta) {
+    begin(MLDG_KERNEL_TRSV);
+    launch_ell(t.ell[0], 1, rhs, scale, cur, other, out, alpha, beta);
+    end(t.nnz * (int64_t)(sizeof(T) + 4) + 4 * (2 * (int64_t)t.n + 1) +
+        (int64_t)t.n * sizeof(T) *
+            (1 + (scale ? 1 : 0) + 1 + (other ? 1 : 0) + (out ? 1 + (beta != T(0)) : 0)));
+  }
+  // Per level: time the ILU pair on the single-vector ELL solve against the
+  // level's other solve (sync-free blocks or windowed) and keep the faster.
+  void autotune_ilu(int reps) {
+    cudaEvent_t e0, e1;
+    MLDG_CUDA(cudaEventCreate(&e0));
+    MLDG_CUDA(cudaEventCreate(&e1));
+    for (auto &L : lv) {
+      if (L.kind != MLDG_SMOOTHER_BJAC || L.minv || !L.L.ell[0].ok || !L.U.ell[0].ok || !L.Ut.ell[0].ok ||
+          !L.Lt.ell[0].ok)
+        continue;
+      float best[2] = {1e30f, 1e30f};
+      for (int v = 0; v < 2; ++v) {
+        L.ell1 = v == 1;
+        ilu_apply(L, 'N', L.x, T(0), L.ty);  // warm
+        MLDG_CUDA(cudaEventRecord(e0, st));
+        for (int r = 0; r < reps; ++r) ilu_apply(L, 'N', L.x, T(0), L.ty);
+        MLDG_CUDA(cudaEventRecord(e1, st));
+        MLDG_CUDA(cudaEventSynchronize(e1));
+        MLDG_CUDA(cudaEventElapsedTime(&best[v], e0, e1));
+      }
+      L.ell1 = best[1] < best[0];
+      if (std::getenv("MLDG_VERBOSE"))
+        std::fprintf(stderr, "mldg: ilu autotune n=%d other %.3f ms ell %.3f ms -> %s\n", L.n, best[0] / reps,
+                     best[1] / reps, L.ell1 ? "ell" : "other");
+    }
+    launches = 0;
+    bytes = 0;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+
   void gather(const DWin<T> &w, const T *src, T *dst) {
     begin(MLDG_KERNEL_VEC);
     k_gather<T><<<blocks_for(w.n), 256, 0, st>>>(w.n, w.orig, src, (const T *)nullptr, dst);
@@ -465,6 +522,16 @@ struct EngineT : Engine {
       begin(MLDG_KERNEL_VEC);
       k_gemv<T><<<blocks_for((int64_t)L.n * 32), 256, 0, st>>>(L.n, M, x, T(1), beta, y);
       end((int64_t)L.n * L.n * sizeof(T) + (int64_t)L.n * sizeof(T) * (2 + (beta != T(0))));
+      return;
+    }
+    if (L.ell1) {
+      if (trans == 'N') {
+        trsv_ell1(L.L, x, nullptr, L.bufA, L.bufB, nullptr, T(1), T(0));
+        trsv_ell1(L.U, L.bufA, L.d, L.bufB, L.bufA, y, T(1), beta);
+      } else {
+        trsv_ell1(L.Ut, x, nullptr, L.bufA, L.bufB, nullptr, T(1), T(0));
+        trsv_ell1(L.Lt, L.bufA, L.d, L.bufB, L.bufA, y, T(1), beta);
+      }
       return;
     }
     if (L.win) {
@@ -616,6 +683,101 @@ struct EngineT : Engine {
     const int warps = std::max(32, std::min(4 * per_level, nsm * 32));
     t.gridm[ki] = (warps + 7) / 8;
   }
+  template <int KK, int EE, bool PF>
+  static int ell_occupancy() {
+    int nb = 0;
+    MLDG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_trsv_ell<T, KK, EE, PF>, 256, 0));
+    return nb;
+  }
+  void build_ell(DTri<T> &t, int Kw, Arena &ar) {
+    const int ki = ilog2(Kw), rpw = 32 / Kw;
+    auto &el = t.ell[ki];
+    el = typename DTri<T>::Ell();
+    if (std::getenv("MLDG_NO_ELL")) return;
+    const int nl = (int)t.h_lvl.size() - 1;
+    int64_t npad = 0;
+    for (int L = 0; L < nl; ++L) {
+      const int cnt = t.h_lvl[L + 1] - t.h_lvl[L];
+      npad += (cnt + rpw - 1) / rpw * rpw;
+    }
+    if (npad * 16 >= (int64_t)INT32_MAX) return;
+    // level of every row (transformed index space) to order entries by dependency level
+    std::vector<int> lev_of((size_t)t.n, 0);
+    int emax = 0;
+    for (int L = 0; L < nl; ++L)
+      for (int p = t.h_lvl[L]; p < t.h_lvl[L + 1]; ++p) lev_of[t.h_prow[p]] = L;
+    for (int p = 0; p < t.n; ++p) emax = std::max(emax, t.h_pirp[p + 1] - t.h_pirp[p]);
+    const int E = emax <= 4 ? 4 : (emax <= 8 ? 8 : 16);
+    std::vector<int> prow((size_t)npad, -1), ej((size_t)npad * E, -1), ovp((size_t)npad + 1, 0), ovj;
+    std::vector<T> ev((size_t)npad * E, T(0)), ovv;
+    std::vector<int> ord;
+    int64_t pp = 0;
+    for (int L = 0; L < nl; ++L) {
+      for (int p = t.h_lvl[L]; p < t.h_lvl[L + 1]; ++p, ++pp) {
+        const int i = t.h_prow[p];
+        prow[pp] = t.rev ? t.n - 1 - i : i;
+        const int k0 = t.h_pirp[p], len = t.h_pirp[p + 1] - k0;
+        ord.resize(len);
+        for (int e = 0; e < len; ++e) ord[e] = k0 + e;
+        std::stable_sort(ord.begin(), ord.end(),
+                         [&](int x, int y) { return lev_of[t.h_pja[x]] < lev_of[t.h_pja[y]]; });
+        const int nov = std::max(0, len - E);
+        for (int e = 0; e < len; ++e) {
+          const int k = ord[e], jj = t.h_pja[k];
+          const int oj = t.rev ? t.n - 1 - jj : jj;
+          if (e < nov) {
+            ovj.push_back(oj);
+            ovv.push_back((T)t.h_pval[k]);
+          } else {
+            ej[(size_t)(e - nov) * npad + pp] = oj;
+            ev[(size_t)(e - nov) * npad + pp] = (T)t.h_pval[k];
+          }
+        }
+        ovp[pp + 1] = (int)ovj.size();
+      }
+      while (pp % rpw) {
+        ovp[pp + 1] = ovp[pp];
+        ++pp;
+      }
+    }
+    el.npad = (int)npad;
+    el.ntask = (int)(npad / rpw);
+    el.E = E;
+    el.S = Kw >= 16 ? 16 : 1;
+    if (const char *e = std::getenv("MLDG_ELL_BACKOFF")) el.backoff = std::max(0, std::atoi(e));
+    if (const char *e = std::getenv("MLDG_ELL_S")) el.S = std::max(1, std::min(64, std::atoi(e)));
+    int nb = 0;
+    kdispatch_ell(Kw, [&](auto kc) {
+      constexpr int KK = decltype(kc)::value;
+      switch (E) {
+        case 4: nb = ell_occupancy<KK, 4, true>(); break;
+        case 8: nb = ell_occupancy<KK, 8, true>(); break;
+        default: nb = ell_occupancy<KK, 16, false>(); break;
+      }
+    });
+    if (std::getenv("MLDG_VERBOSE"))
+      std::fprintf(stderr, "mldg: ell K=%d n=%d rev=%d levels=%d npad=%lld max row entries %d E=%d overflow %zu S=%d occ %d\n",
+                   Kw, t.n, t.rev, nl, (long long)npad, emax, E, ovj.size(), el.S, nb);
+    if (nb < 1) return;
+    // every ticket stream needs running warps: grid <= co-resident capacity
+    const int per_level = (el.ntask + nl - 1) / std::max(nl, 1);
+    int mult = 4;
+    if (const char *e = std::getenv("MLDG_ELL_MULT")) mult = std::max(1, std::atoi(e));
+    const int64_t warps = std::max<int64_t>(32, std::min<int64_t>((int64_t)mult * per_level, el.ntask));
+    el.grid = (int)std::min<int64_t>((warps + 7) / 8, (int64_t)nb * nsm);
+    el.grid = std::max(el.grid, (el.S + 7) / 8);
+    el.prow = ar.upload(prow);
+    el.ej = ar.upload(ej);
+    el.ev = ar.upload(ev);
+    if (!ovj.empty()) {
+      el.ovp = ar.upload(ovp);
+      el.ovj = ar.upload(ovj);
+      el.ovv = ar.upload(ovv);
+    }
+    el.ctr = ar.alloc<int>((size_t)32 * (el.S + 1));
+    MLDG_CUDA(cudaMemsetAsync(el.ctr, 0, sizeof(int) * 32 * (el.S + 1), st));
+    el.ok = true;
+  }
   bool ensure_multi(int Kw) override {
     bool grown = false;
     if (Kw > mcap) {
@@ -623,9 +785,10 @@ struct EngineT : Engine {
       for (auto &L : lv) {
         L.xm = L.ym = L.tym = L.twm = L.bufAm = L.bufBm = nullptr;
         for (DTri<T> *t : {&L.L, &L.U, &L.Ut, &L.Lt})
-          for (int q = 0; q < 6; ++q) {
+          for (int q = 1; q < 6; ++q) {  // [0] (one column) lives in the main arena
             t->blkm[q] = nullptr;
             t->nblkm[q] = t->gridm[q] = 0;
+            t->ell[q] = typename DTri<T>::Ell();
           }
       }
       mcap = Kw;
@@ -664,7 +827,10 @@ struct EngineT : Engine {
       if (L.kind != MLDG_SMOOTHER_BJAC || L.minv) continue;
       for (DTri<T> *t : {&L.L, &L.U, &L.Ut, &L.Lt}) {
         if (!t->present()) fail(MLDG_ERR_INTERNAL, "multi-RHS solve without a level schedule");
-        if (!t->blkm[ki]) build_blk_m(*t, Kw);
+        if (!t->blkm[ki]) {
+          build_blk_m(*t, Kw);
+          build_ell(*t, Kw, marena);
+        }
       }
     }
     MLDG_CUDA(cudaStreamSynchronize(st));
@@ -733,12 +899,50 @@ struct EngineT : Engine {
     a.blk = nullptr;
     const int ki = ilog2(K);
     begin(MLDG_KERNEL_TRSV);
-    kdispatch(K, [&](auto kc) {
-      constexpr int KK = decltype(kc)::value;
-      k_trsv_sf_m<T, KK><<<t.gridm[ki], 256, 0, st>>>(a, t.nblkm[ki], t.blkm[ki]);
-    });
+    const auto &el = t.ell[ki];
+    if (el.ok) {
+      launch_ell(el, K, rhs, scale, cur, other, out, alpha, beta);
+    } else {
+      kdispatch(K, [&](auto kc) {
+        constexpr int KK = decltype(kc)::value;
+        k_trsv_sf_m<T, KK><<<t.gridm[ki], 256, 0, st>>>(a, t.nblkm[ki], t.blkm[ki]);
+      });
+    }
     end(t.nnz * (int64_t)(sizeof(T) + 4) + 4 * (2 * (int64_t)t.n + 1) + (scale ? (int64_t)t.n * sizeof(T) : 0) +
         nk(t.n) * (int64_t)sizeof(T) * (1 + 1 + (other ? 1 : 0) + (out ? 1 + (beta != T(0)) : 0)));
+  }
+  void launch_ell(const typename DTri<T>::Ell &el, int Kw, const T *rhs, const T *scale, T *cur, T *other, T *out,
+                  T alpha, T beta) {
+    {
+      EllArgs<T> e;
+      e.ntask = el.ntask;
+      e.npad = el.npad;
+      e.S = el.S;
+      e.backoff = el.backoff;
+      e.prow = el.prow;
+      e.ej = el.ej;
+      e.ev = el.ev;
+      e.ovp = el.ovp;
+      e.ovj = el.ovj;
+      e.ovv = el.ovv;
+      e.ctr = el.ctr;
+      e.rhs_src = rhs;
+      e.rhs_scale = scale;
+      e.cur = cur;
+      e.other = other;
+      e.out = out;
+      e.alpha = alpha;
+      e.beta = beta;
+      e.err = err;
+      kdispatch_ell(Kw, [&](auto kc) {
+        constexpr int KK = decltype(kc)::value;
+        switch (el.E) {
+          case 4: k_trsv_ell<T, KK, 4, true><<<el.grid, 256, 0, st>>>(e); break;
+          case 8: k_trsv_ell<T, KK, 8, true><<<el.grid, 256, 0, st>>>(e); break;
+          default: k_trsv_ell<T, KK, 16, false><<<el.grid, 256, 0, st>>>(e); break;
+        }
+      });
+    }
   }
   void ilu_apply_m(Lev &L, char trans, const T *x, T beta, T *y) {
     if (L.minv) {
@@ -1274,6 +1478,10 @@ static DTri<T> build_tri_dev(Arena &ar, const HostCSR &m, bool upper, int nsm) {
   t.rev = upper ? 1 : 0;
   t.nlevels = (int)s.lvl_ptr.size() - 1;
   t.h_lvl = s.lvl_ptr;
+  t.h_prow = s.prow;
+  t.h_pirp = s.pirp;
+  t.h_pja = s.pja;
+  t.h_pval = s.pval;
   t.nnz = m.nnz();
   t.lvl_ptr = ar.upload(s.lvl_ptr);
   t.prow = ar.upload(s.prow);
@@ -1555,6 +1763,15 @@ static Engine *make_engine(Handle *h) {
       L.bufB = ar.alloc<T>(n);
       k_fill<T><<<64, 256, 0, h->st>>>(n, Sentinel<T>::value(), L.bufA);
       k_fill<T><<<64, 256, 0, h->st>>>(n, Sentinel<T>::value(), L.bufB);
+      if (!L.minv) {
+        bool ok = true;
+        for (DTri<T> *f : {&L.L, &L.U, &L.Ut, &L.Lt}) {
+          e->build_ell(*f, 1, ar);
+          ok = ok && f->ell[0].ok;
+        }
+        const char *ev = std::getenv("MLDG_ELL1");
+        L.ell1 = ok && !(ev && ev[0] == '0');
+      }
     }
   }
   MLDG_CUDA(cudaStreamSynchronize(h->st));
@@ -1566,6 +1783,7 @@ static Engine *make_engine(Handle *h) {
     e->tune_buf[1] = ar.alloc<T>(nmax);
     k_fill<T><<<64, 256, 0, h->st>>>(nmax, T(1), e->tune_buf[0]);
     e->autotune_spmv(5);
+    if (!std::getenv("MLDG_ELL1")) e->autotune_ilu(3);
     MLDG_CUDA(cudaStreamSynchronize(h->st));
   }
   return e;
@@ -2290,44 +2508,57 @@ extern "C" int mldg_probe_read(mldg_handle *hp, double *total_ms, int64_t *count
   return MLDG_SUCCESS;
 }
 
-extern "C" int mldg_profile(mldg_handle *hp, char trans, int max, mldg_kernel_stat *stats, int *n) {
-  if (!hp) return MLDG_ERR_ARG;
-  MLDG_GUARD(hp, {
-    Handle &h = hp->h;
-    if (!h.finalized) mldg::fail(MLDG_ERR_NOT_BUILT, "profile before build");
-    if (trans == 'C') trans = 'T';
-    if (trans != 'N' && trans != 'T') mldg::fail(MLDG_ERR_TRANS, "invalid trans");
-    std::vector<mldg::Engine::Prof> prof;
-    h.eng->prof = &prof;
-    const int pk = h.eng->probe_kind;
-    h.eng->probe_kind = 0;
-    try {
+static void profile_run(Handle &h, char trans, int nrhs, int max, mldg_kernel_stat *stats, int *n) {
+  if (!h.finalized) mldg::fail(MLDG_ERR_NOT_BUILT, "profile before build");
+  if (trans == 'C') trans = 'T';
+  if (trans != 'N' && trans != 'T') mldg::fail(MLDG_ERR_TRANS, "invalid trans");
+  if (nrhs < 1 || nrhs > 32) mldg::fail(MLDG_ERR_ARG, "profile width must be 1..32");
+  const int K = nrhs > 1 ? mldg::width_for(nrhs) : 1;
+  if (K > 1) mldg::prepare_multi(&h, K);
+  std::vector<mldg::Engine::Prof> prof;
+  h.eng->prof = &prof;
+  const int pk = h.eng->probe_kind;
+  h.eng->probe_kind = 0;
+  try {
+    if (K > 1)
+      h.eng->record_multi(trans, K);
+    else
       h.eng->record(trans);
-    } catch (...) {
-      h.eng->prof = nullptr;
-      h.eng->probe_kind = pk;
-      throw;
-    }
+  } catch (...) {
     h.eng->prof = nullptr;
     h.eng->probe_kind = pk;
-    MLDG_CUDA(cudaStreamSynchronize(h.st));
-    int k = 0;
-    for (auto &e : prof) {
-      float ms = 0;
-      cudaEventElapsedTime(&ms, e.e0, e.e1);
-      if (k < max && stats) {
-        stats[k].kind = e.kind;
-        stats[k].level = e.lev;
-        stats[k].bytes = e.bytes;
-        stats[k].ms = ms;
-      }
-      ++k;
-      cudaEventDestroy(e.e0);
-      cudaEventDestroy(e.e1);
+    throw;
+  }
+  h.eng->prof = nullptr;
+  h.eng->probe_kind = pk;
+  MLDG_CUDA(cudaStreamSynchronize(h.st));
+  int k = 0;
+  for (auto &e : prof) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e.e0, e.e1);
+    if (k < max && stats) {
+      stats[k].kind = e.kind;
+      stats[k].level = e.lev;
+      stats[k].bytes = e.bytes;
+      stats[k].ms = ms;
     }
-    if (n) *n = k;
-    mldg::check_device_error(&h);
-  });
+    ++k;
+    cudaEventDestroy(e.e0);
+    cudaEventDestroy(e.e1);
+  }
+  if (n) *n = k;
+  mldg::check_device_error(&h);
+}
+
+extern "C" int mldg_profile_multi(mldg_handle *hp, char trans, int nrhs, int max, mldg_kernel_stat *stats,
+                                  int *n) {
+  if (!hp) return MLDG_ERR_ARG;
+  MLDG_GUARD(hp, { profile_run(hp->h, trans, nrhs, max, stats, n); });
+}
+
+extern "C" int mldg_profile(mldg_handle *hp, char trans, int max, mldg_kernel_stat *stats, int *n) {
+  if (!hp) return MLDG_ERR_ARG;
+  MLDG_GUARD(hp, { profile_run(hp->h, trans, 1, max, stats, n); });
 }
 
 // ---------------------------------------------------------------------------

@@ -191,6 +191,174 @@ __global__ void __launch_bounds__(256) k_trsv_sf_m(TriArgs<T> a, int nblk_m, con
   }
 }
 
+// ---------------------------------------------------------------------------
+// ELL form of the multi-RHS sync-free solve.  The level-ordered rows are laid
+// out in padded positions: every level starts at a multiple of RPW = 32/K, so
+// the RPW rows of a warp task never straddle a level (no lane waits on its own
+// warp).  Per padded position pp: the original row prow[pp] (-1 = padding) and
+// E entry slots ej/ev[e*npad + pp] with the original index of the dependency
+// row (-1 = empty) and the factor value.  A row's entries are ordered by the
+// level of their dependency; rows longer than E keep their E most recent
+// dependencies in the slots and the older ones in an overflow list
+// (ovp/ovj/ovv), accumulated first.  All slot loads of a row are in flight at
+// once, so a row costs one round trip once its last dependency is written.
+//
+// Tasks are claimed from S ticket streams (task k*S + s is ticket k of stream
+// s, each stream a counter on its own 128-byte line), so that S atomics
+// proceed in parallel.  A warp claims one ticket ahead and, for E <= 8 (PF),
+// loads the next task's metadata while its current task waits.  Within a
+// stream tickets are claimed in order and a warp finishes its current task
+// before starting the next, so the lowest unfinished task is always being
+// processed and only depends on finished tasks: every wait ends (each is
+// bounded anyway).  The grid never exceeds the co-resident capacity, so every
+// stream keeps running warps.
+template <typename T>
+struct EllArgs {
+  int ntask, npad, S;
+  int backoff;  // ns slept between polls after the first few (0: poll back to back)
+  const int *prow;
+  const int *ej;
+  const T *ev;
+  const int *ovp;  // npad + 1 overflow offsets, or null
+  const int *ovj;
+  const T *ovv;
+  const T *rhs_src;
+  const T *rhs_scale;
+  T *cur;
+  T *other;
+  T *out;
+  T alpha, beta;
+  int *ctr;  // S ticket counters (stride 32 ints), then the finished-warp count
+  int *err;
+};
+
+template <typename T, int E>
+struct EllMeta {
+  int o, q0, q1;
+  int j[E];
+  T v[E];
+};
+
+template <typename T, int E>
+__device__ __forceinline__ void ell_meta(const EllArgs<T> &a, int pp, EllMeta<T, E> &m) {
+  m.o = a.prow[pp];
+  m.q0 = m.q1 = 0;
+  if (a.ovp) {
+    m.q0 = a.ovp[pp];
+    m.q1 = a.ovp[pp + 1];
+  }
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    m.j[e] = a.ej[(size_t)e * a.npad + pp];
+    m.v[e] = a.ev[(size_t)e * a.npad + pp];
+  }
+}
+
+// wait until none of raw[0..N) holds the sentinel (bounded); returns false on failure
+template <typename T, int N, int K>
+__device__ __forceinline__ bool ell_wait(typename Bits<T>::U (&raw)[N], const int (&j)[N], const T *cur, int c,
+                                         int *err, int backoff) {
+  typedef typename Bits<T>::U U;
+  const U sent = (U)Sentinel<T>::bits;
+  for (int it = 0;; ++it) {
+    bool missing = false;
+#pragma unroll
+    for (int e = 0; e < N; ++e) missing |= (raw[e] == sent);
+    if (!missing) return true;
+    if (it >= kSpinLimit) {
+      atomicExch(err, kErrTimeout);
+      return false;
+    }
+    if ((it % kSpinCheck) == kSpinCheck - 1) {
+      if (ld_relaxed_u32(err) != 0u) return false;
+      __nanosleep(32);
+    } else if (backoff && it >= 2) {
+      __nanosleep(backoff);
+    }
+#pragma unroll
+    for (int e = 0; e < N; ++e)
+      if (raw[e] == sent) raw[e] = Bits<T>::load(cur + (size_t)j[e] * K + c);
+  }
+}
+
+template <typename T, int K, int E, bool PF>
+__global__ void __launch_bounds__(256) k_trsv_ell(EllArgs<T> a) {
+  constexpr int RPW = 32 / K;
+  typedef typename Bits<T>::U U;
+  const U sent = (U)Sentinel<T>::bits;
+  const int lane = threadIdx.x & 31;
+  const int c = lane % K;
+  const int grp = lane / K;
+  const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int s = warp % a.S;
+  int *ctr = a.ctr + 32 * s;
+  int pend = 0;
+  if (lane == 0) pend = atomicAdd(ctr, 1);
+  int t = __shfl_sync(0xffffffffu, pend, 0) * a.S + s;
+  if (lane == 0) pend = atomicAdd(ctr, 1);
+  int tn = __shfl_sync(0xffffffffu, pend, 0) * a.S + s;
+  if (lane == 0) pend = atomicAdd(ctr, 1);
+  EllMeta<T, E> m, mn;
+  if (t < a.ntask) ell_meta<T, E>(a, t * RPW + grp, m);
+  while (t < a.ntask) {
+    if (PF && tn < a.ntask) ell_meta<T, E>(a, tn * RPW + grp, mn);
+    if (m.o >= 0) {
+      const size_t oc = (size_t)m.o * K + c;
+      T rhs = a.rhs_src[oc];
+      if (a.rhs_scale) rhs = rhs * a.rhs_scale[m.o];
+      T acc = T(0);
+      // older dependencies beyond the E slots, four loads in flight at a time
+      for (int q = m.q0; q < m.q1; q += 4) {
+        U raw[4];
+        int jj[4];
+        T vv[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const bool has = q + e < m.q1;
+          jj[e] = has ? a.ovj[q + e] : 0;
+          vv[e] = has ? a.ovv[q + e] : T(0);
+          raw[e] = has ? Bits<T>::load(a.cur + (size_t)jj[e] * K + c) : (U)0;
+        }
+        ell_wait<T, 4, K>(raw, jj, a.cur, c, a.err, a.backoff);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc = fma(vv[e], Bits<T>::from(raw[e] == sent ? (U)0 : raw[e]), acc);
+      }
+      U raw[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) raw[e] = m.j[e] >= 0 ? Bits<T>::load(a.cur + (size_t)m.j[e] * K + c) : (U)0;
+      ell_wait<T, E, K>(raw, m.j, a.cur, c, a.err, a.backoff);
+#pragma unroll
+      for (int e = 0; e < E; ++e) acc = fma(m.v[e], Bits<T>::from(raw[e] == sent ? (U)0 : raw[e]), acc);
+      const T r = Bits<T>::canon(rhs - acc);
+      Bits<T>::store(a.cur + oc, r);
+      if (a.other) a.other[oc] = Sentinel<T>::value();
+      if (a.out) {
+        T w = a.alpha * r;
+        if (a.beta != T(0)) w = fma(a.beta, a.out[oc], w);
+        a.out[oc] = w;
+      }
+    }
+    t = tn;
+    tn = __shfl_sync(0xffffffffu, pend, 0) * a.S + s;
+    if (lane == 0) pend = atomicAdd(ctr, 1);
+    if (PF) {
+      m = mn;
+    } else if (t < a.ntask) {
+      ell_meta<T, E>(a, t * RPW + grp, m);
+    }
+  }
+  // the last warp to leave resets the ticket streams for the next launch
+  if (lane == 0) {
+    const int nw = (int)((gridDim.x * blockDim.x) >> 5);
+    __threadfence();
+    const int done = atomicAdd(a.ctr + 32 * a.S, 1);
+    if (done == nw - 1) {
+      for (int q = 0; q < a.S; ++q) a.ctr[32 * q] = 0;
+      a.ctr[32 * a.S] = 0;
+    }
+  }
+}
+
 // column-major (ld) <-> row-interleaved (K) FP64 boundary conversions, with
 // precision change; columns >= k are zero
 template <typename T>
