@@ -29,6 +29,9 @@ import time
 
 import numpy as np
 
+# independent systems run on their own streams: give them separate hardware queues
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 METRIC = "time-to-1e-10 residual (mixed vs FP64 GPU V-cycle); V-cycle apply HBM GB/s"
 S3 = 1.0 / np.sqrt(3.0)
@@ -268,6 +271,93 @@ def time_variant(mld, a, b, smoother, precision, args, dev, torch, probe=False, 
     return res
 
 
+def time_systems(mld, args, dev, torch, nsys=64, lo=24, hi=96):
+    """Batching form (b): nsys independent systems, idim uniform in lo..hi
+    (seed 1), each with its own hierarchy (FP32 V-cycle, FP64 FCG), solved
+    together (mldg_krylov_batch) against solving them one after the other."""
+    dims = np.random.default_rng(1).integers(lo, hi + 1, nsys)
+    precs, bs, mats, rows = [], [], [], 0
+    for idim in dims:
+        a = mld.gen_pde3d(int(idim), 1, ISO)
+        mats.append(a)
+        precs.append(make_prec(mld, a, "BJAC", "FP32", device=dev))
+        bs.append(torch.tensor(a.matvec(np.ones(a.nrows)), dtype=torch.float64, device=f"cuda:{dev}"))
+        rows += a.nrows
+    xs = [torch.zeros_like(b) for b in bs]
+    mld.krylov_batch("FCG", precs, bs, xs, eps=args.eps, itmax=500)  # warm: captures the graphs
+    reps = max(1, min(args.steps, 3))
+    ms = []
+    for _ in range(reps):
+        for x in xs:
+            x.zero_()
+        _, its, rel, t = mld.krylov_batch("FCG", precs, bs, xs, eps=args.eps, itmax=500)
+        ms.append(t)
+    err = max(float(torch.max(torch.abs(x - 1.0))) for x in xs)
+    seq = 0.0
+    its1 = []
+    for a, p, b, x in zip(mats, precs, bs, xs):
+        x.zero_()
+        _, it, _ = mld.krylov("FCG", a, p, b, x, eps=args.eps, itmax=500, use_prec_matrix=True)
+        seq += p.last_timing()[0]
+        its1.append(it)
+    for p in precs:
+        p.free()
+    bms = statistics.median(ms)
+    return {"form": f"{nsys} independent systems, idim uniform {lo}..{hi} (seed 1), own hierarchies, "
+                    f"FP32 V-cycle, FP64 FCG to {args.eps:g}, b = A*1",
+            "rows_total": rows, "idim_min": int(dims.min()), "idim_max": int(dims.max()),
+            "batched_ms": bms, "batched_systems_per_s": nsys / (bms * 1e-3),
+            "sequential_ms": seq, "sequential_systems_per_s": nsys / (seq * 1e-3),
+            "speedup": seq / bms, "iterations_batched": [int(its.min()), int(its.max())],
+            "iterations_single": [min(its1), max(its1)], "max_relres": float(rel.max()),
+            "max_abs_err_vs_ones": err}
+
+
+def time_batch(mld, args, dev, torch, nrhs=32, idim=128):
+    """Batching form (a): nrhs right-hand sides (uniform[-1,1], seed 1) through
+    one multi-vector V-cycle per FCG iteration (mldg_krylov_multi; FP32 V-cycle,
+    FP64 FCG) against nrhs single-vector FCG solves."""
+    a = mld.gen_pde3d(idim, 1, ISO)
+    p = make_prec(mld, a, "BJAC", "FP32", device=dev)
+    n = a.nrows
+    B = np.random.default_rng(1).uniform(-1.0, 1.0, (nrhs, n))
+    Bd = torch.tensor(B, dtype=torch.float64, device=f"cuda:{dev}")
+    Xd = torch.zeros_like(Bd)
+    p.krylov_multi("FCG", Bd, Xd, eps=args.eps, itmax=500)  # warm (captures the graphs)
+    reps = max(1, min(args.steps, 3))
+    ms = []
+    for _ in range(reps):
+        Xd.zero_()
+        _, its, rel = p.krylov_multi("FCG", Bd, Xd, eps=args.eps, itmax=500)
+        ms.append(p.last_timing()[0])
+    single = 0.0
+    its1 = []
+    x = torch.zeros(n, dtype=torch.float64, device=f"cuda:{dev}")
+    for c in range(nrhs):
+        x.zero_()
+        _, it, _ = mld.krylov("FCG", a, p, Bd[c], x, eps=args.eps, itmax=500, use_prec_matrix=True)
+        single += p.last_timing()[0]
+        its1.append(it)
+    Y = torch.zeros_like(Bd)
+    ap = []
+    for _ in range(5):
+        p.apply_block(Bd, Y)
+        ap.append(p.last_timing()[0])
+    ap1 = []
+    for _ in range(5):
+        p.apply(Bd[0].contiguous(), x)
+        ap1.append(p.last_timing()[0])
+    bms = statistics.median(ms)
+    p.free()
+    return {"form": f"{nrhs} right-hand sides, idim={idim}, BJAC FP32 V-cycle, FP64 FCG to {args.eps:g}",
+            "rows": n, "batched_ms": bms, "batched_solves_per_s": nrhs / (bms * 1e-3),
+            "sequential_ms": single, "sequential_solves_per_s": nrhs / (single * 1e-3),
+            "speedup": single / bms, "iterations_batched": [int(its.min()), int(its.max())],
+            "iterations_single": [min(its1), max(its1)], "max_relres": float(rel.max()),
+            "block_apply_ms": min(ap), "single_apply_ms": min(ap1),
+            "apply_per_rhs_speedup": min(ap1) * nrhs / min(ap)}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     mld = load_package()
@@ -291,6 +381,10 @@ def run_ours(args, rank, world, local_rank):
                 r = time_variant(mld, a, b, sm, pr, args, dev, torch, dist=dist)
                 others[f"{sm.lower()}_{pr.lower()}"] = r
                 r["p"].free()
+        batch = None
+        if not args.no_variants and not args.no_batch:
+            batch = {"rhs32_idim128": time_batch(mld, args, dev, torch),
+                     "systems64_idim24_96": time_systems(mld, args, dev, torch)}
     p = main["p"]
     # end-to-end through the public API with host buffers (pinned)
     bh = torch.empty(n, dtype=torch.float64, pin_memory=True)
@@ -341,6 +435,7 @@ def run_ours(args, rank, world, local_rank):
                      "avg_launch_ms": probe_ms / probe_cnt if probe_cnt else None,
                      "launches_timed": probe_cnt, "share_of_apply": main["share"]},
         "variants": variants,
+        "batching": batch,
         "e2e": {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "solves/s",
                 "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 8 * n},
         "gpu_launches": main["launches"],
@@ -372,6 +467,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true",
                     help="time only the selected smoother/precision form")
+    ap.add_argument("--no-batch", action="store_true", help="skip the many-right-hand-sides form")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -149,6 +149,20 @@ int mldg_krylov_multi(mldg_handle *h, int method, const mldg_csr *A, int nrhs,
                       const double *b, int ldb, double *x, int ldx, double tol,
                       int itmax, int *iters, double *relres, int mem_kind);
 
+/* nsys independent systems, each with its own finalized handle (hierarchy
+ * and finest-level matrix A_i, all on one device), solved together by CG/FCG
+ * in FP64: an iteration of system i (its V-cycle, in the handle's precision,
+ * and its Krylov kernels) is one CUDA graph captured on first use, and every
+ * iteration launches the graphs of all unconverged systems on their own
+ * streams so that the small systems' latency-bound V-cycles overlap.  b[i],
+ * x[i] are vectors of handle i's size (x[i] holds the initial guess); each
+ * system stops on its own ||b_i - A_i x_i||_2 / ||b_i||_2 <= tol.  Results
+ * equal mldg_krylov on each handle.  *ms (optional) receives the device time
+ * of the whole batch.  No counterpart in the reference. */
+int mldg_krylov_batch(int nsys, mldg_handle *const *h, int method, const double *const *b,
+                      double *const *x, double tol, int itmax, int *iters, double *relres,
+                      int mem_kind, double *ms);
+
 /* Adjoint solve A^T lambda = g with flexible CG in FP64, preconditioned by
  * the transposed V-cycle M^{-T} (the reference's trans='T' apply,
  * mld_dmlprec_aply.f90:634-656,765-777: smoothers swapped, A^T residuals,

@@ -176,6 +176,10 @@ def lib():
         L.mldg_krylov_multi.argtypes = [vp, C.c_int, C.POINTER(_CSR), C.c_int, C.c_void_p, C.c_int,
                                         C.c_void_p, C.c_int, C.c_double, C.c_int,
                                         C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int]
+        L.mldg_krylov_batch.argtypes = [C.c_int, C.POINTER(vp), C.c_int, C.POINTER(C.c_void_p),
+                                        C.POINTER(C.c_void_p), C.c_double, C.c_int,
+                                        C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int,
+                                        C.POINTER(C.c_double)]
         L.mldg_level_info.argtypes = [vp, C.c_int, C.POINTER(C.c_int64)]
         L.mldg_last_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
         L.mldg_apply_bytes.argtypes = [vp, C.POINTER(C.c_int64)]
@@ -537,3 +541,29 @@ def krylov(method: str, a: CSR, prec: MldPrec, b, x=None, eps: float = 1e-10,
     if rc and rc != ERR_NOT_CONVERGED:
         prec._check(rc)
     return x, it.value, err.value
+
+
+def krylov_batch(method: str, precs, bs, xs=None, eps: float = 1e-10, itmax: int = 500):
+    """Independent systems solved together (mldg_krylov_batch): precs[i] is a built
+    MldPrec or a finalized Hierarchy whose finest level is system i's matrix; bs[i]
+    its right-hand side (numpy or torch, all of one kind).  Returns
+    (xs, iters[nsys], relres[nsys], device ms of the whole batch)."""
+    m = {"CG": 0, "FCG": 1}[method.upper()]
+    nsys = len(precs)
+    if xs is None:
+        xs = [np.zeros_like(b) if isinstance(b, np.ndarray) else b.new_zeros(b.shape) for b in bs]
+    hs = (C.c_void_p * max(nsys, 1))()
+    bp = (C.c_void_p * max(nsys, 1))()
+    xp = (C.c_void_p * max(nsys, 1))()
+    mem = MEM_HOST
+    for i, (p, b, x) in enumerate(zip(precs, bs, xs)):
+        hs[i] = p._gpu()
+        xptr, bptr, mem = _vec_args(x, b)
+        xp[i], bp[i] = xptr, bptr
+    it = (C.c_int * max(nsys, 1))()
+    rr = (C.c_double * max(nsys, 1))()
+    ms = C.c_double(0)
+    rc = lib().mldg_krylov_batch(nsys, hs, m, bp, xp, eps, itmax, it, rr, mem, C.byref(ms))
+    if rc and rc != ERR_NOT_CONVERGED:
+        raise MldError(rc, lib().mldg_last_error(hs[0]).decode() if nsys else "krylov_batch")
+    return xs, np.array(it[:nsys]), np.array(rr[:nsys]), ms.value

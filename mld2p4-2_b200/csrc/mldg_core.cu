@@ -174,10 +174,12 @@ struct DTri {
   int nblkm[6] = {}, gridm[6] = {};
   // its ELL form (k_trsv_ell), per log2(K); ok = false falls back to k_trsv_sf_m
   struct Ell {
-    bool ok = false;
+    bool ok = false, pf = false;
     int ntask = 0, npad = 0, E = 0, S = 1, grid = 0, backoff = 0;
     int *prow = nullptr, *ej = nullptr, *ovp = nullptr, *ovj = nullptr, *ctr = nullptr;
     T *ev = nullptr, *ovv = nullptr;
+    unsigned long long *trace = nullptr;  // MLDG_ELL_TRACE: per-task timestamps
+    std::vector<int> h_task_level;
   } ell[6];
   bool present() const { return prow != nullptr; }
 };
@@ -245,6 +247,31 @@ static void kdispatch_ell(int K, F &&f) {
   else
     kdispatch(K, f);
 }
+// (K, E, PF) instances of k_trsv_ell: E in {4, 8, 16}, the next task's
+// metadata prefetched for E <= 8
+template <int V>
+using IC = std::integral_constant<int, V>;
+template <int KK, typename F>
+static void ell_dispatch_k(int E, bool pf, F &f) {
+  if constexpr (KK == 1) {
+    switch (E) {
+      case 4: f(IC<KK>(), IC<4>(), std::true_type()); break;
+      case 8: f(IC<KK>(), IC<8>(), std::true_type()); break;
+      default: f(IC<KK>(), IC<16>(), std::false_type()); break;
+    }
+  } else {
+    switch (E) {
+      case 4: f(IC<KK>(), IC<4>(), std::true_type()); break;
+      case 8: f(IC<KK>(), IC<8>(), std::true_type()); break;
+      default: f(IC<KK>(), IC<16>(), std::false_type()); break;
+    }
+  }
+}
+template <typename F>
+static void ell_dispatch(int K, int E, bool pf, F &&f) {
+  kdispatch_ell(K, [&](auto kc) { ell_dispatch_k<decltype(kc)::value>(E, pf, f); });
+}
+
 static int ilog2(int K) {
   int r = 0;
   while ((1 << r) < K) ++r;
@@ -707,7 +734,13 @@ struct EngineT : Engine {
     for (int L = 0; L < nl; ++L)
       for (int p = t.h_lvl[L]; p < t.h_lvl[L + 1]; ++p) lev_of[t.h_prow[p]] = L;
     for (int p = 0; p < t.n; ++p) emax = std::max(emax, t.h_pirp[p + 1] - t.h_pirp[p]);
-    const int E = emax <= 4 ? 4 : (emax <= 8 ? 8 : 16);
+    // slots per row: the longest row rounded up to a power of two, at most 16
+    // (measured best: wider slot sets cost registers and gained nothing);
+    // longer rows spill their oldest dependencies to the overflow
+    int ecap = 16;
+    if (const char *e = std::getenv("MLDG_ELL_ECAP")) ecap = std::max(4, std::min(ecap, std::atoi(e)));
+    int E = 4;
+    while (E < emax && E < ecap) E *= 2;
     std::vector<int> prow((size_t)npad, -1), ej((size_t)npad * E, -1), ovp((size_t)npad + 1, 0), ovj;
     std::vector<T> ev((size_t)npad * E, T(0)), ovv;
     std::vector<int> ord;
@@ -743,21 +776,18 @@ struct EngineT : Engine {
     el.npad = (int)npad;
     el.ntask = (int)(npad / rpw);
     el.E = E;
+    el.pf = E <= 8;
+    if (const char *e = std::getenv("MLDG_ELL_PF")) el.pf = el.pf && e[0] != '0';
     el.S = Kw >= 16 ? 16 : 1;
     if (const char *e = std::getenv("MLDG_ELL_BACKOFF")) el.backoff = std::max(0, std::atoi(e));
     if (const char *e = std::getenv("MLDG_ELL_S")) el.S = std::max(1, std::min(64, std::atoi(e)));
     int nb = 0;
-    kdispatch_ell(Kw, [&](auto kc) {
-      constexpr int KK = decltype(kc)::value;
-      switch (E) {
-        case 4: nb = ell_occupancy<KK, 4, true>(); break;
-        case 8: nb = ell_occupancy<KK, 8, true>(); break;
-        default: nb = ell_occupancy<KK, 16, false>(); break;
-      }
+    ell_dispatch(Kw, E, el.pf, [&](auto kc, auto ec, auto pc) {
+      nb = ell_occupancy<decltype(kc)::value, decltype(ec)::value, decltype(pc)::value>();
     });
     if (std::getenv("MLDG_VERBOSE"))
-      std::fprintf(stderr, "mldg: ell K=%d n=%d rev=%d levels=%d npad=%lld max row entries %d E=%d overflow %zu S=%d occ %d\n",
-                   Kw, t.n, t.rev, nl, (long long)npad, emax, E, ovj.size(), el.S, nb);
+      std::fprintf(stderr, "mldg: ell K=%d n=%d rev=%d levels=%d npad=%lld max row entries %d E=%d pf=%d overflow %zu S=%d occ %d\n",
+                   Kw, t.n, t.rev, nl, (long long)npad, emax, E, (int)el.pf, ovj.size(), el.S, nb);
     if (nb < 1) return;
     // every ticket stream needs running warps: grid <= co-resident capacity
     const int per_level = (el.ntask + nl - 1) / std::max(nl, 1);
@@ -773,6 +803,16 @@ struct EngineT : Engine {
       el.ovp = ar.upload(ovp);
       el.ovj = ar.upload(ovj);
       el.ovv = ar.upload(ovv);
+    }
+    if (std::getenv("MLDG_ELL_TRACE")) {
+      el.trace = ar.alloc<unsigned long long>((size_t)2 * el.ntask);
+      MLDG_CUDA(cudaMemsetAsync(el.trace, 0, sizeof(unsigned long long) * 2 * el.ntask, st));
+      el.h_task_level.resize(el.ntask);
+      int64_t q = 0;
+      for (int L = 0; L < nl; ++L) {
+        const int cnt = t.h_lvl[L + 1] - t.h_lvl[L];
+        for (int k = 0; k < (cnt + rpw - 1) / rpw; ++k) el.h_task_level[q++] = L;
+      }
     }
     el.ctr = ar.alloc<int>((size_t)32 * (el.S + 1));
     MLDG_CUDA(cudaMemsetAsync(el.ctr, 0, sizeof(int) * 32 * (el.S + 1), st));
@@ -926,6 +966,7 @@ struct EngineT : Engine {
       e.ovj = el.ovj;
       e.ovv = el.ovv;
       e.ctr = el.ctr;
+      e.trace = el.trace;
       e.rhs_src = rhs;
       e.rhs_scale = scale;
       e.cur = cur;
@@ -934,13 +975,8 @@ struct EngineT : Engine {
       e.alpha = alpha;
       e.beta = beta;
       e.err = err;
-      kdispatch_ell(Kw, [&](auto kc) {
-        constexpr int KK = decltype(kc)::value;
-        switch (el.E) {
-          case 4: k_trsv_ell<T, KK, 4, true><<<el.grid, 256, 0, st>>>(e); break;
-          case 8: k_trsv_ell<T, KK, 8, true><<<el.grid, 256, 0, st>>>(e); break;
-          default: k_trsv_ell<T, KK, 16, false><<<el.grid, 256, 0, st>>>(e); break;
-        }
+      ell_dispatch(Kw, el.E, el.pf, [&](auto kc, auto ec, auto pc) {
+        k_trsv_ell<T, decltype(kc)::value, decltype(ec)::value, decltype(pc)::value><<<el.grid, 256, 0, st>>>(e);
       });
     }
   }
@@ -1063,7 +1099,48 @@ struct EngineT : Engine {
     }
   }
 
+  // per-level timing of the last ELL solve of each factor (MLDG_ELL_TRACE)
+  void dump_ell_trace() {
+    for (size_t l = 0; l < lv.size(); ++l) {
+      const DTri<T> *fs[4] = {&lv[l].L, &lv[l].U, &lv[l].Ut, &lv[l].Lt};
+      const char *nm[4] = {"L", "U", "Ut", "Lt"};
+      for (int q = 0; q < 4; ++q)
+        for (int ki = 0; ki < 6; ++ki) {
+          const auto &el = fs[q]->ell[ki];
+          if (!el.ok || !el.trace) continue;
+          std::vector<unsigned long long> tr((size_t)2 * el.ntask);
+          cudaMemcpy(tr.data(), el.trace, tr.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+          const int nl = el.h_task_level.empty() ? 0 : el.h_task_level.back() + 1;
+          std::vector<unsigned long long> lend(nl, 0), lbeg_min(nl, ~0ull), lbeg_max(nl, 0);
+          double dur = 0;
+          unsigned long long t_first = ~0ull;
+          for (int t = 0; t < el.ntask; ++t) {
+            const int L = el.h_task_level[t];
+            lend[L] = std::max(lend[L], tr[2 * t + 1]);
+            lbeg_min[L] = std::min(lbeg_min[L], tr[2 * t]);
+            lbeg_max[L] = std::max(lbeg_max[L], tr[2 * t]);
+            dur += (double)(tr[2 * t + 1] - tr[2 * t]);
+            t_first = std::min(t_first, tr[2 * t]);
+          }
+          double step = 0, lag_last = 0, spread = 0;
+          for (int L = 1; L < nl; ++L) {
+            step += (double)(lend[L] - lend[L - 1]);
+            // how long after level L-1 completed did level L's last task start
+            lag_last += (double)lbeg_max[L] - (double)lend[L - 1];
+            spread += (double)(lend[L] - lbeg_max[L]);
+          }
+          std::fprintf(stderr,
+                       "mldg ell trace: level %zu %s K=%d tasks %d levels %d total %.1f us: per level %.0f ns "
+                       "(last task start - prev level end %.0f ns, last start -> level end %.0f ns), "
+                       "task duration avg %.0f ns\n",
+                       l, nm[q], 1 << ki, el.ntask, nl, (lend[nl - 1] - t_first) * 1e-3,
+                       nl > 1 ? step / (nl - 1) : 0.0, nl > 1 ? lag_last / (nl - 1) : 0.0,
+                       nl > 1 ? spread / (nl - 1) : 0.0, dur / el.ntask);
+        }
+    }
+  }
   void dump_trace() override {
+    dump_ell_trace();
     for (size_t l = 0; l < lv.size(); ++l) {
       if (!lv[l].win) continue;
       const DWin<T> *ws[4] = {&lv[l].wL, &lv[l].wU, &lv[l].wUt, &lv[l].wLt};
@@ -1178,7 +1255,19 @@ struct Handle {
   int kcap = 0;
   double *kb_m = nullptr, *kx_m = nullptr, *kd_m = nullptr, *kq_m = nullptr, *kpart_m = nullptr;
   KrylovM *ksc_m = nullptr, *hksc_m = nullptr;  // device state, pinned host mirror
+  // one captured CG/FCG iteration per [method][first] (systems solved in a batch)
+  cudaGraphExec_t kgraph[2][2] = {};
+  int64_t kglaunch[2][2] = {};
 };
+
+static void drop_krylov_graphs(Handle *h) {
+  for (int m = 0; m < 2; ++m)
+    for (int f = 0; f < 2; ++f)
+      if (h->kgraph[m][f]) {
+        cudaGraphExecDestroy(h->kgraph[m][f]);
+        h->kgraph[m][f] = nullptr;
+      }
+}
 
 static void drop_multi_graphs(Handle *h) {
   for (int t = 0; t < 2; ++t)
@@ -1830,6 +1919,7 @@ static void finalize(Handle *h, int nlev, int precision) {
       h->gexec[t] = nullptr;
     }
   drop_multi_graphs(h);
+  drop_krylov_graphs(h);
   h->eng.reset();
   h->arena.release();
   h->karena.release();
@@ -2058,6 +2148,34 @@ static void spmv64(Handle *h, const DCSR<double> &A, const double *v, double a1,
   h->last_launches++;
 }
 
+// One CG/FCG iteration after the preconditioner apply z = M^{-1} r: the
+// direction update, q = A d, the step and ||r||^2 into sc->dots[0]
+// (psb_dcg / psb_dfcg, one iteration; all scalars stay on the device).
+static void krylov_body(Handle *h, const DCSR<double> &A, int method, bool first) {
+  const int n = h->n0, nb = kRedBlocks;
+  double *r = h->xin, *z = h->yout, *d = h->kd, *q = h->kq, *xx = h->kx;
+  KrylovScalars *sc = h->ksc;
+  if (method == 1) {
+    if (!first) {
+      dots(h, n, 1, z, q, nullptr, nullptr, nullptr, nullptr);
+      k_scal_store<<<1, 32, 0, h->st>>>(sc, 0);
+      h->last_launches++;
+    }
+  } else {
+    dots(h, n, 1, r, z, nullptr, nullptr, nullptr, nullptr);
+    k_scal_store<<<1, 32, 0, h->st>>>(sc, 0);
+    h->last_launches++;
+  }
+  k_dir_update<<<nb, 256, 0, h->st>>>(n, method, first ? 1 : 0, z, d, sc);
+  spmv64(h, A, d, 1.0, nullptr, 0.0, q);  // q = A d
+  dots(h, n, 2, d, q, d, r, nullptr, nullptr);
+  k_scal_store<<<1, 32, 0, h->st>>>(sc, 1);
+  k_xr_update<<<nb, kRedThreads, 0, h->st>>>(n, method, d, q, xx, r, sc, h->kpart);
+  k_dots_final<<<1, kRedThreads, 0, h->st>>>(nb, h->kpart, sc->dots);
+  k_scal_store<<<1, 32, 0, h->st>>>(sc, 2);
+  h->last_launches += 6;
+}
+
 static void krylov(Handle *h, int method, const mldg_csr *Acsr, const double *b, double *x,
                    double tol, int itmax, int *iters, double *relres, int mem, char trans = 'N') {
   if (!h->finalized) fail(MLDG_ERR_NOT_BUILT, "krylov before build");
@@ -2079,7 +2197,7 @@ static void krylov(Handle *h, int method, const mldg_csr *Acsr, const double *b,
   }
   const cudaMemcpyKind h2d = mem == MLDG_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   const cudaMemcpyKind d2h = mem == MLDG_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
-  double *r = h->xin, *z = h->yout, *d = h->kd, *q = h->kq, *xx = h->kx, *bb = h->kb;
+  double *r = h->xin, *xx = h->kx, *bb = h->kb;
   KrylovScalars *sc = h->ksc;
   h->last_launches = 0;
   MLDG_CUDA(cudaEventRecord(h->ev0, h->st));
@@ -2093,29 +2211,10 @@ static void krylov(Handle *h, int method, const mldg_csr *Acsr, const double *b,
   if (bn2 == 0.0) bn2 = 1.0;
   double err = std::sqrt(h->hpin[1]) / bn2;
   int it = 0;
-  const int nb = kRedBlocks;
   while (err > tol && it < itmax) {
     ++it;
     run_vcycle(h, trans);  // z = M^{-1} r (or M^{-T} r)
-    if (method == 1) {
-      if (it > 1) {
-        dots(h, n, 1, z, q, nullptr, nullptr, nullptr, nullptr);
-        k_scal_store<<<1, 32, 0, h->st>>>(sc, 0);
-        h->last_launches++;
-      }
-    } else {
-      dots(h, n, 1, r, z, nullptr, nullptr, nullptr, nullptr);
-      k_scal_store<<<1, 32, 0, h->st>>>(sc, 0);
-      h->last_launches++;
-    }
-    k_dir_update<<<nb, 256, 0, h->st>>>(n, method, it == 1 ? 1 : 0, z, d, sc);
-    spmv64(h, A, d, 1.0, nullptr, 0.0, q);  // q = A d
-    dots(h, n, 2, d, q, d, r, nullptr, nullptr);
-    k_scal_store<<<1, 32, 0, h->st>>>(sc, 1);
-    k_xr_update<<<nb, kRedThreads, 0, h->st>>>(n, method, d, q, xx, r, sc, h->kpart);
-    k_dots_final<<<1, kRedThreads, 0, h->st>>>(nb, h->kpart, sc->dots);
-    k_scal_store<<<1, 32, 0, h->st>>>(sc, 2);
-    h->last_launches += 6;
+    krylov_body(h, A, method, it == 1);
     MLDG_CUDA(cudaMemcpyAsync(h->hpin, sc->dots, sizeof(double), cudaMemcpyDeviceToHost, h->st));
     MLDG_CUDA(cudaStreamSynchronize(h->st));
     probe_collect(h);
@@ -2278,6 +2377,140 @@ static void krylov_multi(Handle *h, int method, const mldg_csr *Acsr, int nrhs, 
   tmp.release();
   check_device_error(h);
 }
+
+// ---------------------------------------------------------------------------
+// Independent systems solved together: every handle keeps its own hierarchy,
+// stream and FP64 Krylov state; one CG/FCG iteration of a system (V-cycle +
+// Krylov kernels + the D2H copy of ||r||^2) is one CUDA graph captured once
+// per handle, and an iteration of the batch launches the graphs of all
+// still-active systems on their own streams so that they run concurrently.
+// Each system follows exactly the kernel sequence of krylov() (same results).
+
+static void capture_iteration(Handle *h, int method, int first) {
+  if (h->kgraph[method][first]) return;
+  cudaGraph_t g;
+  MLDG_CUDA(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+  h->eng->capturing = true;
+  const int64_t l0 = h->last_launches;
+  try {
+    h->eng->record('N');
+    krylov_body(h, h->A0, method, first != 0);
+    MLDG_CUDA(cudaMemcpyAsync(h->hpin, h->ksc->dots, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  } catch (...) {
+    h->eng->capturing = false;
+    cudaStreamEndCapture(h->st, &g);
+    throw;
+  }
+  h->eng->capturing = false;
+  MLDG_CUDA(cudaStreamEndCapture(h->st, &g));
+  MLDG_CUDA(cudaGraphInstantiate(&h->kgraph[method][first], g, 0));
+  cudaGraphDestroy(g);
+  h->kglaunch[method][first] = h->eng->launches + (h->last_launches - l0);
+  h->last_launches = l0;
+}
+
+static void krylov_batch(int nsys, Handle **hs, int method, const double *const *b, double *const *x, double tol,
+                         int itmax, int *iters, double *relres, int mem, double *ms_out) {
+  if (nsys < 0) fail(MLDG_ERR_ARG, "nsys < 0");
+  if (nsys == 0) return;
+  if (!hs || !b || !x || !iters || !relres) fail(MLDG_ERR_ARG, "null argument");
+  if (method != 0 && method != 1) fail(MLDG_ERR_ARG, "method must be 0 (CG) or 1 (FCG)");
+  if (itmax < 0) fail(MLDG_ERR_ARG, "itmax < 0");
+  if (mem != MLDG_MEM_HOST && mem != MLDG_MEM_DEVICE) fail(MLDG_ERR_ARG, "bad mem_kind");
+  const int dev = hs[0]->opts.device;
+  for (int i = 0; i < nsys; ++i) {
+    if (!hs[i]) fail(MLDG_ERR_ARG, "system %d: null handle", i);
+    if (!hs[i]->finalized) fail(MLDG_ERR_NOT_BUILT, "system %d: krylov before build", i);
+    if (hs[i]->opts.device != dev) fail(MLDG_ERR_ARG, "system %d: handles on different devices", i);
+    if (!b[i] || !x[i]) fail(MLDG_ERR_ARG, "system %d: null vector", i);
+    for (int k = 0; k < i; ++k)
+      if (hs[k] == hs[i]) fail(MLDG_ERR_ARG, "system %d: handle repeated", i);
+  }
+  MLDG_CUDA(cudaSetDevice(dev));
+  const cudaMemcpyKind h2d = mem == MLDG_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  const cudaMemcpyKind d2h = mem == MLDG_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  cudaStream_t ms = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  MLDG_CUDA(cudaStreamCreateWithFlags(&ms, cudaStreamNonBlocking));
+  MLDG_CUDA(cudaEventCreate(&e0));
+  MLDG_CUDA(cudaEventCreate(&e1));
+  std::vector<double> bn(nsys, 1.0), err(nsys, 0.0);
+  std::vector<char> active(nsys, 0);
+  try {
+    // graphs first (capture is not timed)
+    for (int i = 0; i < nsys; ++i) {
+      hs[i]->last_launches = 0;
+      capture_iteration(hs[i], method, 1);
+      capture_iteration(hs[i], method, 0);
+    }
+    MLDG_CUDA(cudaEventRecord(e0, ms));
+    for (int i = 0; i < nsys; ++i) {
+      Handle *h = hs[i];
+      const int n = h->n0;
+      MLDG_CUDA(cudaStreamWaitEvent(h->st, e0, 0));
+      MLDG_CUDA(cudaMemcpyAsync(h->kb, b[i], sizeof(double) * n, h2d, h->st));
+      MLDG_CUDA(cudaMemcpyAsync(h->kx, x[i], sizeof(double) * n, h2d, h->st));
+      spmv64(h, h->A0, h->kx, -1.0, h->kb, 1.0, h->xin);  // r = b - A x
+      dots(h, n, 2, h->kb, h->kb, h->xin, h->xin, nullptr, nullptr);
+      MLDG_CUDA(cudaMemcpyAsync(h->hpin, h->ksc->dots, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    }
+    for (int i = 0; i < nsys; ++i) {
+      MLDG_CUDA(cudaStreamSynchronize(hs[i]->st));
+      bn[i] = std::sqrt(hs[i]->hpin[0]);
+      if (bn[i] == 0.0) bn[i] = 1.0;
+      err[i] = std::sqrt(hs[i]->hpin[1]) / bn[i];
+      active[i] = err[i] > tol && itmax > 0;
+      iters[i] = 0;
+    }
+    int it = 0;
+    auto any = [&]() {
+      for (char a : active)
+        if (a) return true;
+      return false;
+    };
+    while (any() && it < itmax) {
+      ++it;
+      const int f = it == 1 ? 1 : 0;
+      for (int i = 0; i < nsys; ++i)
+        if (active[i]) {
+          MLDG_CUDA(cudaGraphLaunch(hs[i]->kgraph[method][f], hs[i]->st));
+          hs[i]->last_launches += hs[i]->kglaunch[method][f];
+        }
+      for (int i = 0; i < nsys; ++i)
+        if (active[i]) {
+          MLDG_CUDA(cudaStreamSynchronize(hs[i]->st));
+          err[i] = std::sqrt(std::max(hs[i]->hpin[0], 0.0)) / bn[i];
+          iters[i] = it;
+          if (!(err[i] > tol)) active[i] = 0;
+        }
+    }
+    for (int i = 0; i < nsys; ++i) {
+      Handle *h = hs[i];
+      relres[i] = err[i];
+      MLDG_CUDA(cudaMemcpyAsync(x[i], h->kx, sizeof(double) * h->n0, d2h, h->st));
+      MLDG_CUDA(cudaEventRecord(h->ev1, h->st));
+      MLDG_CUDA(cudaStreamWaitEvent(ms, h->ev1, 0));
+    }
+    MLDG_CUDA(cudaEventRecord(e1, ms));
+    MLDG_CUDA(cudaStreamSynchronize(ms));
+    float t = 0;
+    MLDG_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    if (ms_out) *ms_out = t;
+    for (int i = 0; i < nsys; ++i) {
+      hs[i]->last_ms = t;
+      check_device_error(hs[i]);
+    }
+  } catch (...) {
+    cudaStreamSynchronize(ms);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(ms);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamDestroy(ms);
+}
 }  // namespace mldg
 
 // ===========================================================================
@@ -2400,6 +2633,29 @@ extern "C" int mldg_krylov_multi(mldg_handle *hp, int method, const mldg_csr *A,
   });
 }
 
+extern "C" int mldg_krylov_batch(int nsys, mldg_handle *const *hps, int method, const double *const *b,
+                                 double *const *x, double tol, int itmax, int *iters, double *relres, int mem_kind,
+                                 double *ms) {
+  if (nsys > 0 && !hps) return MLDG_ERR_ARG;
+  for (int i = 0; i < nsys; ++i)
+    if (!hps[i]) return MLDG_ERR_ARG;
+  mldg_handle *hp = nsys > 0 ? hps[0] : nullptr;
+  std::vector<Handle *> hs((size_t)std::max(nsys, 0));
+  for (int i = 0; i < nsys; ++i) hs[i] = &hps[i]->h;
+  MLDG_GUARD(hp, {
+    try {
+      mldg::krylov_batch(nsys, hs.data(), method, b, x, tol, itmax, iters, relres, mem_kind, ms);
+    } catch (const Error &e) {
+      for (int i = 1; i < nsys; ++i) hps[i]->h.last_error = e.msg;
+      throw;
+    }
+    for (int i = 0; i < nsys; ++i)
+      if (iters[i] >= itmax && !(relres[i] <= tol))
+        mldg::fail(MLDG_ERR_NOT_CONVERGED, "system %d not converged in %d iterations (relres %.3e)", i, iters[i],
+                   relres[i]);
+  });
+}
+
 extern "C" int mldg_adjoint(mldg_handle *hp, const double *g, double *lambda, double tol, int itmax,
                             int *iters, double *relres, int mem_kind) {
   if (!hp) return MLDG_ERR_ARG;
@@ -2486,6 +2742,8 @@ extern "C" int mldg_probe_set(mldg_handle *hp, int kind, int lev, int index) {
         cudaGraphExecDestroy(h.gexec[t]);
         h.gexec[t] = nullptr;
       }
+    mldg::drop_multi_graphs(&h);
+    mldg::drop_krylov_graphs(&h);
     if (h.eng) {
       h.eng->probe_kind = kind;
       h.eng->probe_lev = lev;
@@ -2655,10 +2913,11 @@ extern "C" void mldg_destroy(mldg_handle *hp) {
   Handle &h = hp->h;
   cudaSetDevice(h.opts.device);
   if (h.st) cudaStreamSynchronize(h.st);
-  if (h.eng && std::getenv("MLDG_WIN_TRACE")) h.eng->dump_trace();
+  if (h.eng && (std::getenv("MLDG_WIN_TRACE") || std::getenv("MLDG_ELL_TRACE"))) h.eng->dump_trace();
   for (int t = 0; t < 2; ++t)
     if (h.gexec[t]) cudaGraphExecDestroy(h.gexec[t]);
   mldg::drop_multi_graphs(&h);
+  mldg::drop_krylov_graphs(&h);
   h.eng.reset();
   h.arena.release();
   h.karena.release();

@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(256) k_trsv_sf_m(TriArgs<T> a, int nblk_m, con
 template <typename T>
 struct EllArgs {
   int ntask, npad, S;
-  int backoff;  // ns slept between polls after the first few (0: poll back to back)
+  int backoff;  // > 0: ns slept between polls after the first few (0: back to back)
   const int *prow;
   const int *ej;
   const T *ev;
@@ -230,7 +230,14 @@ struct EllArgs {
   T alpha, beta;
   int *ctr;  // S ticket counters (stride 32 ints), then the finished-warp count
   int *err;
+  unsigned long long *trace;  // diagnostics: per task [start, end] globaltimer ns, or null
 };
+
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 template <typename T, int E>
 struct EllMeta {
@@ -272,8 +279,8 @@ __device__ __forceinline__ bool ell_wait(typename Bits<T>::U (&raw)[N], const in
     if ((it % kSpinCheck) == kSpinCheck - 1) {
       if (ld_relaxed_u32(err) != 0u) return false;
       __nanosleep(32);
-    } else if (backoff && it >= 2) {
-      __nanosleep(backoff);
+    } else if (backoff > 0 && it >= 2) {
+      __nanosleep(backoff);  // measured: no gain on B200, off by default
     }
 #pragma unroll
     for (int e = 0; e < N; ++e)
@@ -302,6 +309,8 @@ __global__ void __launch_bounds__(256) k_trsv_ell(EllArgs<T> a) {
   if (t < a.ntask) ell_meta<T, E>(a, t * RPW + grp, m);
   while (t < a.ntask) {
     if (PF && tn < a.ntask) ell_meta<T, E>(a, tn * RPW + grp, mn);
+    unsigned long long t0 = 0;
+    if (a.trace) t0 = gtimer();
     if (m.o >= 0) {
       const size_t oc = (size_t)m.o * K + c;
       T rhs = a.rhs_src[oc];
@@ -336,6 +345,13 @@ __global__ void __launch_bounds__(256) k_trsv_ell(EllArgs<T> a) {
         T w = a.alpha * r;
         if (a.beta != T(0)) w = fma(a.beta, a.out[oc], w);
         a.out[oc] = w;
+      }
+    }
+    if (a.trace) {
+      __syncwarp();
+      if (lane == 0) {
+        a.trace[2 * (size_t)t] = t0;
+        a.trace[2 * (size_t)t + 1] = gtimer();
       }
     }
     t = tn;
