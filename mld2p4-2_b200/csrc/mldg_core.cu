@@ -177,7 +177,9 @@ struct DTri {
     bool ok = false, pf = false;
     int ntask = 0, npad = 0, E = 0, S = 1, grid = 0, backoff = 0;
     int *prow = nullptr, *ej = nullptr, *ovp = nullptr, *ovj = nullptr, *ctr = nullptr;
+    int2 *toff = nullptr;
     T *ev = nullptr, *ovv = nullptr;
+    int64_t slots = 0;  // entry slots stored (sum over tasks of slots per row x rows per task)
     unsigned long long *trace = nullptr;  // MLDG_ELL_TRACE: per-task timestamps
     std::vector<int> h_task_level;
   } ell[6];
@@ -741,40 +743,65 @@ struct EngineT : Engine {
     if (const char *e = std::getenv("MLDG_ELL_ECAP")) ecap = std::max(4, std::min(ecap, std::atoi(e)));
     int E = 4;
     while (E < emax && E < ecap) E *= 2;
-    std::vector<int> prow((size_t)npad, -1), ej((size_t)npad * E, -1), ovp((size_t)npad + 1, 0), ovj;
-    std::vector<T> ev((size_t)npad * E, T(0)), ovv;
-    std::vector<int> ord;
-    int64_t pp = 0;
-    for (int L = 0; L < nl; ++L) {
-      for (int p = t.h_lvl[L]; p < t.h_lvl[L + 1]; ++p, ++pp) {
-        const int i = t.h_prow[p];
-        prow[pp] = t.rev ? t.n - 1 - i : i;
-        const int k0 = t.h_pirp[p], len = t.h_pirp[p + 1] - k0;
-        ord.resize(len);
-        for (int e = 0; e < len; ++e) ord[e] = k0 + e;
-        std::stable_sort(ord.begin(), ord.end(),
-                         [&](int x, int y) { return lev_of[t.h_pja[x]] < lev_of[t.h_pja[y]]; });
-        const int nov = std::max(0, len - E);
-        for (int e = 0; e < len; ++e) {
-          const int k = ord[e], jj = t.h_pja[k];
-          const int oj = t.rev ? t.n - 1 - jj : jj;
-          if (e < nov) {
-            ovj.push_back(oj);
-            ovv.push_back((T)t.h_pval[k]);
-          } else {
-            ej[(size_t)(e - nov) * npad + pp] = oj;
-            ev[(size_t)(e - nov) * npad + pp] = (T)t.h_pval[k];
-          }
-        }
-        ovp[pp + 1] = (int)ovj.size();
-      }
-      while (pp % rpw) {
-        ovp[pp + 1] = ovp[pp];
-        ++pp;
+    // padded positions: position -> schedule index (-1 = padding)
+    std::vector<int> pos((size_t)npad, -1);
+    {
+      int64_t pp = 0;
+      for (int L = 0; L < nl; ++L) {
+        for (int p = t.h_lvl[L]; p < t.h_lvl[L + 1]; ++p) pos[pp++] = p;
+        while (pp % rpw) ++pp;
       }
     }
+    const int ntask = (int)(npad / rpw);
+    std::vector<int2> toff((size_t)ntask);
+    int64_t slots = 0;
+    // one or two rows per task (K >= 16): uniform E slots, no per-task lookup
+    const bool uniform = rpw <= 2;
+    for (int tk = 0; tk < ntask; ++tk) {
+      int et = 0;
+      for (int g = 0; g < rpw; ++g) {
+        const int p = pos[(size_t)tk * rpw + g];
+        if (p >= 0) et = std::max(et, t.h_pirp[p + 1] - t.h_pirp[p]);
+      }
+      et = uniform ? E : std::min(et, E);
+      toff[tk] = make_int2((int)slots, et);
+      slots += (int64_t)et * rpw;
+    }
+    if (slots >= (int64_t)INT32_MAX) return;
+    std::vector<int> prow((size_t)npad, -1), ej((size_t)std::max<int64_t>(slots, 1), -1),
+        ovp((size_t)npad + 1, 0), ovj;
+    std::vector<T> ev((size_t)std::max<int64_t>(slots, 1), T(0)), ovv;
+    std::vector<int> ord;
+    for (int64_t pp = 0; pp < npad; ++pp) {
+      const int p = pos[pp];
+      ovp[pp + 1] = ovp[pp];
+      if (p < 0) continue;
+      const int tk = (int)(pp / rpw), g = (int)(pp % rpw), et = toff[tk].y;
+      const int i = t.h_prow[p];
+      prow[pp] = t.rev ? t.n - 1 - i : i;
+      const int k0 = t.h_pirp[p], len = t.h_pirp[p + 1] - k0;
+      ord.resize(len);
+      for (int e = 0; e < len; ++e) ord[e] = k0 + e;
+      std::stable_sort(ord.begin(), ord.end(),
+                       [&](int x, int y) { return lev_of[t.h_pja[x]] < lev_of[t.h_pja[y]]; });
+      const int nov = std::max(0, len - et);
+      for (int e = 0; e < len; ++e) {
+        const int k = ord[e], jj = t.h_pja[k];
+        const int oj = t.rev ? t.n - 1 - jj : jj;
+        if (e < nov) {
+          ovj.push_back(oj);
+          ovv.push_back((T)t.h_pval[k]);
+        } else {
+          const size_t q = (size_t)toff[tk].x + (size_t)(e - nov) * rpw + g;
+          ej[q] = oj;
+          ev[q] = (T)t.h_pval[k];
+        }
+      }
+      ovp[pp + 1] = (int)ovj.size();
+    }
     el.npad = (int)npad;
-    el.ntask = (int)(npad / rpw);
+    el.ntask = ntask;
+    el.slots = slots;
     el.E = E;
     el.pf = E <= 8;
     if (const char *e = std::getenv("MLDG_ELL_PF")) el.pf = el.pf && e[0] != '0';
@@ -786,8 +813,11 @@ struct EngineT : Engine {
       nb = ell_occupancy<decltype(kc)::value, decltype(ec)::value, decltype(pc)::value>();
     });
     if (std::getenv("MLDG_VERBOSE"))
-      std::fprintf(stderr, "mldg: ell K=%d n=%d rev=%d levels=%d npad=%lld max row entries %d E=%d pf=%d overflow %zu S=%d occ %d\n",
-                   Kw, t.n, t.rev, nl, (long long)npad, emax, E, (int)el.pf, ovj.size(), el.S, nb);
+      std::fprintf(stderr,
+                   "mldg: ell K=%d n=%d rev=%d levels=%d npad=%lld max row entries %d E=%d pf=%d slots %lld "
+                   "(entries %lld) overflow %zu S=%d occ %d\n",
+                   Kw, t.n, t.rev, nl, (long long)npad, emax, E, (int)el.pf, (long long)slots, (long long)t.nnz,
+                   ovj.size(), el.S, nb);
     if (nb < 1) return;
     // every ticket stream needs running warps: grid <= co-resident capacity
     const int per_level = (el.ntask + nl - 1) / std::max(nl, 1);
@@ -797,6 +827,7 @@ struct EngineT : Engine {
     el.grid = (int)std::min<int64_t>((warps + 7) / 8, (int64_t)nb * nsm);
     el.grid = std::max(el.grid, (el.S + 7) / 8);
     el.prow = ar.upload(prow);
+    if (!uniform) el.toff = ar.upload(toff);
     el.ej = ar.upload(ej);
     el.ev = ar.upload(ev);
     if (!ovj.empty()) {
@@ -957,6 +988,7 @@ struct EngineT : Engine {
       EllArgs<T> e;
       e.ntask = el.ntask;
       e.npad = el.npad;
+      e.toff = el.toff;
       e.S = el.S;
       e.backoff = el.backoff;
       e.prow = el.prow;

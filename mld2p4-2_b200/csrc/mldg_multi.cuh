@@ -195,9 +195,12 @@ __global__ void __launch_bounds__(256) k_trsv_sf_m(TriArgs<T> a, int nblk_m, con
 // ELL form of the multi-RHS sync-free solve.  The level-ordered rows are laid
 // out in padded positions: every level starts at a multiple of RPW = 32/K, so
 // the RPW rows of a warp task never straddle a level (no lane waits on its own
-// warp).  Per padded position pp: the original row prow[pp] (-1 = padding) and
-// E entry slots ej/ev[e*npad + pp] with the original index of the dependency
-// row (-1 = empty) and the factor value.  A row's entries are ordered by the
+// warp).  Per padded position pp = t*RPW + g (task t, row g of the task): the
+// original row prow[pp] (-1 = padding).  Task t owns E_t = toff[t].y entry
+// slots per row (the longest row of the task, at most E), stored at
+// ej/ev[toff[t].x + e*RPW + g]: the original index of the dependency row
+// (-1 = empty) and the factor value, so padding costs no more than the
+// longest row of each task.  A row's entries are ordered by the
 // level of their dependency; rows longer than E keep their E most recent
 // dependencies in the slots and the older ones in an overflow list
 // (ovp/ovj/ovv), accumulated first.  All slot loads of a row are in flight at
@@ -215,6 +218,7 @@ __global__ void __launch_bounds__(256) k_trsv_sf_m(TriArgs<T> a, int nblk_m, con
 template <typename T>
 struct EllArgs {
   int ntask, npad, S;
+  const int2 *toff;  // per task: slot base, slots per row; null: uniform (t*E*RPW, E)
   int backoff;  // > 0: ns slept between polls after the first few (0: back to back)
   const int *prow;
   const int *ej;
@@ -246,8 +250,9 @@ struct EllMeta {
   T v[E];
 };
 
-template <typename T, int E>
-__device__ __forceinline__ void ell_meta(const EllArgs<T> &a, int pp, EllMeta<T, E> &m) {
+template <typename T, int E, int RPW>
+__device__ __forceinline__ void ell_meta(const EllArgs<T> &a, int t, int g, int2 to, EllMeta<T, E> &m) {
+  const int pp = t * RPW + g;
   m.o = a.prow[pp];
   m.q0 = m.q1 = 0;
   if (a.ovp) {
@@ -256,8 +261,10 @@ __device__ __forceinline__ void ell_meta(const EllArgs<T> &a, int pp, EllMeta<T,
   }
 #pragma unroll
   for (int e = 0; e < E; ++e) {
-    m.j[e] = a.ej[(size_t)e * a.npad + pp];
-    m.v[e] = a.ev[(size_t)e * a.npad + pp];
+    const bool has = e < to.y;
+    const size_t q = (size_t)to.x + (size_t)e * RPW + g;
+    m.j[e] = has ? a.ej[q] : -1;
+    m.v[e] = has ? a.ev[q] : T(0);
   }
 }
 
@@ -306,9 +313,14 @@ __global__ void __launch_bounds__(256) k_trsv_ell(EllArgs<T> a) {
   int tn = __shfl_sync(0xffffffffu, pend, 0) * a.S + s;
   if (lane == 0) pend = atomicAdd(ctr, 1);
   EllMeta<T, E> m, mn;
-  if (t < a.ntask) ell_meta<T, E>(a, t * RPW + grp, m);
+  auto slot_of = [&](int tt) {
+    return a.toff ? (tt < a.ntask ? a.toff[tt] : make_int2(0, 0)) : make_int2(tt * E * RPW, E);
+  };
+  int2 to = slot_of(t);
+  int2 ton = slot_of(tn);
+  if (t < a.ntask) ell_meta<T, E, RPW>(a, t, grp, to, m);
   while (t < a.ntask) {
-    if (PF && tn < a.ntask) ell_meta<T, E>(a, tn * RPW + grp, mn);
+    if (PF && tn < a.ntask) ell_meta<T, E, RPW>(a, tn, grp, ton, mn);
     unsigned long long t0 = 0;
     if (a.trace) t0 = gtimer();
     if (m.o >= 0) {
@@ -355,12 +367,14 @@ __global__ void __launch_bounds__(256) k_trsv_ell(EllArgs<T> a) {
       }
     }
     t = tn;
+    to = ton;
     tn = __shfl_sync(0xffffffffu, pend, 0) * a.S + s;
     if (lane == 0) pend = atomicAdd(ctr, 1);
+    ton = slot_of(tn);
     if (PF) {
       m = mn;
     } else if (t < a.ntask) {
-      ell_meta<T, E>(a, t * RPW + grp, m);
+      ell_meta<T, E, RPW>(a, t, grp, to, m);
     }
   }
   // the last warp to leave resets the ticket streams for the next launch
