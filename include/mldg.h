@@ -46,6 +46,8 @@ extern "C" {
 /* ---- smoother / solver kinds (mld_base_prec_type.F90 names) ------------- */
 #define MLDG_SMOOTHER_JACOBI 1   /* mld_jac_: jac smoother + diag solver      */
 #define MLDG_SMOOTHER_BJAC 2     /* mld_bjac_: jac smoother + ILU(0) solver   */
+#define MLDG_SMOOTHER_FBGS 3     /* mld_fbgs_: jac smoother + forward GS (pre),
+                                    jac smoother + backward GS (post)         */
 
 /* ---- precision forms chosen at finalize -------------------------------- */
 #define MLDG_PREC_FP64 0         /* plain FP64 drop-in                        */
@@ -81,6 +83,15 @@ typedef struct {
  *                         (mld_d_ilu_solver.f90:63-68, mld_dilu0_fact.f90:436-457)
  *   MLDG_SMOOTHER_JACOBI: ND = off-diagonal part, d = 1/a_ii with 0 -> 1
  *                         (mld_d_jac_smoother.f90:56-62, mld_d_diag_solver_bld.f90:86-92)
+ *   MLDG_SMOOTHER_FBGS  : L = strictly lower, U = strictly upper triangle of
+ *                         A, d = the diagonal a_ii (nonzero): the GS solver's
+ *                         tril/triu split (mld_d_gs_solver_bld.f90:73-81);
+ *                         pre-smoothing sweeps are forward GS, post-smoothing
+ *                         sweeps backward GS (mld_d_base_onelev_cseti.F90:128-132).
+ *                         trans 'T' is rejected like the reference's GS solver
+ *                         (mld_d_gs_solver_apply_vect.f90:68-75, MLDG_ERR_TRANS).
+ *                         A one-level hierarchy applies forward then backward GS
+ *                         max(sweeps_pre, sweeps_post) times (mld_dprecaply.f90:374-409).
  * Level l >= 1 also carries P and R (mld_d_onelev_mod.f90:122-158, map).
  * sweeps_pre/sweeps_post: mld_dml_parms (the coarsest level uses
  * sweeps_pre, mld_dmlprec_aply.f90:787-793).  damping: extension, 1.0 is the

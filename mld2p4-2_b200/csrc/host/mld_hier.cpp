@@ -456,6 +456,33 @@ int smoothers_build(std::vector<Level> &lv, const Parms &p, std::string &msg) {
         msg = "ILU(0): pivot too small at level " + std::to_string(l) + " row " + std::to_string(rc - 1);
         return 2;
       }
+    } else if (L.kind == SM_FBGS) {
+      // GS / BWGS solvers (mld_d_gs_solver_bld.f90:73-81): strict lower and
+      // strict upper triangles and the diagonal; the GS solve divides by a_ii
+      L.L.nr = L.L.nc = L.U.nr = L.U.nc = n;
+      L.L.irp.assign((size_t)n + 1, 0);
+      L.U.irp.assign((size_t)n + 1, 0);
+      L.d.assign((size_t)n, 0.0);
+      for (int i = 0; i < n; ++i) {
+        for (int k = a.irp[i]; k < a.irp[i + 1]; ++k) {
+          const int j = a.ja[k];
+          if (j < i) {
+            L.L.ja.push_back(j);
+            L.L.val.push_back(a.val[k]);
+          } else if (j > i) {
+            L.U.ja.push_back(j);
+            L.U.val.push_back(a.val[k]);
+          } else {
+            L.d[i] = a.val[k];
+          }
+        }
+        L.L.irp[i + 1] = (int)L.L.ja.size();
+        L.U.irp[i + 1] = (int)L.U.ja.size();
+        if (L.d[i] == 0.0) {
+          msg = "Gauss-Seidel: zero diagonal at level " + std::to_string(l) + " row " + std::to_string(i);
+          return 2;
+        }
+      }
     } else {
       msg = "unsupported smoother kind";
       return 30;

@@ -20,7 +20,7 @@ struct CSR {
   bool present() const { return !irp.empty(); }
 };
 
-enum SmootherKind { SM_JACOBI = 1, SM_BJAC = 2 };
+enum SmootherKind { SM_JACOBI = 1, SM_BJAC = 2, SM_FBGS = 3 };
 
 struct Parms {
   // global (mld_dprec_type, mlprec/mld_d_prec_type.f90:84-110)
@@ -47,8 +47,8 @@ struct Level {
   double omega = 0;
   int kind = SM_BJAC, sweeps_pre = 1, sweeps_post = 1;
   double damping = 1.0;
-  CSR L, U, ND;  // ILU(0) factors / off-diagonal part
-  std::vector<double> d;  // ILU 1/pivot or diag-solver inverse diagonal
+  CSR L, U, ND;  // ILU(0) factors, FBGS strict triangles / off-diagonal part
+  std::vector<double> d;  // ILU 1/pivot, diag-solver inverse diagonal or FBGS diagonal a_ii
 };
 
 // tests/pdegen/mld_d_pde3d.f90:98-412 with constant coefficients

@@ -20,7 +20,6 @@ struct mldp_prec {
   bool inited = false;
   std::string ptype;
   mld::Parms parms;
-  bool fbgs_requested = false;  // the reference ML default smoother (not on the GPU path)
   std::string unsupported;      // first unsupported setting, reported at build
   int precision = MLDG_PREC_FP64;
   std::vector<mld::Level> lv;
@@ -85,18 +84,21 @@ extern "C" int mldp_init(mldp_prec *p, const char *ptype) {
   p->lv.clear();
   p->hier_built = p->smoothers_built = false;
   p->unsupported.clear();
-  p->fbgs_requested = false;
   p->precision = MLDG_PREC_FP64;
   if (t == "ML") {
     // mld_dprecinit.F90:188-207: VCYCLE, FBGS smoother, ILU coarse solver
     // (no UMFPACK/MUMPS/SuperLU): BJAC + ILU(0), replicated coarse matrix.
     p->parms.max_levs = 20;
-    p->fbgs_requested = true;
+    p->parms.smoother = mld::SM_FBGS;
     p->parms.coarse_solver = mld::SM_BJAC;
     p->parms.coarse_sweeps = 1;
   } else if (t == "BJAC" || t == "JACOBI") {
     p->parms.max_levs = 1;
     p->parms.smoother = smoother_code(t);
+  } else if (t == "FBGS") {
+    // mld_dprecinit.F90:162-166: one level, forward GS then backward GS
+    p->parms.max_levs = 1;
+    p->parms.smoother = mld::SM_FBGS;
   } else {
     return fail(p, MLDG_ERR_ARG, "init: unknown preconditioner type '" + t + "'");
   }
@@ -120,12 +122,10 @@ static int set_common(mldp_prec *p, const std::string &w, const std::string *sv,
   };
   if (w == "SMOOTHER_TYPE") {
     const std::string v = sv ? upper(sv->c_str()) : "";
-    const int c = smoother_code(v);
+    const int c = v == "FBGS" ? (int)mld::SM_FBGS : smoother_code(v);
     if (c < 0) {
-      p->fbgs_requested = (v == "FBGS");
-      if (!p->fbgs_requested && p->unsupported.empty()) p->unsupported = w + "=" + v;
+      if (p->unsupported.empty()) p->unsupported = w + "=" + v;
     } else {
-      p->fbgs_requested = false;
       q.smoother = c;
     }
   } else if (w == "SUB_SOLVE") {
@@ -217,9 +217,6 @@ extern "C" int mldp_hierarchy_build(mldp_prec *p, int n, const int32_t *irp, con
   if (!p) return MLDG_ERR_ARG;
   if (!p->inited) return fail(p, 3111, "hierarchy_build before init");
   if (n <= 0 || !irp || !ja || !val) return fail(p, MLDG_ERR_ARG, "hierarchy_build: bad matrix");
-  if (p->fbgs_requested)
-    return fail(p, MLDG_ERR_ARG,
-                "smoother FBGS (the ML default) has no GPU apply; set SMOOTHER_TYPE to JACOBI or BJAC");
   if (!p->unsupported.empty())
     return fail(p, MLDG_ERR_ARG, "setting not supported by the GPU apply: " + p->unsupported);
   mld::CSR a = make_csr(n, irp, ja, val);
@@ -387,7 +384,7 @@ extern "C" int mldp_descr(const mldp_prec *p, char *buf, int len) {
     opc += (double)L.A.nnz();
     std::snprintf(line, sizeof line,
                   "  level %zu: rows %d nnz %lld  smoother %s sweeps %d/%d%s", l, L.A.nr,
-                  (long long)L.A.nnz(), L.kind == mld::SM_BJAC ? "BJAC-ILU(0)" : "JACOBI",
+                  (long long)L.A.nnz(), L.kind == mld::SM_BJAC ? "BJAC-ILU(0)" : (L.kind == mld::SM_FBGS ? "FBGS" : "JACOBI"),
                   L.sweeps_pre, L.sweeps_post, l ? "" : "\n");
     s += line;
     if (l) {

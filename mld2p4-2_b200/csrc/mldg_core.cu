@@ -366,13 +366,20 @@ struct EngineT : Engine {
     DCSR<T> A, AT, P, R, ND, NDT;
     DTri<T> L, U, Lt, Ut;
     T *d = nullptr;
-    T *x = nullptr, *y = nullptr, *ty = nullptr, *tw = nullptr, *bufA = nullptr, *bufB = nullptr;
+    // ty: residual of the cycle; tz, tw: smoother iterates (never aliasing
+    // the smoother's input, which may be ty)
+    T *x = nullptr, *y = nullptr, *ty = nullptr, *tw = nullptr, *tz = nullptr, *bufA = nullptr, *bufB = nullptr;
     // K-wide (row-interleaved) counterparts for the multi-RHS V-cycle
-    T *xm = nullptr, *ym = nullptr, *tym = nullptr, *twm = nullptr, *bufAm = nullptr, *bufBm = nullptr;
+    T *xm = nullptr, *ym = nullptr, *tym = nullptr, *twm = nullptr, *tzm = nullptr, *bufAm = nullptr,
+      *bufBm = nullptr;
     // windowed cluster solves (k_trsv_win) for both factors of each pair
     bool win = false;
     // single-vector solves through the ELL kernel (k_trsv_ell, K = 1) instead
     bool ell1 = false;
+    // FBGS: unscaled strict triangles for sweeps > 1, and which exchange
+    // buffer the next single solve writes (one-column and K-column forms)
+    DCSR<T> GL, GU;
+    int gflip = 0, gflip_m = 0;
     DWin<T> wL, wU, wUt, wLt;
     // coarsest level: explicit inverse of its ILU(0) factorisation (and its transpose)
     T *minv = nullptr, *minvT = nullptr;
@@ -475,15 +482,25 @@ struct EngineT : Engine {
     MLDG_CUDA(cudaEventCreate(&e0));
     MLDG_CUDA(cudaEventCreate(&e1));
     for (auto &L : lv) {
-      if (L.kind != MLDG_SMOOTHER_BJAC || L.minv || !L.L.ell[0].ok || !L.U.ell[0].ok || !L.Ut.ell[0].ok ||
-          !L.Lt.ell[0].ok)
+      const bool gs = L.kind == MLDG_SMOOTHER_FBGS;
+      if ((L.kind != MLDG_SMOOTHER_BJAC && !gs) || L.minv || !L.L.ell[0].ok || !L.U.ell[0].ok ||
+          (!gs && (!L.Ut.ell[0].ok || !L.Lt.ell[0].ok)))
         continue;
+      // the timed operation: the ILU solve pair, or a forward + backward GS solve
+      auto op = [&]() {
+        if (gs) {
+          fbgs_solve(L, false, L.x, L.ty, T(0));
+          fbgs_solve(L, true, L.x, L.ty, T(0));
+        } else {
+          ilu_apply(L, 'N', L.x, T(0), L.ty);
+        }
+      };
       float best[2] = {1e30f, 1e30f};
       for (int v = 0; v < 2; ++v) {
         L.ell1 = v == 1;
-        ilu_apply(L, 'N', L.x, T(0), L.ty);  // warm
+        op();  // warm
         MLDG_CUDA(cudaEventRecord(e0, st));
-        for (int r = 0; r < reps; ++r) ilu_apply(L, 'N', L.x, T(0), L.ty);
+        for (int r = 0; r < reps; ++r) op();
         MLDG_CUDA(cudaEventRecord(e1, st));
         MLDG_CUDA(cudaEventSynchronize(e1));
         MLDG_CUDA(cudaEventElapsedTime(&best[v], e0, e1));
@@ -580,8 +597,48 @@ struct EngineT : Engine {
     }
   }
 
+  // One GS solve out = (D+L)^{-1} rhs (forward) or (D+U)^{-1} rhs (backward)
+  // [+ beta*out] on the scaled unit-triangular factors.  Single solves
+  // alternate the two exchange buffers (the solve leaves its own buffer
+  // holding values and the other one reset); end_fbgs() restores the start
+  // state at the end of a recorded cycle.
+  void fbgs_solve(Lev &L, bool backward, const T *rhs, T *out, T beta) {
+    const DTri<T> &t = backward ? L.U : L.L;
+    T *cur = L.gflip ? L.bufB : L.bufA, *other = L.gflip ? L.bufA : L.bufB;
+    L.gflip ^= 1;
+    if (L.ell1)
+      trsv_ell1(t, rhs, L.d, cur, other, out, T(1), beta);
+    else
+      trsv(t, rhs, L.d, cur, other, out, T(1), beta);
+  }
+  void end_fbgs() {
+    for (auto &L : lv)
+      if (L.kind == MLDG_SMOOTHER_FBGS && L.gflip) {
+        fill(L.n, Sentinel<T>::value(), L.bufA);
+        L.gflip = 0;
+      }
+  }
+  // jac smoother + GS solver: sweeps forward (pre, sm) or backward (post,
+  // sm2) Gauss-Seidel sweeps from a zero start; y = S(x) + beta*y
+  void fbgs_smoother(Lev &L, bool post, const T *x, T beta, T *y, int sweeps) {
+    if (sweeps == 1) {
+      fbgs_solve(L, post, x, y, beta);
+      return;
+    }
+    fbgs_solve(L, post, x, L.tz, T(0));
+    for (int s = 1; s < sweeps; ++s) {
+      spmv(post ? L.GL : L.GU, L.tz, T(-1), x, T(1), L.tw, T(0));  // wv = x - (U|L) xit
+      fbgs_solve(L, post, L.tw, L.tz, T(0));
+    }
+    k_axpby_impl(L.n, L.tz, beta, y);
+  }
+
   // jac smoother apply with init 'Z': y = alpha*S^sweeps(x) + beta*y, alpha = 1
-  void smoother(Lev &L, char trans, const T *x, T beta, T *y, int sweeps) {
+  void smoother(Lev &L, char trans, const T *x, T beta, T *y, int sweeps, bool post = false) {
+    if (L.kind == MLDG_SMOOTHER_FBGS) {
+      fbgs_smoother(L, post, x, beta, y, sweeps);
+      return;
+    }
     const DCSR<T> &ND = (trans == 'N') ? L.ND : L.NDT;
     if (L.kind == MLDG_SMOOTHER_BJAC) {
       if (sweeps == 1 || L.nnz_nd == 0) {
@@ -590,12 +647,12 @@ struct EngineT : Engine {
       }
       // block-Jacobi sweeps with a non-empty off-block part (several ranks'
       // worth of blocks): ty = S(x); ty = S(x - ND ty) ...; y = ty + beta*y
-      ilu_apply(L, trans, x, T(0), L.ty);
+      ilu_apply(L, trans, x, T(0), L.tz);
       for (int s = 1; s < sweeps; ++s) {
-        spmv(ND, L.ty, T(-1), x, T(1), L.tw, T(0));
-        ilu_apply(L, trans, L.tw, T(0), L.ty);
+        spmv(ND, L.tz, T(-1), x, T(1), L.tw, T(0));
+        ilu_apply(L, trans, L.tw, T(0), L.tz);
       }
-      k_axpby_impl(L.n, L.ty, beta, y);
+      k_axpby_impl(L.n, L.tz, beta, y);
       return;
     }
     // point Jacobi (diag solver)
@@ -606,7 +663,7 @@ struct EngineT : Engine {
     }
     // sweeps >= 2: first sweep folded into the second (ty = w*d o x on the fly)
     T *src = nullptr;
-    T *bufs[2] = {L.ty, L.tw};
+    T *bufs[2] = {L.tz, L.tw};
     for (int s = 1; s < sweeps; ++s) {
       const bool last = (s == sweeps - 1);
       T *dst = last ? y : bufs[s & 1];
@@ -627,7 +684,7 @@ struct EngineT : Engine {
       Lev &C = lv[l + 1];
       const DCSR<T> &A = (trans == 'N') ? L.A : L.AT;
       if (pre) {
-        smoother(L, trans, L.x, T(0), L.y, trans == 'N' ? L.spre : L.spost);
+        smoother(L, trans, L.x, T(0), L.y, trans == 'N' ? L.spre : L.spost, trans != 'N');
         spmv(A, L.y, T(-1), L.x, T(1), L.ty, T(0));    // ty = x - op(A) y
         spmv(C.R, L.ty, T(1), nullptr, T(0), C.x, T(0));  // x_{l+1} = R ty
       } else {
@@ -639,7 +696,7 @@ struct EngineT : Engine {
       prolong(C, L.y);                                   // y += P y_{l+1}
       if (post) {
         spmv(A, L.y, T(-1), L.x, T(1), L.ty, T(0));
-        smoother(L, trans, L.ty, T(1), L.y, trans == 'N' ? L.spost : L.spre);
+        smoother(L, trans, L.ty, T(1), L.y, trans == 'N' ? L.spost : L.spre, trans == 'N');
       }
     } else {
       smoother(L, trans, L.x, T(0), L.y, L.spre);
@@ -854,7 +911,7 @@ struct EngineT : Engine {
     if (Kw > mcap) {
       marena.release();
       for (auto &L : lv) {
-        L.xm = L.ym = L.tym = L.twm = L.bufAm = L.bufBm = nullptr;
+        L.xm = L.ym = L.tym = L.twm = L.tzm = L.bufAm = L.bufBm = nullptr;
         for (DTri<T> *t : {&L.L, &L.U, &L.Ut, &L.Lt})
           for (int q = 1; q < 6; ++q) {  // [0] (one column) lives in the main arena
             t->blkm[q] = nullptr;
@@ -879,11 +936,13 @@ struct EngineT : Engine {
           L.ym = marena.alloc<T>(n);
         }
         L.tym = marena.alloc<T>(n);
+        L.tzm = marena.alloc<T>(n);
+        MLDG_CUDA(cudaMemsetAsync(L.tzm, 0, sizeof(T) * n, st));
         L.twm = marena.alloc<T>(n);
         MLDG_CUDA(cudaMemsetAsync(L.ym, 0, sizeof(T) * n, st));
         MLDG_CUDA(cudaMemsetAsync(L.tym, 0, sizeof(T) * n, st));
         MLDG_CUDA(cudaMemsetAsync(L.twm, 0, sizeof(T) * n, st));
-        if (L.kind == MLDG_SMOOTHER_BJAC && !L.minv) {
+        if ((L.kind == MLDG_SMOOTHER_BJAC || L.kind == MLDG_SMOOTHER_FBGS) && !L.minv) {
           // exchange buffers start as all-sentinel (bufAm stays so after every solve pair)
           L.bufAm = marena.alloc<T>(n);
           L.bufBm = marena.alloc<T>(n);
@@ -895,8 +954,9 @@ struct EngineT : Engine {
     }
     const int ki = ilog2(Kw);
     for (auto &L : lv) {
-      if (L.kind != MLDG_SMOOTHER_BJAC || L.minv) continue;
+      if ((L.kind != MLDG_SMOOTHER_BJAC && L.kind != MLDG_SMOOTHER_FBGS) || L.minv) continue;
       for (DTri<T> *t : {&L.L, &L.U, &L.Ut, &L.Lt}) {
+        if (!t->present() && L.kind == MLDG_SMOOTHER_FBGS) continue;
         if (!t->present()) fail(MLDG_ERR_INTERNAL, "multi-RHS solve without a level schedule");
         if (!t->blkm[ki]) {
           build_blk_m(*t, Kw);
@@ -1031,20 +1091,54 @@ struct EngineT : Engine {
       trsv_m(L.Lt, L.bufAm, L.d, L.bufBm, L.bufAm, y, T(1), beta);
     }
   }
+  // K-wide fbgs_solve / end_fbgs / fbgs_smoother
+  void fbgs_solve_m(Lev &L, bool backward, const T *rhs, T *out, T beta) {
+    DTri<T> &t = backward ? L.U : L.L;
+    T *cur = L.gflip_m ? L.bufBm : L.bufAm, *other = L.gflip_m ? L.bufAm : L.bufBm;
+    L.gflip_m ^= 1;
+    trsv_m(t, rhs, L.d, cur, other, out, T(1), beta);
+  }
+  void end_fbgs_m() {
+    for (auto &L : lv)
+      if (L.kind == MLDG_SMOOTHER_FBGS && L.gflip_m) {
+        // the whole allocated width: every K keeps bufAm all-sentinel
+        begin(MLDG_KERNEL_VEC);
+        const int64_t nn = (int64_t)std::max(L.n, 1) * mcap;
+        k_fill<T><<<blocks_for(nn), 256, 0, st>>>((int)nn, Sentinel<T>::value(), L.bufAm);
+        end(nn * (int64_t)sizeof(T));
+        L.gflip_m = 0;
+      }
+  }
+  void fbgs_smoother_m(Lev &L, bool post, const T *x, T beta, T *y, int sweeps) {
+    if (sweeps == 1) {
+      fbgs_solve_m(L, post, x, y, beta);
+      return;
+    }
+    fbgs_solve_m(L, post, x, L.tzm, T(0));
+    for (int s = 1; s < sweeps; ++s) {
+      spmm(post ? L.GL : L.GU, L.tzm, T(-1), x, T(1), L.twm, T(0));
+      fbgs_solve_m(L, post, L.twm, L.tzm, T(0));
+    }
+    axpby_m(L.n, L.tzm, beta, y);
+  }
   // the single-vector smoother() with K-wide kernels
-  void smoother_m(Lev &L, char trans, const T *x, T beta, T *y, int sweeps) {
+  void smoother_m(Lev &L, char trans, const T *x, T beta, T *y, int sweeps, bool post = false) {
+    if (L.kind == MLDG_SMOOTHER_FBGS) {
+      fbgs_smoother_m(L, post, x, beta, y, sweeps);
+      return;
+    }
     const DCSR<T> &ND = (trans == 'N') ? L.ND : L.NDT;
     if (L.kind == MLDG_SMOOTHER_BJAC) {
       if (sweeps == 1 || L.nnz_nd == 0) {
         ilu_apply_m(L, trans, x, beta, y);
         return;
       }
-      ilu_apply_m(L, trans, x, T(0), L.tym);
+      ilu_apply_m(L, trans, x, T(0), L.tzm);
       for (int s = 1; s < sweeps; ++s) {
-        spmm(ND, L.tym, T(-1), x, T(1), L.twm, T(0));
-        ilu_apply_m(L, trans, L.twm, T(0), L.tym);
+        spmm(ND, L.tzm, T(-1), x, T(1), L.twm, T(0));
+        ilu_apply_m(L, trans, L.twm, T(0), L.tzm);
       }
-      axpby_m(L.n, L.tym, beta, y);
+      axpby_m(L.n, L.tzm, beta, y);
       return;
     }
     const T w = (T)L.damp;
@@ -1053,7 +1147,7 @@ struct EngineT : Engine {
       return;
     }
     T *src = nullptr;
-    T *bufs[2] = {L.tym, L.twm};
+    T *bufs[2] = {L.tzm, L.twm};
     for (int s = 1; s < sweeps; ++s) {
       const bool last = (s == sweeps - 1);
       T *dst = last ? y : bufs[s & 1];
@@ -1086,7 +1180,7 @@ struct EngineT : Engine {
       Lev &C = lv[l + 1];
       const DCSR<T> &A = (trans == 'N') ? L.A : L.AT;
       if (pre) {
-        smoother_m(L, trans, L.xm, T(0), L.ym, trans == 'N' ? L.spre : L.spost);
+        smoother_m(L, trans, L.xm, T(0), L.ym, trans == 'N' ? L.spre : L.spost, trans != 'N');
         spmm(A, L.ym, T(-1), L.xm, T(1), L.tym, T(0));
         spmm(C.R, L.tym, T(1), nullptr, T(0), C.xm, T(0));
       } else {
@@ -1098,7 +1192,7 @@ struct EngineT : Engine {
       prolong_m(C, L.ym);
       if (post) {
         spmm(A, L.ym, T(-1), L.xm, T(1), L.tym, T(0));
-        smoother_m(L, trans, L.tym, T(1), L.ym, trans == 'N' ? L.spost : L.spre);
+        smoother_m(L, trans, L.tym, T(1), L.ym, trans == 'N' ? L.spost : L.spre, trans == 'N');
       }
     } else {
       smoother_m(L, trans, L.xm, T(0), L.ym, L.spre);
@@ -1119,10 +1213,21 @@ struct EngineT : Engine {
       k_cast<double, T><<<blocks_for(n), 256, 0, st>>>((int)n, xin_m, F.xm);
       end(n * (8 + (int64_t)sizeof(T)));
     }
-    if (lv.size() == 1)
+    if (lv.size() == 1 && F.kind == MLDG_SMOOTHER_FBGS) {
+      const int nsw = std::max(F.spre, F.spost);
+      const T *src = F.xm;
+      for (int k = 0; k < nsw; ++k) {
+        fbgs_solve_m(F, false, src, F.tym, T(0));
+        fbgs_solve_m(F, true, F.tym, k == nsw - 1 ? F.ym : F.twm, T(0));
+        src = F.twm;
+      }
+      if (nsw == 0) axpby_m(F.n, F.xm, T(0), F.ym);
+    } else if (lv.size() == 1) {
       smoother_m(F, trans, F.xm, T(0), F.ym, F.spre);
-    else
+    } else {
       vcycle_m(0, trans);
+    }
+    end_fbgs_m();
     if (!std::is_same<T, double>::value) {
       cur_lev = 0;
       begin(MLDG_KERNEL_VEC);
@@ -1203,10 +1308,22 @@ struct EngineT : Engine {
       k_cast<double, T><<<blocks_for(F.n), 256, 0, st>>>(F.n, xin, F.x);
       end((int64_t)F.n * (8 + sizeof(T)));
     }
-    if (lv.size() == 1)
+    if (lv.size() == 1 && F.kind == MLDG_SMOOTHER_FBGS) {
+      // one level: nswps times forward then backward GS, one sweep each
+      const int nsw = std::max(F.spre, F.spost);
+      const T *src = F.x;
+      for (int k = 0; k < nsw; ++k) {
+        fbgs_solve(F, false, src, F.ty, T(0));
+        fbgs_solve(F, true, F.ty, k == nsw - 1 ? F.y : F.tw, T(0));
+        src = F.tw;
+      }
+      if (nsw == 0) k_axpby_impl(F.n, F.x, T(0), F.y);
+    } else if (lv.size() == 1) {
       smoother(F, trans, F.x, T(0), F.y, F.spre);
-    else
+    } else {
       vcycle(0, trans);
+    }
+    end_fbgs();
     if (!std::is_same<T, double>::value) {
       cur_lev = 0;
       begin(MLDG_KERNEL_VEC);
@@ -1249,6 +1366,7 @@ void EngineT<float>::prolong(Lev &C, float *y) {
 // ---------------------------------------------------------------------------
 struct Handle {
   mldg_opts opts{};
+  bool has_fbgs = false;  // a Gauss-Seidel level: trans 'T' is rejected
   std::string last_error;
   std::vector<HostLevel> host;
   int nlev = 0;
@@ -1291,6 +1409,12 @@ struct Handle {
   cudaGraphExec_t kgraph[2][2] = {};
   int64_t kglaunch[2][2] = {};
 };
+
+// the GS solvers accept trans = 'N' only (mld_d_gs_solver_apply_vect.f90:68-75)
+static void check_trans(const Handle *h, char trans) {
+  if (trans != 'N' && h->has_fbgs)
+    fail(MLDG_ERR_TRANS, "trans '%c': the Gauss-Seidel smoother (FBGS) applies with trans 'N' only", trans);
+}
 
 static void drop_krylov_graphs(Handle *h) {
   for (int m = 0; m < 2; ++m)
@@ -1852,6 +1976,24 @@ static Engine *make_engine(Handle *h) {
                        ts[q]->smem, ts[q]->grid);
       }
     }
+    std::vector<double> dh = H.d;
+    if (H.kind == MLDG_SMOOTHER_FBGS) {
+      // (D+L)^{-1} and (D+U)^{-1} as unit-triangular solves of the rows
+      // scaled by 1/a_ii, the right-hand side scaled by 1/a_ii
+      for (double &v : dh) v = 1.0 / v;
+      HostCSR Ls = H.L, Us = H.U;
+      for (int i = 0; i < Ls.nr; ++i) {
+        for (int k = Ls.irp[i]; k < Ls.irp[i + 1]; ++k) Ls.val[k] *= dh[i];
+        for (int k = Us.irp[i]; k < Us.irp[i + 1]; ++k) Us.val[k] *= dh[i];
+      }
+      L.L = build_tri_dev<T>(ar, Ls, false, h->nsm);
+      L.U = build_tri_dev<T>(ar, Us, true, h->nsm);
+      if (std::max(H.sweeps_pre, H.sweeps_post) > 1) {
+        // later sweeps: wv = x - U xit (forward) / x - L xit (backward)
+        L.GU = to_dev<T>(ar, H.U);
+        L.GL = to_dev<T>(ar, H.L);
+      }
+    }
     if (H.ND.present() && L.nnz_nd > 0) {
       L.ND = to_dev<T>(ar, H.ND);
       L.NDT = to_dev<T>(ar, transpose(H.ND));
@@ -1864,7 +2006,7 @@ static Engine *make_engine(Handle *h) {
       L.minv = ar.upload(m);
       L.minvT = ar.upload(mt);
     }
-    std::vector<T> dv(H.d.begin(), H.d.end());
+    std::vector<T> dv(dh.begin(), dh.end());
     L.d = ar.upload(dv);
     const int n = std::max(L.n, 1);
     if (l == 0 && std::is_same<T, double>::value) {
@@ -1875,11 +2017,13 @@ static Engine *make_engine(Handle *h) {
       L.y = ar.alloc<T>(n);
     }
     L.ty = ar.alloc<T>(n);
+    L.tz = ar.alloc<T>(n);
+    MLDG_CUDA(cudaMemset(L.tz, 0, sizeof(T) * n));
     L.tw = ar.alloc<T>(n);
     MLDG_CUDA(cudaMemset(L.y, 0, sizeof(T) * n));
     MLDG_CUDA(cudaMemset(L.ty, 0, sizeof(T) * n));
     MLDG_CUDA(cudaMemset(L.tw, 0, sizeof(T) * n));
-    if (H.kind == MLDG_SMOOTHER_BJAC) {
+    if (H.kind == MLDG_SMOOTHER_BJAC || H.kind == MLDG_SMOOTHER_FBGS) {
       L.bufA = ar.alloc<T>(n);
       L.bufB = ar.alloc<T>(n);
       k_fill<T><<<64, 256, 0, h->st>>>(n, Sentinel<T>::value(), L.bufA);
@@ -1887,6 +2031,7 @@ static Engine *make_engine(Handle *h) {
       if (!L.minv) {
         bool ok = true;
         for (DTri<T> *f : {&L.L, &L.U, &L.Ut, &L.Lt}) {
+          if (!f->present()) continue;  // FBGS: forward and backward factors only
           e->build_ell(*f, 1, ar);
           ok = ok && f->ell[0].ok;
         }
@@ -1921,7 +2066,7 @@ static void check_level(const HostLevel &H, int l, const HostLevel *prev) {
     if (H.R.nr != n || H.R.nc != nf) fail(MLDG_ERR_ARG, "level %d: R must be %d x %d", l, n, nf);
   }
   if ((int)H.d.size() != n) fail(MLDG_ERR_NO_DIAG, "level %d: missing d (length %d)", l, n);
-  if (H.kind == MLDG_SMOOTHER_BJAC) {
+  if (H.kind == MLDG_SMOOTHER_BJAC || H.kind == MLDG_SMOOTHER_FBGS) {
     if (!H.L.present() || !H.U.present()) fail(MLDG_ERR_NO_SOLVER, "level %d: missing L/U", l);
     if (H.L.nr != n || H.U.nr != n) fail(MLDG_ERR_ARG, "level %d: L/U size", l);
     for (int i = 0; i < n; ++i) {
@@ -1930,6 +2075,9 @@ static void check_level(const HostLevel &H, int l, const HostLevel *prev) {
       for (int k = H.U.irp[i]; k < H.U.irp[i + 1]; ++k)
         if (H.U.ja[k] <= i) fail(MLDG_ERR_ARG, "level %d: U not strictly upper at row %d", l, i);
     }
+    if (H.kind == MLDG_SMOOTHER_FBGS)
+      for (int i = 0; i < n; ++i)
+        if (H.d[i] == 0.0) fail(MLDG_ERR_NO_DIAG, "level %d: zero diagonal at row %d (Gauss-Seidel)", l, i);
   } else if (H.kind != MLDG_SMOOTHER_JACOBI) {
     fail(MLDG_ERR_ARG, "level %d: unknown smoother kind %d", l, H.kind);
   }
@@ -1957,6 +2105,8 @@ static void finalize(Handle *h, int nlev, int precision) {
   h->karena.release();
   h->kcap = 0;
   h->nlev = nlev;
+  h->has_fbgs = false;
+  for (int l = 0; l < nlev; ++l) h->has_fbgs = h->has_fbgs || h->host[l].kind == MLDG_SMOOTHER_FBGS;
   h->precision = precision;
   h->n0 = h->host[0].A.nr;
   const int n0 = std::max(h->n0, 1);
@@ -2128,6 +2278,7 @@ static void apply(Handle *h, const double *x, double *y, char trans, int nrhs, i
   if (!h->finalized) fail(MLDG_ERR_NOT_BUILT, "apply before build (mldg_finalize not called)");
   if (trans == 'C') trans = 'T';
   if (trans != 'N' && trans != 'T') fail(MLDG_ERR_TRANS, "invalid trans '%c'", trans);
+  check_trans(h, trans);
   if (nrhs < 0) fail(MLDG_ERR_ARG, "nrhs < 0");
   const int n = h->n0;
   if (nrhs > 1 && ld < n) fail(MLDG_ERR_SIZE, "ld %d < n %d", ld, n);
@@ -2213,6 +2364,7 @@ static void krylov(Handle *h, int method, const mldg_csr *Acsr, const double *b,
   if (!h->finalized) fail(MLDG_ERR_NOT_BUILT, "krylov before build");
   if (method != 0 && method != 1) fail(MLDG_ERR_ARG, "method must be 0 (CG) or 1 (FCG)");
   if (!b || !x) fail(MLDG_ERR_ARG, "null vector");
+  check_trans(h, trans);
   if (itmax < 0) fail(MLDG_ERR_ARG, "itmax < 0");
   const int n = h->n0;
   DCSR<double> A = h->A0;
@@ -2802,6 +2954,7 @@ static void profile_run(Handle &h, char trans, int nrhs, int max, mldg_kernel_st
   if (!h.finalized) mldg::fail(MLDG_ERR_NOT_BUILT, "profile before build");
   if (trans == 'C') trans = 'T';
   if (trans != 'N' && trans != 'T') mldg::fail(MLDG_ERR_TRANS, "invalid trans");
+  mldg::check_trans(&h, trans);
   if (nrhs < 1 || nrhs > 32) mldg::fail(MLDG_ERR_ARG, "profile width must be 1..32");
   const int K = nrhs > 1 ? mldg::width_for(nrhs) : 1;
   if (K > 1) mldg::prepare_multi(&h, K);

@@ -32,11 +32,12 @@ typedef struct {
   int *ilaggr;     /* aggregate of each row of the previous level */
   int naggr;
   double omega;
-  int smoother;    /* ORC_JACOBI / ORC_BJAC */
+  int smoother;    /* ORC_JACOBI / ORC_BJAC / ORC_FBGS */
   int sweeps_pre, sweeps_post;
   double damp;
-  csr L, U;        /* ILU(0): unit lower / unit upper (U rows scaled by 1/pivot) */
-  double *d;       /* ILU(0): 1/pivot */
+  csr L, U;        /* ILU(0): unit lower / unit upper (U rows scaled by 1/pivot);
+                      FBGS: the strict lower / strict upper triangles of A */
+  double *d;       /* ILU(0): 1/pivot; FBGS: the diagonal a_ii */
   double *dinv;    /* diag solver: 1/a_ii (0 -> 1) */
   csr ND;          /* jac smoother off-(block-)diagonal part */
   long nnz_nd;
@@ -549,6 +550,33 @@ static void diag_apply(const level *lv, double alpha, const double *x,
                          : alpha * (lv->dinv[i] * x[i]) + beta * y[i];
 }
 
+/* One Gauss-Seidel sweep of the GS solver (forward: wv = x - U xit,
+ * xit = (D+L)^{-1} wv; mlprec/impl/solver/mld_d_gs_solver_apply_vect.f90:143-158)
+ * or of the BWGS solver (backward: wv = x - L xit, xit = (D+U)^{-1} wv;
+ * mld_d_bwgs_solver_apply_vect.f90:150-156).  The triangular solve with a
+ * non-unit diagonal sums the row from zero, subtracts, divides by a_ii. */
+static void gs_sweep(const level *lv, int backward, const double *x, double *xit,
+                     double *wv) {
+  int n = lv->A.nr;
+  const csr *off = backward ? &lv->L : &lv->U;
+  const csr *tri = backward ? &lv->U : &lv->L;
+  memcpy(wv, x, sizeof(double) * (size_t)n);
+  spmv_op(off, 'N', -1.0, xit, 1.0, wv);
+  if (!backward) {
+    for (int i = 0; i < n; i++) {
+      double s = 0.0;
+      for (int k = tri->irp[i]; k < tri->irp[i + 1]; k++) s = s + tri->val[k] * xit[tri->ja[k]];
+      xit[i] = (wv[i] - s) / lv->d[i];
+    }
+  } else {
+    for (int i = n - 1; i >= 0; i--) {
+      double s = 0.0;
+      for (int k = tri->irp[i]; k < tri->irp[i + 1]; k++) s = s + tri->val[k] * xit[tri->ja[k]];
+      xit[i] = (wv[i] - s) / lv->d[i];
+    }
+  }
+}
+
 static void solver_apply(const level *lv, char trans, double alpha,
                          const double *x, double beta, double *y, double *w1,
                          double *w2) {
@@ -564,11 +592,21 @@ static void solver_apply(const level *lv, char trans, double alpha,
  * reference iteration exactly. */
 static void jac_smoother_apply(orc_prec *p, int l, char trans, double alpha,
                                const double *x, double beta, double *y,
-                               int sweeps) {
+                               int sweeps, int post) {
   level *lv = &p->lv[l];
   int n = lv->A.nr;
   double *tx = p->tx[l], *ty2 = p->w1[l];
   double *wa = p->wa[l], *wb = p->wb[l];
+  if (lv->smoother == ORC_FBGS) {
+    /* GS solvers are iterative: always the general branch (:117-177).
+     * init Z, then sweeps-1 more sweeps from the previous iterate; the
+     * off-block part ND is empty on one rank (tx = x).  Pre smoother sm:
+     * forward GS; post smoother sm2: backward GS (onelev_cseti.F90:128-132). */
+    memset(ty2, 0, sizeof(double) * (size_t)n);
+    for (int s = 0; s < sweeps; s++) gs_sweep(lv, post, x, ty2, wa);
+    axpby(n, alpha, ty2, beta, y);
+    return;
+  }
   if (sweeps == 1 || lv->nnz_nd == 0) {
     /* single solver application (:107-109); the diag solver is not iterative */
     if (lv->smoother == ORC_JACOBI && lv->damp != 1.0)
@@ -606,7 +644,7 @@ static void inner_mult(orc_prec *p, int l, char trans) {
     if (pre) {
       /* (:644-664) sm (N) / sm2 (T); init Z, beta 0 */
       jac_smoother_apply(p, l, trans, 1.0, x, 0.0, y,
-                         trans == 'N' ? spre : spost);
+                         trans == 'N' ? spre : spost, trans == 'N' ? 0 : 1);
       /* residual (:669-676) and restriction (:682-684) */
       memcpy(ty, x, sizeof(double) * (size_t)n);
       spmv_op(&lv->A, trans, -1.0, y, 1.0, ty);
@@ -624,11 +662,11 @@ static void inner_mult(orc_prec *p, int l, char trans) {
       memcpy(ty, x, sizeof(double) * (size_t)n);
       spmv_op(&lv->A, trans, -1.0, y, 1.0, ty); /* (:748-755) */
       jac_smoother_apply(p, l, trans, 1.0, ty, 1.0, y,
-                         trans == 'N' ? spost : spre); /* (:765-777) */
+                         trans == 'N' ? spost : spre, trans == 'N' ? 1 : 0); /* (:765-777) */
     }
   } else {
     /* coarsest level (:787-793) */
-    jac_smoother_apply(p, l, trans, 1.0, x, 0.0, y, spre);
+    jac_smoother_apply(p, l, trans, 1.0, x, 0.0, y, spre, 0);
   }
 }
 
@@ -720,6 +758,41 @@ static int smoother_build(level *lv, int kind, int spre, int spost, double damp)
     lv->dinv = csr_diag(a);
     for (int i = 0; i < n; i++)
       lv->dinv[i] = (lv->dinv[i] == 0.0) ? 1.0 : 1.0 / lv->dinv[i];
+    return 0;
+  }
+  if (kind == ORC_FBGS) {
+    /* GS / BWGS solvers (mld_d_gs_solver_bld.f90:73-81: tril with the
+     * diagonal + the rest): kept here as strict lower L, strict upper U and
+     * the diagonal d; ND is empty on one rank */
+    long nl = 0, nu = 0;
+    for (int i = 0; i < n; i++)
+      for (int k = a->irp[i]; k < a->irp[i + 1]; k++) {
+        if (a->ja[k] < i) nl++;
+        if (a->ja[k] > i) nu++;
+      }
+    csr_alloc(&lv->L, n, n, nl);
+    csr_alloc(&lv->U, n, n, nu);
+    lv->d = (double *)xcalloc((size_t)n, sizeof(double));
+    long tl = 0, tu = 0;
+    for (int i = 0; i < n; i++) {
+      for (int k = a->irp[i]; k < a->irp[i + 1]; k++) {
+        int j = a->ja[k];
+        if (j < i) {
+          lv->L.ja[tl] = j;
+          lv->L.val[tl++] = a->val[k];
+        } else if (j > i) {
+          lv->U.ja[tu] = j;
+          lv->U.val[tu++] = a->val[k];
+        } else {
+          lv->d[i] = a->val[k];
+        }
+      }
+      lv->L.irp[i + 1] = (int)tl;
+      lv->U.irp[i + 1] = (int)tu;
+      if (lv->d[i] == 0.0) return 1; /* zero diagonal: the GS solve divides by it */
+    }
+    csr_alloc(&lv->ND, n, a->nc, 0);
+    lv->nnz_nd = 0;
     return 0;
   }
   /* BJAC + ILU(0): on one rank the off-block part (columns > nrow) is empty */
@@ -876,13 +949,29 @@ int orc_prec_level_vec(const orc_prec *p, int l, int which, double *dv, int *iv)
 int orc_prec_apply(orc_prec *p, const double *x, double *y, char trans) {
   if (!p || p->nlev < 1) return 3112; /* apply before build */
   if (trans != 'N' && trans != 'T') return 1;
+  /* the GS solvers accept trans = 'N' only (mld_d_gs_solver_apply_vect.f90:68-75) */
+  for (int l = 0; l < p->nlev; l++)
+    if (p->lv[l].smoother == ORC_FBGS && trans != 'N') return 40;
   int n = p->lv[0].A.nr;
   memcpy(p->x2l[0], x, sizeof(double) * (size_t)n);
-  if (p->nlev == 1)
+  if (p->nlev == 1 && p->lv[0].smoother == ORC_FBGS) {
+    /* one-level symmetrized GS (mld_dprecaply.f90:374-409): nswps times
+     * w2 = sm(w1), w1 = sm2(w2), one sweep each; y = w1 */
+    level *lv = &p->lv[0];
+    int nswps = lv->sweeps_pre > lv->sweeps_post ? lv->sweeps_pre : lv->sweeps_post;
+    double *w1 = p->ty[0], *w2 = p->y2l[0];
+    memcpy(w1, x, sizeof(double) * (size_t)n);
+    for (int k = 0; k < nswps; k++) {
+      jac_smoother_apply(p, 0, 'N', 1.0, w1, 0.0, w2, 1, 0);
+      jac_smoother_apply(p, 0, 'N', 1.0, w2, 0.0, w1, 1, 1);
+    }
+    memcpy(p->y2l[0], w1, sizeof(double) * (size_t)n);
+  } else if (p->nlev == 1) {
     jac_smoother_apply(p, 0, trans, 1.0, p->x2l[0], 0.0, p->y2l[0],
-                       p->lv[0].sweeps_pre);
-  else
+                       p->lv[0].sweeps_pre, 0);
+  } else {
     inner_mult(p, 0, trans);
+  }
   memcpy(y, p->y2l[0], sizeof(double) * (size_t)n);
   return 0;
 }

@@ -24,10 +24,11 @@ extern "C" {
 #endif
 
 /* smoother / solver kinds (values follow mld_base_prec_type.F90 names) */
-enum { ORC_JACOBI = 1, ORC_BJAC = 2 };
+enum { ORC_JACOBI = 1, ORC_BJAC = 2, ORC_FBGS = 3 };
 
 typedef struct {
-  int smoother;        /* ORC_JACOBI: jac smoother + diag solver; ORC_BJAC: jac + ILU(0) */
+  int smoother;        /* ORC_JACOBI: jac smoother + diag solver; ORC_BJAC: jac + ILU(0);
+                          ORC_FBGS: jac + forward GS (pre) / backward GS (post) */
   int sweeps_pre;
   int sweeps_post;
   double jac_damp;     /* extension (not in the reference): 1.0 == reference Jacobi */

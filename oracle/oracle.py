@@ -18,6 +18,7 @@ _lib = None
 
 JACOBI = 1
 BJAC = 2
+FBGS = 3  # forward GS pre / backward GS post (jac smoother + GS / BWGS solvers)
 
 
 class Params(C.Structure):

@@ -47,7 +47,7 @@ ANISO = (1.0, 1.0, 0.01, S3, S3, S3, 0.0)
 
 
 def oracle_params(orc, smoother="BJAC", sweeps=1, damp=1.0, coarse_sweeps=4, mcs=2000):
-    sm = orc.BJAC if smoother == "BJAC" else orc.JACOBI
+    sm = {"BJAC": orc.BJAC, "JACOBI": orc.JACOBI, "FBGS": orc.FBGS}[smoother]
     return orc.default_params(smoother=sm, sweeps_pre=sweeps, sweeps_post=sweeps,
                               jac_damp=damp, coarse_solver=orc.BJAC,
                               coarse_sweeps=coarse_sweeps, min_coarse_size=mcs)
@@ -61,14 +61,15 @@ def upload_oracle_hierarchy(mld, orc, oprec, use_graphs=True, precision=0, autot
         def conv(m):
             return None if m is None else mld.CSR(m.irp, m.ja, m.val, ncols=m.ncols)
         kind = info["smoother"]
-        d = oprec.level_vec(l, "d") if kind == orc.BJAC else oprec.level_vec(l, "dinv")
+        tri = kind in (orc.BJAC, orc.FBGS)
+        d = oprec.level_vec(l, "d") if tri else oprec.level_vec(l, "dinv")
         h.upload_level(
             l, conv(oprec.level_csr(l, "A")),
             P=conv(oprec.level_csr(l, "P")) if l else None,
             R=conv(oprec.level_csr(l, "R")) if l else None,
             ND=conv(oprec.level_csr(l, "ND")) if info["nnzND"] else None,
-            L=conv(oprec.level_csr(l, "L")) if kind == orc.BJAC else None,
-            U=conv(oprec.level_csr(l, "U")) if kind == orc.BJAC else None,
+            L=conv(oprec.level_csr(l, "L")) if tri else None,
+            U=conv(oprec.level_csr(l, "U")) if tri else None,
             d=d, smoother=kind, sweeps_pre=info["sweeps_pre"], sweeps_post=info["sweeps_pre"],
             damping=info["damp"])
     h.finalize(oprec.nlev, precision)

@@ -43,12 +43,17 @@ def test_host_mirror_set_and_build_errors(mld):
     with pytest.raises(mld.MldError):
         p.set("NO_SUCH_KEY", 1)
     a = mld.gen_pde3d(6, 1)
-    # the reference's ML default smoother (FBGS) has no GPU apply
+    # the reference's ML default (FBGS smoother, ILU coarse solve) builds
+    p.hierarchy_build(a)
+    assert p.nlev >= 1
+    # a smoother without a GPU apply is refused with the keyword named
+    p.set("SMOOTHER_TYPE", "AS")
     with pytest.raises(mld.MldError) as e:
         p.hierarchy_build(a)
-    assert "FBGS" in str(e.value)
+    assert "SMOOTHER_TYPE" in str(e.value)
+    p.init("ML")
     p.set("SMOOTHER_TYPE", "BJAC")
-    p.set("ML_CYCLE", "WCYCLE")
+    p.set("ML_CYCLE", "KCYCLE")
     with pytest.raises(mld.MldError) as e:
         p.hierarchy_build(a)
     assert "ML_CYCLE" in str(e.value)

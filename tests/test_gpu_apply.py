@@ -21,7 +21,8 @@ def _rel(a, b):
 
 @pytest.mark.parametrize("idim,coef", [(8, ISO), (12, ISO), (16, ANISO), (28, ISO)])
 @pytest.mark.parametrize("smoother,sweeps,damp", [("BJAC", 1, 1.0), ("JACOBI", 2, 0.8),
-                                                  ("JACOBI", 1, 1.0), ("JACOBI", 3, 1.0)])
+                                                  ("JACOBI", 1, 1.0), ("JACOBI", 3, 1.0),
+                                                  ("JACOBI", 4, 0.9)])
 def test_apply_matches_oracle(mld, orc, idim, coef, smoother, sweeps, damp):
     a = orc.gen_pde3d(idim, 1, coef)
     op = orc.Prec(oracle_params(orc, smoother, sweeps, damp, mcs=200))
