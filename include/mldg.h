@@ -126,6 +126,15 @@ int mldg_upload_level(mldg_handle *h, int lev, const mldg_level_desc *desc);
  * (impl/mld_dprecbld.f90:60-159). */
 int mldg_finalize(mldg_handle *h, int nlev, int precision);
 
+/* Multilevel cycle of every later apply: MLDG_CYCLE_V (default) or
+ * MLDG_CYCLE_W, which repeats the coarse correction once from the updated
+ * residual before post-smoothing (mld_dmlprec_aply.f90:716-745).  May be
+ * called before or after mldg_finalize.  replaces: prec%set('ML_CYCLE',
+ * 'VCYCLE'|'WCYCLE') (mld_d_base_onelev_cseti.F90, ML_CYCLE). */
+#define MLDG_CYCLE_V 0
+#define MLDG_CYCLE_W 1
+int mldg_set_cycle(mldg_handle *h, int cycle);
+
 /* y = M^{-1} x (trans 'N') or y = M^{-T} x (trans 'T'/'C') for nrhs vectors
  * stored column by column with leading dimension ld (ld >= n).
  * mem_kind: MLDG_MEM_HOST or MLDG_MEM_DEVICE for both x and y.

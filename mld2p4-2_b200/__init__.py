@@ -28,6 +28,8 @@ _lib = None
 # smoother kinds / precision forms / memory kinds (include/mldg.h)
 SMOOTHER_JACOBI = 1
 SMOOTHER_BJAC = 2
+SMOOTHER_FBGS = 3
+CYCLE_V, CYCLE_W = 0, 1
 PREC_FP64, PREC_FP32, PREC_FP32_P16 = 0, 1, 2
 MEM_HOST, MEM_DEVICE = 0, 1
 
@@ -180,6 +182,7 @@ def lib():
                                         C.POINTER(C.c_void_p), C.c_double, C.c_int,
                                         C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_int,
                                         C.POINTER(C.c_double)]
+        L.mldg_set_cycle.argtypes = [vp, C.c_int]
         L.mldg_level_info.argtypes = [vp, C.c_int, C.POINTER(C.c_int64)]
         L.mldg_last_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
         L.mldg_apply_bytes.argtypes = [vp, C.POINTER(C.c_int64)]
@@ -362,6 +365,10 @@ class Hierarchy(_GpuDiag):
         self._check(lib().mldg_upload_level(self._h, lev, C.byref(desc)))
         if lev == 0:
             self.n = A.nrows
+
+    def set_cycle(self, cycle: int):
+        """MLDG_CYCLE_V (0) or MLDG_CYCLE_W (1)."""
+        self._check(lib().mldg_set_cycle(self._h, cycle))
 
     def finalize(self, nlev: int, precision: int = PREC_FP64):
         self._check(lib().mldg_finalize(self._h, nlev, precision))

@@ -22,6 +22,7 @@ struct mldp_prec {
   mld::Parms parms;
   std::string unsupported;      // first unsupported setting, reported at build
   int precision = MLDG_PREC_FP64;
+  int cycle = MLDG_CYCLE_V;
   std::vector<mld::Level> lv;
   bool hier_built = false, smoothers_built = false;
   mldg_handle *gpu = nullptr;
@@ -85,6 +86,7 @@ extern "C" int mldp_init(mldp_prec *p, const char *ptype) {
   p->hier_built = p->smoothers_built = false;
   p->unsupported.clear();
   p->precision = MLDG_PREC_FP64;
+  p->cycle = MLDG_CYCLE_V;
   if (t == "ML") {
     // mld_dprecinit.F90:188-207: VCYCLE, FBGS smoother, ILU coarse solver
     // (no UMFPACK/MUMPS/SuperLU): BJAC + ILU(0), replicated coarse matrix.
@@ -143,7 +145,12 @@ static int set_common(mldp_prec *p, const std::string &w, const std::string *sv,
     if (ival() != 0 && p->unsupported.empty()) p->unsupported = w + " > 0 (ILU(k))";
   } else if (w == "ML_CYCLE") {
     const std::string v = sv ? upper(sv->c_str()) : "";
-    if (v != "VCYCLE" && v != "MULT" && p->unsupported.empty()) p->unsupported = w + "=" + v;
+    if (v == "VCYCLE" || v == "MULT")
+      p->cycle = MLDG_CYCLE_V;
+    else if (v == "WCYCLE")
+      p->cycle = MLDG_CYCLE_W;
+    else if (p->unsupported.empty())
+      p->unsupported = w + "=" + v;
   } else if (w == "COARSE_SOLVE") {
     const std::string v = sv ? upper(sv->c_str()) : "";
     if (v == "BJAC" || v == "ILU")
@@ -269,7 +276,8 @@ extern "C" int mldp_smoothers_build(mldp_prec *p) {
     rc = mldg_upload_level(p->gpu, l, &d);
     if (rc) return fail(p, rc, mldg_last_error(p->gpu));
   }
-  rc = mldg_finalize(p->gpu, nlev, p->precision);
+  rc = mldg_set_cycle(p->gpu, p->cycle);
+  if (rc == 0) rc = mldg_finalize(p->gpu, nlev, p->precision);
   if (rc) return fail(p, rc, mldg_last_error(p->gpu));
   p->smoothers_built = true;
   return 0;

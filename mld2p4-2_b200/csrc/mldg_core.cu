@@ -296,6 +296,7 @@ struct Engine {
   int64_t launches = 0;
   int64_t bytes = 0;
   cudaStream_t st = nullptr;
+  int cycle = MLDG_CYCLE_V;  // MLDG_CYCLE_V / MLDG_CYCLE_W
   // ---- launch accounting, probe and profile hooks ----
   int cur_lev = 0;
   int probe_kind = 0, probe_lev = 0, probe_idx = 0;
@@ -694,6 +695,14 @@ struct EngineT : Engine {
       vcycle(l + 1, trans);
       cur_lev = l;
       prolong(C, L.y);                                   // y += P y_{l+1}
+      if (cycle == MLDG_CYCLE_W) {
+        // W-cycle: second coarse correction from the new residual (mld_dmlprec_aply.f90:716-745)
+        spmv(A, L.y, T(-1), L.x, T(1), L.ty, T(0));
+        spmv(C.R, L.ty, T(1), nullptr, T(0), C.x, T(0));
+        vcycle(l + 1, trans);
+        cur_lev = l;
+        prolong(C, L.y);
+      }
       if (post) {
         spmv(A, L.y, T(-1), L.x, T(1), L.ty, T(0));
         smoother(L, trans, L.ty, T(1), L.y, trans == 'N' ? L.spost : L.spre, trans == 'N');
@@ -1190,6 +1199,13 @@ struct EngineT : Engine {
       vcycle_m(l + 1, trans);
       cur_lev = l;
       prolong_m(C, L.ym);
+      if (cycle == MLDG_CYCLE_W) {
+        spmm(A, L.ym, T(-1), L.xm, T(1), L.tym, T(0));
+        spmm(C.R, L.tym, T(1), nullptr, T(0), C.xm, T(0));
+        vcycle_m(l + 1, trans);
+        cur_lev = l;
+        prolong_m(C, L.ym);
+      }
       if (post) {
         spmm(A, L.ym, T(-1), L.xm, T(1), L.tym, T(0));
         smoother_m(L, trans, L.tym, T(1), L.ym, trans == 'N' ? L.spost : L.spre, trans == 'N');
@@ -1366,6 +1382,7 @@ void EngineT<float>::prolong(Lev &C, float *y) {
 // ---------------------------------------------------------------------------
 struct Handle {
   mldg_opts opts{};
+  int cycle = MLDG_CYCLE_V;
   bool has_fbgs = false;  // a Gauss-Seidel level: trans 'T' is rejected
   std::string last_error;
   std::vector<HostLevel> host;
@@ -1888,6 +1905,7 @@ static Engine *make_engine(Handle *h) {
   e->probe_lev = h->probe_lev;
   e->probe_idx = h->probe_idx;
   e->err = h->err;
+  e->cycle = h->cycle;
   e->xin = h->xin;
   e->yout = h->yout;
   e->nsm = h->nsm;
@@ -2782,6 +2800,25 @@ extern "C" int mldg_finalize(mldg_handle *hp, int nlev, int precision) {
   MLDG_GUARD(hp, {
     MLDG_CUDA(cudaSetDevice(hp->h.opts.device));
     mldg::finalize(&hp->h, nlev, precision);
+  });
+}
+
+extern "C" int mldg_set_cycle(mldg_handle *hp, int cycle) {
+  if (!hp) return MLDG_ERR_ARG;
+  MLDG_GUARD(hp, {
+    Handle &h = hp->h;
+    if (cycle != MLDG_CYCLE_V && cycle != MLDG_CYCLE_W) mldg::fail(MLDG_ERR_ARG, "unknown cycle %d", cycle);
+    if (h.cycle != cycle) {
+      h.cycle = cycle;
+      for (int t = 0; t < 2; ++t)
+        if (h.gexec[t]) {
+          cudaGraphExecDestroy(h.gexec[t]);
+          h.gexec[t] = nullptr;
+        }
+      mldg::drop_multi_graphs(&h);
+      mldg::drop_krylov_graphs(&h);
+      if (h.eng) h.eng->cycle = cycle;
+    }
   });
 }
 

@@ -658,6 +658,14 @@ static void inner_mult(orc_prec *p, int l, char trans) {
     inner_mult(p, l + 1, trans); /* (:702) */
     /* prolongation + correction y += P y_c (:707-709) */
     orc_spmv(lc->P.nr, lc->P.irp, lc->P.ja, lc->P.val, 1.0, p->y2l[l + 1], 1.0, y);
+    if (p->par.ml_cycle == ORC_WCYCLE) {
+      /* W-cycle: a second coarse correction from the new residual (:716-745) */
+      memcpy(ty, x, sizeof(double) * (size_t)n);
+      spmv_op(&lv->A, trans, -1.0, y, 1.0, ty);
+      orc_spmv(lc->R.nr, lc->R.irp, lc->R.ja, lc->R.val, 1.0, ty, 0.0, p->x2l[l + 1]);
+      inner_mult(p, l + 1, trans);
+      orc_spmv(lc->P.nr, lc->P.irp, lc->P.ja, lc->P.val, 1.0, p->y2l[l + 1], 1.0, y);
+    }
     if (post) {
       memcpy(ty, x, sizeof(double) * (size_t)n);
       spmv_op(&lv->A, trans, -1.0, y, 1.0, ty); /* (:748-755) */
@@ -682,6 +690,7 @@ void orc_default_params(orc_params *p) {
   p->max_levs = 20;
   p->min_cr_ratio = 1.5;
   p->aggr_thresh = 0.01;
+  p->ml_cycle = ORC_VCYCLE;
 }
 
 orc_prec *orc_prec_new(const orc_params *par) {

@@ -38,7 +38,10 @@ typedef struct {
   int max_levs;        /* default 20 (mld_d_prec_type.f90:92) */
   double min_cr_ratio; /* default 1.5 (mld_d_prec_type.f90:94) */
   double aggr_thresh;  /* default 0.01 (mld_d_onelev_mod.f90:445) */
+  int ml_cycle;        /* ORC_VCYCLE (default) or ORC_WCYCLE */
 } orc_params;
+
+enum { ORC_VCYCLE = 0, ORC_WCYCLE = 1 };
 
 typedef struct orc_prec orc_prec;
 

@@ -18,6 +18,7 @@ _lib = None
 
 JACOBI = 1
 BJAC = 2
+VCYCLE, WCYCLE = 0, 1  # ml_cycle
 FBGS = 3  # forward GS pre / backward GS post (jac smoother + GS / BWGS solvers)
 
 
@@ -33,6 +34,7 @@ class Params(C.Structure):
         ("max_levs", C.c_int),
         ("min_cr_ratio", C.c_double),
         ("aggr_thresh", C.c_double),
+        ("ml_cycle", C.c_int),
     ]
 
 

@@ -107,6 +107,26 @@ def test_gauss_seidel_exact_on_triangular(orc):
     assert np.linalg.norm(y - ref) <= 1e-13 * np.linalg.norm(ref)
 
 
+def test_wcycle_symmetric_and_not_weaker(orc):
+    """W-cycle on a symmetric operator with a symmetric smoother pair stays
+    symmetric, and converges in no more FCG iterations than the V-cycle."""
+    a = orc.gen_pde3d(14, 1, (1, 1, 1, 0, 0, 0, 0))
+    b = orc.spmv(a, np.ones(a.nrows))
+    its = {}
+    for cyc in (orc.VCYCLE, orc.WCYCLE):
+        par = oracle_params(orc, "FBGS", 1, coarse_sweeps=1, mcs=40)
+        par.ml_cycle = cyc
+        p = orc.Prec(par)
+        p.build(a)
+        assert p.nlev >= 3
+        rng = np.random.default_rng(4)
+        x, z = rng.uniform(-1, 1, a.nrows), rng.uniform(-1, 1, a.nrows)
+        assert abs(p.apply(x) @ z - x @ p.apply(z)) <= 1e-12 * abs(p.apply(x) @ z)
+        _, its[cyc], rr, _ = orc.krylov("FCG", a, p, b, eps=1e-10)
+        assert rr <= 1e-10
+    assert its[orc.WCYCLE] <= its[orc.VCYCLE]
+
+
 def test_hierarchy_invariants(orc):
     a = orc.gen_pde3d(16, 1, ISO)
     p = orc.Prec(oracle_params(orc, "BJAC", mcs=150))
