@@ -52,6 +52,21 @@ int mldp_krylov(mldp_prec *p, const char *method, int n, const int32_t *irp, con
                 int *iters, double *err, int mem_kind);
 /* hierarchy inspection (for tests and descr) */
 int mldp_nlev(const mldp_prec *p);
+
+/* MatrixMarket hierarchy I/O in the file layout of the reference's
+ * prec%dump(info, istart=1, prefix=..., ac=.true., rp=.true., smoother=.true.,
+ * solver=.true.) (mld_d_prec_type.f90:698-729, mld_d_base_onelev_dump.f90):
+ * <prefix>_p000_l<LLL>_{ac,r,p}.mtx for levels >= 2, and the smoother /
+ * solver files <prefix>_sm[2a]_p000_l<LLL>_{nd,lower,diag,upper}.mtx.
+ * mldp_dump writes the built hierarchy.  mldp_load_dump replaces
+ * hierarchy_build + smoothers_build: level 1 is the given matrix, levels
+ * 2..nlev and every level's smoother data come from the files (the
+ * smoother kind of a level follows from the files present: GS + BWGS ->
+ * FBGS, lower/diag/upper -> ILU(0), diag only -> Jacobi), sweeps from set();
+ * the hierarchy is then uploaded to the GPU like mldp_smoothers_build. */
+int mldp_dump(const mldp_prec *p, const char *prefix);
+int mldp_load_dump(mldp_prec *p, const char *prefix, int nlev, int n, const int32_t *irp,
+                   const int32_t *ja, const double *val);
 /* info[0..9] = n, nnzA, nnzP, nnzR, nnzL, nnzU, nnzND, naggr, smoother kind,
  * sweeps_pre ; dinfo[0..1] = omega, damping */
 int mldp_level_info(const mldp_prec *p, int lev, int64_t *info, double *dinfo);

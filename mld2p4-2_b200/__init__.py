@@ -215,6 +215,8 @@ def lib():
                                   C.c_double, C.c_int, C.POINTER(C.c_int),
                                   C.POINTER(C.c_double), C.c_int]
         L.mldp_nlev.argtypes = [vp]
+        L.mldp_dump.argtypes = [vp, C.c_char_p]
+        L.mldp_load_dump.argtypes = [vp, C.c_char_p, C.c_int, C.c_int, ip, ip, dp]
         L.mldp_level_info.argtypes = [vp, C.c_int, C.POINTER(C.c_int64), dp]
         L.mldp_level_csr.argtypes = [vp, C.c_int, C.c_char_p, ip, ip, dp]
         L.mldp_level_vec.argtypes = [vp, C.c_int, C.c_char_p, dp, ip]
@@ -509,6 +511,15 @@ class MldPrec(_GpuDiag):
         dv = np.zeros(n, np.float64)
         rc = lib().mldp_level_vec(self._p, lev, which.encode(), _dp(dv), None)
         return None if rc else dv
+
+    def dump(self, prefix: str):
+        """Write the built hierarchy as the reference's prec%dump would (MatrixMarket)."""
+        self._check(lib().mldp_dump(self._p, prefix.encode()))
+
+    def load_dump(self, prefix: str, nlev: int, a: CSR):
+        """Build from a prec%dump file set: level 1 is `a`, the rest from the files."""
+        self._check(lib().mldp_load_dump(self._p, prefix.encode(), nlev, a.nrows, _ip(a.irp),
+                                         _ip(a.ja), _dp(a.val)))
 
     def descr(self) -> str:
         buf = C.create_string_buffer(8192)

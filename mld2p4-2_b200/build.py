@@ -19,7 +19,7 @@ LIB = os.path.join(HERE, "libmldgpu.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["mldg_core.cu"]
-CXX_SOURCES = ["mldg_tri.cpp", "host/mld_hier.cpp", "host/mld_prec.cpp"]
+CXX_SOURCES = ["mldg_tri.cpp", "host/mld_hier.cpp", "host/mld_prec.cpp", "host/mld_mmio.cpp"]
 
 
 def _nvcc() -> str:

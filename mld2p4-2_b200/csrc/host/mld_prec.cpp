@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "mld_hier.h"
+#include "mld_mmio.h"
 #include "mld_prec.h"
 #include "mldg.h"
 
@@ -242,12 +243,20 @@ extern "C" int mldp_hierarchy_build(mldp_prec *p, int n, const int32_t *irp, con
   return 0;
 }
 
+static int upload_all(mldp_prec *p);
+
 extern "C" int mldp_smoothers_build(mldp_prec *p) {
   if (!p) return MLDG_ERR_ARG;
   if (!p->hier_built) return fail(p, 3112, "smoothers_build before hierarchy_build");
   std::string msg;
   int rc = mld::smoothers_build(p->lv, p->parms, msg);
   if (rc) return fail(p, rc, msg);
+  return upload_all(p);
+}
+
+// the finished host levels -> the GPU handle (mldg_upload_level + finalize)
+static int upload_all(mldp_prec *p) {
+  int rc = 0;
   if (!p->gpu) {
     mldg_opts o;
     o.device = p->device;
@@ -281,6 +290,34 @@ extern "C" int mldp_smoothers_build(mldp_prec *p) {
   if (rc) return fail(p, rc, mldg_last_error(p->gpu));
   p->smoothers_built = true;
   return 0;
+}
+
+extern "C" int mldp_dump(const mldp_prec *p, const char *prefix) {
+  if (!p || !prefix) return MLDG_ERR_ARG;
+  if (!p->smoothers_built) return MLDG_ERR_NOT_BUILT;
+  std::string msg;
+  const int rc = mld::dump_hierarchy(p->lv, prefix, msg);
+  if (rc) {
+    const_cast<mldp_prec *>(p)->err = msg;
+    return MLDG_ERR_ARG;
+  }
+  return 0;
+}
+
+extern "C" int mldp_load_dump(mldp_prec *p, const char *prefix, int nlev, int n, const int32_t *irp,
+                              const int32_t *ja, const double *val) {
+  if (!p || !prefix) return MLDG_ERR_ARG;
+  if (!p->inited) return fail(p, 3111, "load_dump before init");
+  if (n <= 0 || !irp || !ja || !val) return fail(p, MLDG_ERR_ARG, "load_dump: bad matrix");
+  if (!p->unsupported.empty())
+    return fail(p, MLDG_ERR_ARG, "setting not supported by the GPU apply: " + p->unsupported);
+  mld::CSR a = make_csr(n, irp, ja, val);
+  std::string msg;
+  p->hier_built = p->smoothers_built = false;
+  const int rc = mld::load_hierarchy(prefix, nlev, a, p->parms, p->lv, msg);
+  if (rc) return fail(p, rc, msg);
+  p->hier_built = true;
+  return upload_all(p);
 }
 
 extern "C" int mldp_build(mldp_prec *p, int n, const int32_t *irp, const int32_t *ja,
