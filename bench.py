@@ -36,6 +36,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 METRIC = "time-to-1e-10 residual (mixed vs FP64 GPU V-cycle); V-cycle apply HBM GB/s"
 S3 = 1.0 / np.sqrt(3.0)
 ISO = (1.0, 1.0, 1.0, S3, S3, S3, 0.0)
+ANISO = (1.0, 1.0, 0.01, S3, S3, S3, 0.0)
 
 
 def load_package():
@@ -141,7 +142,7 @@ def make_prec(mld, a, smoother, precision="FP64", device=0):
     if smoother == "JACOBI":
         p.set("SMOOTHER_SWEEPS", 2)
         p.set("SMOOTHER_DAMPING", 0.8)
-    else:
+    elif smoother == "BJAC":
         p.set("SUB_SOLVE", "ILU")
         p.set("SMOOTHER_SWEEPS", 1)
     p.set("COARSE_SOLVE", "BJAC")
@@ -271,6 +272,45 @@ def time_variant(mld, a, b, smoother, precision, args, dev, torch, probe=False, 
     return res
 
 
+def time_precision_form(mld, args, dev, torch, idim=160, ref_solution=None):
+    """Precision form: anisotropic -(u_xx + u_yy + 0.01 u_zz) + (1/sqrt3) grad u
+    at idim=160, b uniform[-1,1] (seed 0); the FP64 V-cycle against the FP32
+    V-cycle and the FP32 V-cycle with FP16 prolongator values, each inside the
+    FP64 FCG loop to 1e-10, with the point-Jacobi and the FBGS smoothers
+    (block-Jacobi ILU(0) FCG stagnates near 1e-3 on this problem, on the CPU
+    oracle as on the GPU, and is left out).  ref_solution(a, b) gives the FP64
+    CPU solution the final errors are measured against (or None)."""
+    a = mld.gen_pde3d(idim, 1, ANISO)
+    b = np.random.default_rng(0).uniform(-1.0, 1.0, a.nrows)
+    bd = torch.tensor(b, dtype=torch.float64, device=f"cuda:{dev}")
+    x = torch.zeros_like(bd)
+    xref = ref_solution(a, b) if ref_solution is not None else None
+    out = {"form": f"anisotropic idim={idim} (0.01 u_zz), b uniform[-1,1] seed 0, FCG to {args.eps:g}"}
+    for sm in ("JACOBI", "FBGS"):
+        res = {}
+        for pr in ("FP64", "FP32", "FP32_P16"):
+            p = make_prec(mld, a, sm, pr, device=dev)
+            ms, its = [], None
+            for _ in range(1 + max(1, min(args.steps, 3))):  # first solve warms (graph capture)
+                x.zero_()
+                torch.cuda.synchronize()
+                _, its, rr = mld.krylov("FCG", a, p, bd, x, eps=args.eps, itmax=500, use_prec_matrix=True)
+                ms.append(p.last_timing()[0])
+            t = statistics.median(ms[1:])
+            xs = x.cpu().numpy()
+            r = {"time_to_1e-10_ms": t, "iterations": its, "final_relres": rr}
+            if xref is not None:
+                r["rel_error_vs_cpu_fp64"] = float(np.linalg.norm(xs - xref) / np.linalg.norm(xref))
+            res[pr.lower()] = r
+            p.free()
+        f64 = res["fp64"]["time_to_1e-10_ms"]
+        for pr in ("fp32", "fp32_p16"):
+            res[pr]["speedup_vs_fp64"] = f64 / res[pr]["time_to_1e-10_ms"]
+            res[pr]["extra_iterations"] = res[pr]["iterations"] - res["fp64"]["iterations"]
+        out[sm.lower()] = res
+    return out
+
+
 def time_systems(mld, args, dev, torch, nsys=64, lo=24, hi=96):
     """Batching form (b): nsys independent systems, idim uniform in lo..hi
     (seed 1), each with its own hierarchy (FP32 V-cycle, FP64 FCG), solved
@@ -381,6 +421,17 @@ def run_ours(args, rank, world, local_rank):
                 r = time_variant(mld, a, b, sm, pr, args, dev, torch, dist=dist)
                 others[f"{sm.lower()}_{pr.lower()}"] = r
                 r["p"].free()
+        precision_form = None
+        if not args.no_variants and not args.no_batch:
+            ref = None
+            if world == 1 and not args.no_cpu_baseline:
+                def ref(a, b):
+                    # FP64 CPU solution of the oracle (C restatement), the checker
+                    orc = load_oracle()
+                    ao, op = cpu_solve_oracle(orc, a, "JACOBI", args.eps)
+                    xr, _, _, _ = orc.krylov("FCG", ao, op, b, eps=args.eps, itmax=500)
+                    return xr
+            precision_form = time_precision_form(mld, args, dev, torch, ref_solution=ref)
         batch = None
         if not args.no_variants and not args.no_batch:
             batch = {"rhs32_idim128": time_batch(mld, args, dev, torch),
@@ -436,6 +487,7 @@ def run_ours(args, rank, world, local_rank):
                      "launches_timed": probe_cnt, "share_of_apply": main["share"]},
         "variants": variants,
         "batching": batch,
+        "precision_form": precision_form,
         "e2e": {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "solves/s",
                 "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 8 * n},
         "gpu_launches": main["launches"],

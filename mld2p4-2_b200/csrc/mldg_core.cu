@@ -145,9 +145,11 @@ struct DCSR {
   int nr = 0, nc = 0;
   int64_t nnz = 0;
   int *irp = nullptr, *ja = nullptr;
+  short *jd = nullptr;  // int16 column offsets from the row (square, |j - i| <= 32767), or null
   T *val = nullptr;
   int tpr = 1;
   bool present() const { return irp != nullptr; }
+  int64_t idx_bytes() const { return jd ? 2 : 4; }
 };
 
 template <typename T>
@@ -223,6 +225,21 @@ static DCSR<T> to_dev(Arena &ar, const HostCSR &h) {
   d.nnz = h.nnz();
   d.irp = ar.upload(h.irp);
   d.ja = ar.upload(h.ja);
+  if (h.nr == h.nc && !std::getenv("MLDG_NO_IDX16")) {
+    bool fits = true;
+    for (int i = 0; i < h.nr && fits; ++i)
+      for (int k = h.irp[i]; k < h.irp[i + 1]; ++k)
+        if (std::abs(h.ja[k] - i) > 32767) {
+          fits = false;
+          break;
+        }
+    if (fits) {
+      std::vector<short> jd(h.ja.size());
+      for (int i = 0; i < h.nr; ++i)
+        for (int k = h.irp[i]; k < h.irp[i + 1]; ++k) jd[k] = (short)(h.ja[k] - i);
+      d.jd = ar.upload(jd);
+    }
+  }
   std::vector<T> v(h.val.begin(), h.val.end());
   d.val = ar.upload(v);
   d.tpr = pick_tpr(d.nnz, d.nr);
@@ -404,13 +421,18 @@ struct EngineT : Engine {
     const int g = blocks_for((int64_t)A.nr * A.tpr);
     begin(MLDG_KERNEL_SPMV);
     switch (A.tpr) {
-#define CASE(K) \
-  case K: k_spmv<T, K><<<g, 256, 0, st>>>(A.nr, A.irp, A.ja, A.val, v, a1, b, a0, out, a2); break;
+#define CASE(K)                                                                                  \
+  case K:                                                                                        \
+    if (A.jd)                                                                                    \
+      k_spmv<T, K, short><<<g, 256, 0, st>>>(A.nr, A.irp, A.jd, A.val, v, a1, b, a0, out, a2);  \
+    else                                                                                         \
+      k_spmv<T, K, int><<<g, 256, 0, st>>>(A.nr, A.irp, A.ja, A.val, v, a1, b, a0, out, a2);    \
+    break;
       CASE(1) CASE(2) CASE(4) CASE(8) CASE(16) CASE(32)
 #undef CASE
       default: fail(MLDG_ERR_INTERNAL, "bad tpr %d", A.tpr);
     }
-    end(A.nnz * (int64_t)(sizeof(T) + 4) + 4 * ((int64_t)A.nr + 1) + (int64_t)A.nc * sizeof(T) +
+    end(A.nnz * (int64_t)(sizeof(T) + A.idx_bytes()) + 4 * ((int64_t)A.nr + 1) + (int64_t)A.nc * sizeof(T) +
         (int64_t)A.nr * sizeof(T) * (1 + (b ? 1 : 0) + (a2 != T(0) ? 1 : 0)));
   }
   void jacobi(const DCSR<T> &ND, const T *d, const T *x, const T *ty, int first, T omega,
@@ -418,16 +440,20 @@ struct EngineT : Engine {
     const int g = blocks_for((int64_t)ND.nr * ND.tpr);
     begin(MLDG_KERNEL_JACOBI);
     switch (ND.tpr) {
-#define CASE(K)                                                                           \
-  case K:                                                                                 \
-    k_jacobi<T, K><<<g, 256, 0, st>>>(ND.nr, ND.irp, ND.ja, ND.val, d, x, ty, first, omega, \
-                                      alpha, beta, out);                                  \
+#define CASE(K)                                                                                       \
+  case K:                                                                                             \
+    if (ND.jd)                                                                                        \
+      k_jacobi<T, K, short><<<g, 256, 0, st>>>(ND.nr, ND.irp, ND.jd, ND.val, d, x, ty, first, omega, \
+                                               alpha, beta, out);                                     \
+    else                                                                                              \
+      k_jacobi<T, K, int><<<g, 256, 0, st>>>(ND.nr, ND.irp, ND.ja, ND.val, d, x, ty, first, omega,   \
+                                             alpha, beta, out);                                       \
     break;
       CASE(1) CASE(2) CASE(4) CASE(8) CASE(16) CASE(32)
 #undef CASE
       default: fail(MLDG_ERR_INTERNAL, "bad tpr %d", ND.tpr);
     }
-    end(ND.nnz * (int64_t)(sizeof(T) + 4) + 4 * ((int64_t)ND.nr + 1) +
+    end(ND.nnz * (int64_t)(sizeof(T) + ND.idx_bytes()) + 4 * ((int64_t)ND.nr + 1) +
         (int64_t)ND.nr * sizeof(T) * (3 + (first ? 0 : 1) + (beta != T(0) ? 1 : 0)));
   }
   void diag(int n, const T *d, const T *x, T alpha, T beta, T *out) {
@@ -2340,8 +2366,13 @@ static void spmv64(Handle *h, const DCSR<double> &A, const double *v, double a1,
   const int64_t thr = (int64_t)A.nr * A.tpr;
   const int g = (int)std::max<int64_t>(1, std::min<int64_t>((thr + 255) / 256, (int64_t)h->nsm * 16));
   switch (A.tpr) {
-#define CASE(K) \
-  case K: k_spmv<double, K><<<g, 256, 0, h->st>>>(A.nr, A.irp, A.ja, A.val, v, a1, b, a0, out, 0.0); break;
+#define CASE(K)                                                                                         \
+  case K:                                                                                               \
+    if (A.jd)                                                                                           \
+      k_spmv<double, K, short><<<g, 256, 0, h->st>>>(A.nr, A.irp, A.jd, A.val, v, a1, b, a0, out, 0.0); \
+    else                                                                                                \
+      k_spmv<double, K, int><<<g, 256, 0, h->st>>>(A.nr, A.irp, A.ja, A.val, v, a1, b, a0, out, 0.0);   \
+    break;
     CASE(1) CASE(2) CASE(4) CASE(8) CASE(16) CASE(32)
 #undef CASE
     default: fail(MLDG_ERR_INTERNAL, "bad tpr");

@@ -99,9 +99,15 @@ __device__ __forceinline__ T wait_value(const T *p, int *err) {
 // contiguous block of 32/TPR rows per step, so shuffles always see a full warp.
 // Reference ops: psb_spmm (residual, mld_dmlprec_aply.f90:674,752),
 // psb_map_X2Y / psb_map_Y2X (restriction :682, prolongation :707).
-template <typename T, int TPR>
+// Column of entry k of row `row`: absolute int32 indices, or int16 offsets
+// from the row (square matrices whose entries all lie within 32767 of the
+// diagonal: 2 bytes per entry instead of 4 on a bandwidth-bound sweep).
+__device__ __forceinline__ int colof(const int *__restrict__ cj, int k, int) { return cj[k]; }
+__device__ __forceinline__ int colof(const short *__restrict__ cj, int k, int row) { return row + (int)cj[k]; }
+
+template <typename T, int TPR, typename CI = int>
 __global__ void __launch_bounds__(256) k_spmv(int nr, const int *__restrict__ irp,
-                                              const int *__restrict__ ja,
+                                              const CI *__restrict__ ja,
                                               const T *__restrict__ val,
                                               const T *__restrict__ v, T a1,
                                               const T *__restrict__ b, T a0, T *out, T a2) {
@@ -116,7 +122,7 @@ __global__ void __launch_bounds__(256) k_spmv(int nr, const int *__restrict__ ir
     T s = T(0);
     if (row < nr) {
       const int e = irp[row + 1];
-      for (int k = irp[row] + sub; k < e; k += TPR) s = fma(val[k], __ldg(v + ja[k]), s);
+      for (int k = irp[row] + sub; k < e; k += TPR) s = fma(val[k], __ldg(v + colof(ja, k, row)), s);
     }
 #pragma unroll
     for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, TPR);
@@ -165,9 +171,9 @@ __global__ void __launch_bounds__(256) k_spmv_h(int nr, const int *__restrict__ 
 //   out_i = alpha*v_i + beta*out_i
 // When first != 0 the incoming iterate is ty = omega*d o x (the unrolled first
 // sweep, :136), computed on the fly from x and d instead of being stored.
-template <typename T, int TPR>
+template <typename T, int TPR, typename CI = int>
 __global__ void __launch_bounds__(256) k_jacobi(int nr, const int *__restrict__ irp,
-                                                const int *__restrict__ ja,
+                                                const CI *__restrict__ ja,
                                                 const T *__restrict__ val,
                                                 const T *__restrict__ d,
                                                 const T *__restrict__ x,
@@ -186,11 +192,11 @@ __global__ void __launch_bounds__(256) k_jacobi(int nr, const int *__restrict__ 
       const int e = irp[row + 1];
       if (first) {
         for (int k = irp[row] + sub; k < e; k += TPR) {
-          const int j = ja[k];
+          const int j = colof(ja, k, row);
           s = fma(val[k], omega * (__ldg(d + j) * __ldg(x + j)), s);
         }
       } else {
-        for (int k = irp[row] + sub; k < e; k += TPR) s = fma(val[k], __ldg(ty + ja[k]), s);
+        for (int k = irp[row] + sub; k < e; k += TPR) s = fma(val[k], __ldg(ty + colof(ja, k, row)), s);
       }
     }
 #pragma unroll
