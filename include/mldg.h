@@ -126,13 +126,22 @@ int mldg_upload_level(mldg_handle *h, int lev, const mldg_level_desc *desc);
  * (impl/mld_dprecbld.f90:60-159). */
 int mldg_finalize(mldg_handle *h, int nlev, int precision);
 
-/* Multilevel cycle of every later apply: MLDG_CYCLE_V (default) or
+/* Multilevel cycle of every later apply: MLDG_CYCLE_V (default);
  * MLDG_CYCLE_W, which repeats the coarse correction once from the updated
- * residual before post-smoothing (mld_dmlprec_aply.f90:716-745).  May be
- * called before or after mldg_finalize.  replaces: prec%set('ML_CYCLE',
- * 'VCYCLE'|'WCYCLE') (mld_d_base_onelev_cseti.F90, ML_CYCLE). */
+ * residual before post-smoothing (mld_dmlprec_aply.f90:716-745);
+ * MLDG_CYCLE_K / MLDG_CYCLE_KSYM, the K-cycle: on every level below the
+ * second, at most two steps of GCR (K) or flexible CG (KSYM) with the next
+ * level's cycle as preconditioner, the second step only if the first left
+ * more than 0.25 of the level residual (mld_dmlprec_aply.f90:811-1184).  The
+ * K-cycle decides on the host between its kernels, so its applies are not
+ * replayed from CUDA graphs, a multi-column apply runs column by column, and
+ * mldg_krylov_multi / mldg_krylov_batch reject it.  May be called before or
+ * after mldg_finalize.  replaces: prec%set('ML_CYCLE', 'VCYCLE' | 'WCYCLE' |
+ * 'KCYCLE' | 'KCYCLESYM') (mld_base_prec_type.F90:430-439). */
 #define MLDG_CYCLE_V 0
 #define MLDG_CYCLE_W 1
+#define MLDG_CYCLE_K 2
+#define MLDG_CYCLE_KSYM 3
 int mldg_set_cycle(mldg_handle *h, int cycle);
 
 /* y = M^{-1} x (trans 'N') or y = M^{-T} x (trans 'T'/'C') for nrhs vectors

@@ -29,7 +29,7 @@ _lib = None
 SMOOTHER_JACOBI = 1
 SMOOTHER_BJAC = 2
 SMOOTHER_FBGS = 3
-CYCLE_V, CYCLE_W = 0, 1
+CYCLE_V, CYCLE_W, CYCLE_K, CYCLE_KSYM = 0, 1, 2, 3
 PREC_FP64, PREC_FP32, PREC_FP32_P16 = 0, 1, 2
 MEM_HOST, MEM_DEVICE = 0, 1
 
@@ -369,7 +369,7 @@ class Hierarchy(_GpuDiag):
             self.n = A.nrows
 
     def set_cycle(self, cycle: int):
-        """MLDG_CYCLE_V (0) or MLDG_CYCLE_W (1)."""
+        """MLDG_CYCLE_V (0), _W (1), _K (2, inner GCR) or _KSYM (3, inner FCG)."""
         self._check(lib().mldg_set_cycle(self._h, cycle))
 
     def finalize(self, nlev: int, precision: int = PREC_FP64):

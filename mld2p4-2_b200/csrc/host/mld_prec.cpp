@@ -150,6 +150,10 @@ static int set_common(mldp_prec *p, const std::string &w, const std::string *sv,
       p->cycle = MLDG_CYCLE_V;
     else if (v == "WCYCLE")
       p->cycle = MLDG_CYCLE_W;
+    else if (v == "KCYCLE")
+      p->cycle = MLDG_CYCLE_K;
+    else if (v == "KCYCLESYM")
+      p->cycle = MLDG_CYCLE_KSYM;
     else if (p->unsupported.empty())
       p->unsupported = w + "=" + v;
   } else if (w == "COARSE_SOLVE") {

@@ -313,7 +313,7 @@ struct Engine {
   int64_t launches = 0;
   int64_t bytes = 0;
   cudaStream_t st = nullptr;
-  int cycle = MLDG_CYCLE_V;  // MLDG_CYCLE_V / MLDG_CYCLE_W
+  int cycle = MLDG_CYCLE_V;  // MLDG_CYCLE_V / _W / _K / _KSYM
   // ---- launch accounting, probe and profile hooks ----
   int cur_lev = 0;
   int probe_kind = 0, probe_lev = 0, probe_idx = 0;
@@ -366,6 +366,36 @@ struct Engine {
     }
   }
 };
+
+// y = a*x + b*y (b = 1: an axpy as psb_geaxpby(a, x, 1, y))
+template <typename T>
+__global__ void k_axpby2(int n, T a, const T *__restrict__ x, T b, T *y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    y[i] = a * x[i] + b * y[i];
+}
+// up to three dot products of T vectors accumulated in FP64, per-block
+// partials in the layout of k_dots (summed by k_dots_final)
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_dotsT(int n, int np, const T *__restrict__ x0,
+                                                      const T *__restrict__ y0, const T *__restrict__ x1,
+                                                      const T *__restrict__ y1, const T *__restrict__ x2,
+                                                      const T *__restrict__ y2, double *partial) {
+  __shared__ double sh[32];
+  double s0 = 0, s1 = 0, s2 = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    s0 = fma((double)x0[i], (double)y0[i], s0);
+    if (np > 1) s1 = fma((double)x1[i], (double)y1[i], s1);
+    if (np > 2) s2 = fma((double)x2[i], (double)y2[i], s2);
+  }
+  s0 = block_sum(s0, sh);
+  s1 = block_sum(s1, sh);
+  s2 = block_sum(s2, sh);
+  if (threadIdx.x == 0) {
+    partial[blockIdx.x * 3 + 0] = s0;
+    partial[blockIdx.x * 3 + 1] = s1;
+    partial[blockIdx.x * 3 + 2] = s2;
+  }
+}
 
 template <typename T>
 __global__ void k_axpby1(int n, const T *__restrict__ x, T beta, T *y) {
@@ -738,6 +768,124 @@ struct EngineT : Engine {
     }
   }
   void prolong(Lev &C, T *y);
+
+  // ---- K-cycle (ML_CYCLE = KCYCLE / KCYCLESYM) ----
+  // mld_d_inner_k_cycle / mld_dinneritkcycle (mld_dmlprec_aply.f90:811-1184):
+  // the inner Krylov step on a level needs its inner products on the host
+  // (the second step is taken only if the first left ||w|| > 0.25 ||rhs||),
+  // so a K-cycle is issued with host synchronisations and is not captured.
+  struct KVec {
+    T *w = nullptr, *v = nullptr, *v1 = nullptr, *xk = nullptr, *d0 = nullptr, *d1 = nullptr;
+  };
+  std::vector<KVec> kvec;
+  Arena karena;
+  double *kpart = nullptr, *kres = nullptr, *khost = nullptr;
+  bool kcycle_mode() const { return cycle == MLDG_CYCLE_K || cycle == MLDG_CYCLE_KSYM; }
+  void ensure_k() {
+    if (!kvec.empty()) return;
+    kvec.resize(lv.size());
+    for (size_t l = 0; l < lv.size(); ++l) {
+      const size_t n = (size_t)std::max(lv[l].n, 1);
+      KVec &k = kvec[l];
+      k.w = karena.alloc<T>(n);
+      k.v = karena.alloc<T>(n);
+      k.v1 = karena.alloc<T>(n);
+      k.xk = karena.alloc<T>(n);
+      k.d0 = karena.alloc<T>(n);
+      k.d1 = karena.alloc<T>(n);
+    }
+    kpart = karena.alloc<double>(3 * kRedBlocks);
+    kres = karena.alloc<double>(4);
+    MLDG_CUDA(cudaMallocHost(&khost, 4 * sizeof(double)));
+  }
+  void copy(int n, const T *x, T *y) { k_axpby_impl(n, x, T(0), y); }
+  void axpby2(int n, T a, const T *x, T b, T *y) {
+    begin(MLDG_KERNEL_VEC);
+    k_axpby2<T><<<blocks_for(n), 256, 0, st>>>(n, a, x, b, y);
+    end((int64_t)n * sizeof(T) * 3);
+  }
+  // up to three inner products, returned on the host (FP64 accumulation)
+  void hdots(int n, int np, const T *x0, const T *y0, const T *x1, const T *y1, const T *x2, const T *y2,
+             double *r) {
+    begin(MLDG_KERNEL_VEC);
+    k_dotsT<T><<<kRedBlocks, kRedThreads, 0, st>>>(n, np, x0, y0, x1, y1, x2, y2, kpart);
+    end((int64_t)n * sizeof(T) * 2 * np);
+    begin(MLDG_KERNEL_VEC);
+    k_dots_final<<<1, kRedThreads, 0, st>>>(kRedBlocks, kpart, kres);
+    end(3 * kRedBlocks * 8);
+    MLDG_CUDA(cudaMemcpyAsync(khost, kres, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    MLDG_CUDA(cudaStreamSynchronize(st));
+    for (int q = 0; q < np; ++q) r[q] = khost[q];
+  }
+  void cycle_at(int l, char trans) {
+    if (kcycle_mode())
+      kcycle(l, trans);
+    else
+      vcycle(l, trans);
+  }
+  void kcycle(int l, char trans) {
+    cur_lev = l;
+    Lev &L = lv[l];
+    const int nlev = (int)lv.size();
+    if (l == nlev - 1) {
+      smoother(L, trans, L.x, T(0), L.y, L.spre);
+      return;
+    }
+    Lev &C = lv[l + 1];
+    const DCSR<T> &A = (trans == 'N') ? L.A : L.AT;
+    smoother(L, trans, L.x, T(0), L.y, trans == 'N' ? L.spre : L.spost, trans != 'N');
+    spmv(A, L.y, T(-1), L.x, T(1), L.ty, T(0));
+    spmv(C.R, L.ty, T(1), nullptr, T(0), C.x, T(0));
+    if (l + 1 <= nlev - 2)
+      inneritk(l + 1, trans, cycle == MLDG_CYCLE_K);
+    else
+      cycle_at(l + 1, trans);
+    cur_lev = l;
+    prolong(C, L.y);
+    spmv(A, L.y, T(-1), L.x, T(1), L.ty, T(0));
+    smoother(L, trans, L.ty, T(1), L.y, trans == 'N' ? L.spost : L.spre, trans == 'N');
+  }
+  void inneritk(int l, char trans, bool gcr) {
+    cur_lev = l;
+    Lev &L = lv[l];
+    KVec &k = kvec[l];
+    const int n = L.n;
+    double r[3];
+    fill(n, T(0), k.xk);
+    copy(n, L.x, k.w);
+    fill(n, T(0), L.y);
+    cycle_at(l, trans);
+    cur_lev = l;
+    copy(n, L.y, k.d0);
+    spmv(L.A, k.d0, T(1), nullptr, T(0), k.v, T(0));  // A, untransposed, as in the reference
+    if (gcr)
+      hdots(n, 3, k.v, k.w, k.v, k.v, k.w, k.w, r);
+    else
+      hdots(n, 3, k.d0, k.w, k.d0, k.v, k.w, k.w, r);
+    const double delta0 = std::sqrt(r[2]), tau = r[1];
+    double alpha = r[0] / tau;
+    axpby2(n, (T)(-alpha), k.v, T(1), k.w);
+    hdots(n, 1, k.w, k.w, nullptr, nullptr, nullptr, nullptr, r);
+    if (std::sqrt(r[0]) <= 0.25 * delta0) {
+      axpby2(n, (T)alpha, k.d0, T(1), k.xk);
+    } else {
+      copy(n, k.w, L.x);
+      cycle_at(l, trans);
+      cur_lev = l;
+      copy(n, L.y, k.d1);
+      spmv(L.A, k.d1, T(1), nullptr, T(0), k.v1, T(0));
+      if (gcr)
+        hdots(n, 3, k.v1, k.v, k.v1, k.v1, k.v1, k.w, r);
+      else
+        hdots(n, 3, k.d1, k.v, k.d1, k.v1, k.d1, k.w, r);
+      const double tau1 = r[0], tau2 = r[1], tau3 = r[2];
+      const double tau4 = tau2 - (tau1 * tau1) / tau;
+      alpha = alpha - (tau1 * tau3) / (tau * tau4);
+      axpby2(n, (T)alpha, k.d0, T(1), k.xk);
+      axpby2(n, (T)(tau3 / tau4), k.d1, T(1), k.xk);
+    }
+    copy(n, k.xk, L.y);
+  }
   // Lanes-per-row autotuner: times k_spmv with every TPR on each level's
   // operators (A, A^T, P, R, ND, ND^T) and keeps the fastest.
   void autotune_spmv(int reps) {
@@ -786,7 +934,11 @@ struct EngineT : Engine {
   // ---- multi-RHS V-cycle: K columns row-interleaved, v[i*K + c] ----
   int K = 2;
   Arena marena;  // K-wide buffers and block tables (grown on demand)
-  ~EngineT() override { marena.release(); }
+  ~EngineT() override {
+    marena.release();
+    karena.release();
+    if (khost) cudaFreeHost(khost);
+  }
   int64_t nk(int n) const { return (int64_t)n * K; }
 
   void build_blk_m(DTri<T> &t, int Kw) {
@@ -1242,6 +1394,7 @@ struct EngineT : Engine {
   }
   void record_multi(char trans, int Kw) override {
     if (Kw > mcap) fail(MLDG_ERR_INTERNAL, "multi buffers not allocated for %d columns", Kw);
+    if (kcycle_mode()) fail(MLDG_ERR_ARG, "the K-cycle has no multi-column form");
     launches = 0;
     bytes = 0;
     cur_lev = 0;
@@ -1362,6 +1515,9 @@ struct EngineT : Engine {
       if (nsw == 0) k_axpby_impl(F.n, F.x, T(0), F.y);
     } else if (lv.size() == 1) {
       smoother(F, trans, F.x, T(0), F.y, F.spre);
+    } else if (kcycle_mode()) {
+      ensure_k();
+      kcycle(0, trans);
     } else {
       vcycle(0, trans);
     }
@@ -2175,9 +2331,11 @@ static void finalize(Handle *h, int nlev, int precision) {
   h->finalized = true;
 }
 
+static bool kcycle_handle(const Handle *h) { return h->cycle == MLDG_CYCLE_K || h->cycle == MLDG_CYCLE_KSYM; }
+
 static void run_vcycle(Handle *h, char trans) {
   const int t = (trans == 'N') ? 0 : 1;
-  if (h->opts.use_graphs) {
+  if (h->opts.use_graphs && !kcycle_handle(h)) {
     if (!h->gexec[t]) {
       cudaGraph_t g;
       MLDG_CUDA(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
@@ -2333,7 +2491,7 @@ static void apply(Handle *h, const double *x, double *y, char trans, int nrhs, i
   h->last_launches = 0;
   MLDG_CUDA(cudaEventRecord(h->ev0, h->st));
   const char *em = std::getenv("MLDG_MULTI");
-  const bool multi = nrhs > 1 && !(em && em[0] == '0');
+  const bool multi = nrhs > 1 && !(em && em[0] == '0') && !kcycle_handle(h);
   if (multi) apply_multi(h, x, y, trans, nrhs, ld, mem);
   for (int c = 0; c < (multi ? 0 : nrhs); ++c) {
     const size_t off = (size_t)c * (size_t)(nrhs > 1 ? ld : n);
@@ -2519,6 +2677,7 @@ static void krylov_multi(Handle *h, int method, const mldg_csr *Acsr, int nrhs, 
   if (mem != MLDG_MEM_HOST && mem != MLDG_MEM_DEVICE) fail(MLDG_ERR_ARG, "bad mem_kind");
   const int n = h->n0;
   if (ldb < n || ldx < n) fail(MLDG_ERR_SIZE, "ldb %d / ldx %d < n %d", ldb, ldx, n);
+  if (kcycle_handle(h)) fail(MLDG_ERR_ARG, "the K-cycle is applied column by column: use mldg_krylov per column");
   DCSR<double> A = h->A0;
   Arena tmp;
   if (Acsr) {
@@ -2655,6 +2814,7 @@ static void krylov_batch(int nsys, Handle **hs, int method, const double *const 
     if (!hs[i]) fail(MLDG_ERR_ARG, "system %d: null handle", i);
     if (!hs[i]->finalized) fail(MLDG_ERR_NOT_BUILT, "system %d: krylov before build", i);
     if (hs[i]->opts.device != dev) fail(MLDG_ERR_ARG, "system %d: handles on different devices", i);
+    if (kcycle_handle(hs[i])) fail(MLDG_ERR_ARG, "system %d: K-cycle iterations are not captured; use mldg_krylov", i);
     if (!b[i] || !x[i]) fail(MLDG_ERR_ARG, "system %d: null vector", i);
     for (int k = 0; k < i; ++k)
       if (hs[k] == hs[i]) fail(MLDG_ERR_ARG, "system %d: handle repeated", i);
@@ -2838,7 +2998,7 @@ extern "C" int mldg_set_cycle(mldg_handle *hp, int cycle) {
   if (!hp) return MLDG_ERR_ARG;
   MLDG_GUARD(hp, {
     Handle &h = hp->h;
-    if (cycle != MLDG_CYCLE_V && cycle != MLDG_CYCLE_W) mldg::fail(MLDG_ERR_ARG, "unknown cycle %d", cycle);
+    if (cycle < MLDG_CYCLE_V || cycle > MLDG_CYCLE_KSYM) mldg::fail(MLDG_ERR_ARG, "unknown cycle %d", cycle);
     if (h.cycle != cycle) {
       h.cycle = cycle;
       for (int t = 0; t < 2; ++t)

@@ -631,6 +631,11 @@ static void jac_smoother_apply(orc_prec *p, int l, char trans, double alpha,
 }
 
 /* V-cycle body: mlprec/impl/mld_dmlprec_aply.f90:590-809 (ml_cycle=VCYCLE) */
+static void inner_k_cycle(orc_prec *p, int l, char trans);
+
+/* dispatch on ml_cycle (mld_dmlprec_aply.f90:418-460 inner_ml_aply) */
+static void inner_ml_aply(orc_prec *p, int l, char trans);
+
 static void inner_mult(orc_prec *p, int l, char trans) {
   level *lv = &p->lv[l];
   int nlev = p->nlev;
@@ -676,6 +681,106 @@ static void inner_mult(orc_prec *p, int l, char trans) {
     /* coarsest level (:787-793) */
     jac_smoother_apply(p, l, trans, 1.0, x, 0.0, y, spre, 0);
   }
+}
+
+static void inner_ml_aply(orc_prec *p, int l, char trans) {
+  if (p->par.ml_cycle == ORC_KCYCLE || p->par.ml_cycle == ORC_KCYCLESYM)
+    inner_k_cycle(p, l, trans);
+  else
+    inner_mult(p, l, trans);
+}
+
+/* K-cycle inner iteration at level l (mld_dinneritkcycle,
+ * mld_dmlprec_aply.f90:1017-1184): at most two steps of flexible CG (FCG,
+ * KCYCLESYM) or GCR (KCYCLE) on A_l with the level's own cycle as
+ * preconditioner; the second step only when the first left
+ * ||w|| > 0.25 ||rhs||.  The inner products use A_l (no transpose) for
+ * either trans, as the reference does. */
+static void inneritkcycle(orc_prec *p, int l, char trans, int gcr) {
+  level *lv = &p->lv[l];
+  int n = lv->A.nr;
+  size_t nb = sizeof(double) * (size_t)n;
+  double *w = (double *)xcalloc((size_t)n, sizeof(double));
+  double *v = (double *)xcalloc((size_t)n, sizeof(double));
+  double *v1 = (double *)xcalloc((size_t)n, sizeof(double));
+  double *xk = (double *)xcalloc((size_t)n, sizeof(double));
+  double *d0 = (double *)xcalloc((size_t)n, sizeof(double));
+  double *d1 = (double *)xcalloc((size_t)n, sizeof(double));
+  memcpy(w, p->x2l[l], nb);
+  double delta0 = sqrt(dot(n, w, w));
+  memset(p->y2l[l], 0, nb);
+  inner_ml_aply(p, l, trans);
+  memcpy(d0, p->y2l[l], nb);
+  orc_spmv(n, lv->A.irp, lv->A.ja, lv->A.val, 1.0, d0, 0.0, v);
+  double delta_old, tau;
+  if (gcr) {
+    delta_old = dot(n, v, w);
+    tau = dot(n, v, v);
+  } else {
+    delta_old = dot(n, d0, w);
+    tau = dot(n, d0, v);
+  }
+  double alpha = delta_old / tau;
+  for (int i = 0; i < n; i++) w[i] = -alpha * v[i] + w[i];
+  double l2 = sqrt(dot(n, w, w));
+  if (l2 <= 0.25 * delta0) {
+    for (int i = 0; i < n; i++) xk[i] = alpha * d0[i] + xk[i];
+  } else {
+    memcpy(p->x2l[l], w, nb);
+    inner_ml_aply(p, l, trans);
+    memcpy(d1, p->y2l[l], nb);
+    orc_spmv(n, lv->A.irp, lv->A.ja, lv->A.val, 1.0, d1, 0.0, v1);
+    double tau1, tau2, tau3;
+    if (gcr) {
+      tau1 = dot(n, v1, v);
+      tau2 = dot(n, v1, v1);
+      tau3 = dot(n, v1, w);
+    } else {
+      tau1 = dot(n, d1, v);
+      tau2 = dot(n, d1, v1);
+      tau3 = dot(n, d1, w);
+    }
+    double tau4 = tau2 - (tau1 * tau1) / tau;
+    alpha = alpha - (tau1 * tau3) / (tau * tau4);
+    for (int i = 0; i < n; i++) xk[i] = alpha * d0[i] + xk[i];
+    alpha = tau3 / tau4;
+    for (int i = 0; i < n; i++) xk[i] = alpha * d1[i] + xk[i];
+  }
+  memcpy(p->y2l[l], xk, nb);
+  free(w);
+  free(v);
+  free(v1);
+  free(xk);
+  free(d0);
+  free(d1);
+}
+
+/* K-cycle body (mld_d_inner_k_cycle, mld_dmlprec_aply.f90:811-1000): pre
+ * smoothing, restriction, the inner Krylov iteration on the next level (a
+ * plain cycle call on the coarsest two), prolongation, post smoothing. */
+static void inner_k_cycle(orc_prec *p, int l, char trans) {
+  level *lv = &p->lv[l];
+  int nlev = p->nlev;
+  int n = lv->A.nr;
+  int spre = lv->sweeps_pre, spost = lv->sweeps_post;
+  double *x = p->x2l[l], *y = p->y2l[l], *ty = p->ty[l];
+  if (l == nlev - 1) {
+    jac_smoother_apply(p, l, trans, 1.0, x, 0.0, y, spre, 0);
+    return;
+  }
+  level *lc = &p->lv[l + 1];
+  jac_smoother_apply(p, l, trans, 1.0, x, 0.0, y, trans == 'N' ? spre : spost, trans == 'N' ? 0 : 1);
+  memcpy(ty, x, sizeof(double) * (size_t)n);
+  spmv_op(&lv->A, trans, -1.0, y, 1.0, ty);
+  orc_spmv(lc->R.nr, lc->R.irp, lc->R.ja, lc->R.val, 1.0, ty, 0.0, p->x2l[l + 1]);
+  if (l + 1 <= nlev - 2)
+    inneritkcycle(p, l + 1, trans, p->par.ml_cycle == ORC_KCYCLE);
+  else
+    inner_ml_aply(p, l + 1, trans);
+  orc_spmv(lc->P.nr, lc->P.irp, lc->P.ja, lc->P.val, 1.0, p->y2l[l + 1], 1.0, y);
+  memcpy(ty, x, sizeof(double) * (size_t)n);
+  spmv_op(&lv->A, trans, -1.0, y, 1.0, ty);
+  jac_smoother_apply(p, l, trans, 1.0, ty, 1.0, y, trans == 'N' ? spost : spre, trans == 'N' ? 1 : 0);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -979,7 +1084,7 @@ int orc_prec_apply(orc_prec *p, const double *x, double *y, char trans) {
     jac_smoother_apply(p, 0, trans, 1.0, p->x2l[0], 0.0, p->y2l[0],
                        p->lv[0].sweeps_pre, 0);
   } else {
-    inner_mult(p, 0, trans);
+    inner_ml_aply(p, 0, trans);
   }
   memcpy(y, p->y2l[0], sizeof(double) * (size_t)n);
   return 0;

@@ -41,7 +41,8 @@ typedef struct {
   int ml_cycle;        /* ORC_VCYCLE (default) or ORC_WCYCLE */
 } orc_params;
 
-enum { ORC_VCYCLE = 0, ORC_WCYCLE = 1 };
+/* KCYCLE: inner GCR; KCYCLESYM: inner flexible CG (mld_base_prec_type.F90:220-221) */
+enum { ORC_VCYCLE = 0, ORC_WCYCLE = 1, ORC_KCYCLE = 2, ORC_KCYCLESYM = 3 };
 
 typedef struct orc_prec orc_prec;
 

@@ -127,6 +127,21 @@ def test_wcycle_symmetric_and_not_weaker(orc):
     assert its[orc.WCYCLE] <= its[orc.VCYCLE]
 
 
+@pytest.mark.parametrize("cycle", ["KCYCLE", "KCYCLESYM"])
+def test_kcycle_converges(orc, cycle):
+    """K-cycle with inner GCR / flexible CG (a nonlinear preconditioner, so
+    FCG is the outer method): converges to the same solution as the V-cycle."""
+    a = orc.gen_pde3d(16, 1, ISO)
+    b = orc.spmv(a, np.ones(a.nrows))
+    par = oracle_params(orc, "BJAC", 1, coarse_sweeps=4, mcs=40)
+    par.ml_cycle = getattr(orc, cycle)
+    p = orc.Prec(par)
+    p.build(a)
+    assert p.nlev >= 3
+    x, it, rr, _ = orc.krylov("FCG", a, p, b, eps=1e-10)
+    assert rr <= 1e-10 and np.abs(x - 1.0).max() <= 1e-7
+
+
 def test_hierarchy_invariants(orc):
     a = orc.gen_pde3d(16, 1, ISO)
     p = orc.Prec(oracle_params(orc, "BJAC", mcs=150))
