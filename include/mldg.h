@@ -142,6 +142,9 @@ int mldg_finalize(mldg_handle *h, int nlev, int precision);
 #define MLDG_CYCLE_W 1
 #define MLDG_CYCLE_K 2
 #define MLDG_CYCLE_KSYM 3
+/* MLDG_CYCLE_ADD: the additive cycle, smoothing and coarse corrections of the
+ * restricted input summed (mld_dmlprec_aply.f90:464-588, ML_CYCLE='ADD') */
+#define MLDG_CYCLE_ADD 4
 int mldg_set_cycle(mldg_handle *h, int cycle);
 
 /* y = M^{-1} x (trans 'N') or y = M^{-T} x (trans 'T'/'C') for nrhs vectors

@@ -154,6 +154,8 @@ static int set_common(mldp_prec *p, const std::string &w, const std::string *sv,
       p->cycle = MLDG_CYCLE_K;
     else if (v == "KCYCLESYM")
       p->cycle = MLDG_CYCLE_KSYM;
+    else if (v == "ADD")
+      p->cycle = MLDG_CYCLE_ADD;
     else if (p->unsupported.empty())
       p->unsupported = w + "=" + v;
   } else if (w == "COARSE_SOLVE") {

@@ -820,8 +820,33 @@ struct EngineT : Engine {
   void cycle_at(int l, char trans) {
     if (kcycle_mode())
       kcycle(l, trans);
+    else if (cycle == MLDG_CYCLE_ADD)
+      addcycle(l, trans);
     else
       vcycle(l, trans);
+  }
+  // additive cycle (mld_d_inner_add, mld_dmlprec_aply.f90:464-588): smooth x,
+  // restrict x itself, recurse, add the prolongated correction.  FBGS levels
+  // apply forward then backward GS max(sweeps) times from the previous result.
+  void addcycle(int l, char trans) {
+    cur_lev = l;
+    Lev &L = lv[l];
+    if (L.kind == MLDG_SMOOTHER_FBGS) {
+      copy(L.n, L.x, L.y);
+      for (int k = 0; k < std::max(L.spre, L.spost); ++k) {
+        fbgs_solve(L, false, L.y, L.tw, T(0));
+        fbgs_solve(L, true, L.tw, L.y, T(0));
+      }
+    } else {
+      smoother(L, trans, L.x, T(0), L.y, L.spre);
+    }
+    if (l < (int)lv.size() - 1) {
+      Lev &C = lv[l + 1];
+      spmv(C.R, L.x, T(1), nullptr, T(0), C.x, T(0));
+      cycle_at(l + 1, trans);
+      cur_lev = l;
+      prolong(C, L.y);
+    }
   }
   void kcycle(int l, char trans) {
     cur_lev = l;
@@ -1392,6 +1417,26 @@ struct EngineT : Engine {
       smoother_m(L, trans, L.xm, T(0), L.ym, L.spre);
     }
   }
+  void addcycle_m(int l, char trans) {
+    cur_lev = l;
+    Lev &L = lv[l];
+    if (L.kind == MLDG_SMOOTHER_FBGS) {
+      axpby_m(L.n, L.xm, T(0), L.ym);
+      for (int k = 0; k < std::max(L.spre, L.spost); ++k) {
+        fbgs_solve_m(L, false, L.ym, L.twm, T(0));
+        fbgs_solve_m(L, true, L.twm, L.ym, T(0));
+      }
+    } else {
+      smoother_m(L, trans, L.xm, T(0), L.ym, L.spre);
+    }
+    if (l < (int)lv.size() - 1) {
+      Lev &C = lv[l + 1];
+      spmm(C.R, L.xm, T(1), nullptr, T(0), C.xm, T(0));
+      addcycle_m(l + 1, trans);
+      cur_lev = l;
+      prolong_m(C, L.ym);
+    }
+  }
   void record_multi(char trans, int Kw) override {
     if (Kw > mcap) fail(MLDG_ERR_INTERNAL, "multi buffers not allocated for %d columns", Kw);
     if (kcycle_mode()) fail(MLDG_ERR_ARG, "the K-cycle has no multi-column form");
@@ -1419,6 +1464,8 @@ struct EngineT : Engine {
       if (nsw == 0) axpby_m(F.n, F.xm, T(0), F.ym);
     } else if (lv.size() == 1) {
       smoother_m(F, trans, F.xm, T(0), F.ym, F.spre);
+    } else if (cycle == MLDG_CYCLE_ADD) {
+      addcycle_m(0, trans);
     } else {
       vcycle_m(0, trans);
     }
@@ -1518,6 +1565,8 @@ struct EngineT : Engine {
     } else if (kcycle_mode()) {
       ensure_k();
       kcycle(0, trans);
+    } else if (cycle == MLDG_CYCLE_ADD) {
+      addcycle(0, trans);
     } else {
       vcycle(0, trans);
     }
@@ -2998,7 +3047,7 @@ extern "C" int mldg_set_cycle(mldg_handle *hp, int cycle) {
   if (!hp) return MLDG_ERR_ARG;
   MLDG_GUARD(hp, {
     Handle &h = hp->h;
-    if (cycle < MLDG_CYCLE_V || cycle > MLDG_CYCLE_KSYM) mldg::fail(MLDG_ERR_ARG, "unknown cycle %d", cycle);
+    if (cycle < MLDG_CYCLE_V || cycle > MLDG_CYCLE_ADD) mldg::fail(MLDG_ERR_ARG, "unknown cycle %d", cycle);
     if (h.cycle != cycle) {
       h.cycle = cycle;
       for (int t = 0; t < 2; ++t)

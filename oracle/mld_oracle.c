@@ -683,9 +683,36 @@ static void inner_mult(orc_prec *p, int l, char trans) {
   }
 }
 
+/* additive cycle (mld_d_inner_add, mld_dmlprec_aply.f90:464-588): smooth x
+ * (FBGS: max(sweeps) times forward then backward GS, each from the previous
+ * result), restrict x itself, recurse, add the prolongated correction */
+static void inner_add(orc_prec *p, int l, char trans) {
+  level *lv = &p->lv[l];
+  int n = lv->A.nr;
+  double *x = p->x2l[l], *y = p->y2l[l], *tx = p->tx[l];
+  if (lv->smoother == ORC_FBGS) {
+    memcpy(y, x, sizeof(double) * (size_t)n);
+    int sw = lv->sweeps_pre > lv->sweeps_post ? lv->sweeps_pre : lv->sweeps_post;
+    for (int k = 0; k < sw; k++) {
+      jac_smoother_apply(p, l, trans, 1.0, y, 0.0, tx, 1, 0);
+      jac_smoother_apply(p, l, trans, 1.0, tx, 0.0, y, 1, 1);
+    }
+  } else {
+    jac_smoother_apply(p, l, trans, 1.0, x, 0.0, y, lv->sweeps_pre, 0);
+  }
+  if (l < p->nlev - 1) {
+    level *lc = &p->lv[l + 1];
+    orc_spmv(lc->R.nr, lc->R.irp, lc->R.ja, lc->R.val, 1.0, x, 0.0, p->x2l[l + 1]);
+    inner_ml_aply(p, l + 1, trans);
+    orc_spmv(lc->P.nr, lc->P.irp, lc->P.ja, lc->P.val, 1.0, p->y2l[l + 1], 1.0, y);
+  }
+}
+
 static void inner_ml_aply(orc_prec *p, int l, char trans) {
   if (p->par.ml_cycle == ORC_KCYCLE || p->par.ml_cycle == ORC_KCYCLESYM)
     inner_k_cycle(p, l, trans);
+  else if (p->par.ml_cycle == ORC_ADD)
+    inner_add(p, l, trans);
   else
     inner_mult(p, l, trans);
 }

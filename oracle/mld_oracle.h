@@ -42,7 +42,7 @@ typedef struct {
 } orc_params;
 
 /* KCYCLE: inner GCR; KCYCLESYM: inner flexible CG (mld_base_prec_type.F90:220-221) */
-enum { ORC_VCYCLE = 0, ORC_WCYCLE = 1, ORC_KCYCLE = 2, ORC_KCYCLESYM = 3 };
+enum { ORC_VCYCLE = 0, ORC_WCYCLE = 1, ORC_KCYCLE = 2, ORC_KCYCLESYM = 3, ORC_ADD = 4 };
 
 typedef struct orc_prec orc_prec;
 

@@ -18,7 +18,7 @@ _lib = None
 
 JACOBI = 1
 BJAC = 2
-VCYCLE, WCYCLE, KCYCLE, KCYCLESYM = 0, 1, 2, 3  # ml_cycle
+VCYCLE, WCYCLE, KCYCLE, KCYCLESYM, ADD = 0, 1, 2, 3, 4  # ml_cycle
 FBGS = 3  # forward GS pre / backward GS post (jac smoother + GS / BWGS solvers)
 
 

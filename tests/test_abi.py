@@ -53,7 +53,7 @@ def test_host_mirror_set_and_build_errors(mld):
     assert "SMOOTHER_TYPE" in str(e.value)
     p.init("ML")
     p.set("SMOOTHER_TYPE", "BJAC")
-    p.set("ML_CYCLE", "ADD")
+    p.set("ML_CYCLE", "NO_SUCH_CYCLE")
     with pytest.raises(mld.MldError) as e:
         p.hierarchy_build(a)
     assert "ML_CYCLE" in str(e.value)

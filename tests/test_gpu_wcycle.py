@@ -60,3 +60,22 @@ def test_wcycle_through_host_mirror(mld, orc):
     b = am.matvec(np.ones(am.nrows))
     _, it, rr = mld.krylov("FCG", am, p, b, eps=1e-10, use_prec_matrix=True)
     assert rr <= 1e-10
+
+
+@pytest.mark.parametrize("smoother,sweeps", [("BJAC", 1), ("JACOBI", 2), ("FBGS", 2)])
+def test_additive_cycle_matches_oracle(mld, orc, smoother, sweeps):
+    """ML_CYCLE='ADD' (mld_dmlprec_aply.f90:464-588): single and multi-column."""
+    a = orc.gen_pde3d(20, 1, ISO)
+    par = oracle_params(orc, smoother, sweeps, 0.8 if smoother == "JACOBI" else 1.0, mcs=60)
+    par.ml_cycle = orc.ADD
+    op = orc.Prec(par)
+    op.build(a)
+    assert op.nlev >= 3
+    h = upload_oracle_hierarchy(mld, orc, op)
+    h.set_cycle(mld.CYCLE_ADD)
+    rng = np.random.default_rng(5)
+    x = rng.uniform(-1, 1, a.nrows)
+    assert _rel(h.apply(x), op.apply(x)) <= 1e-12
+    X = rng.uniform(-1, 1, (4, a.nrows))
+    Y = h.apply_block(X)
+    assert max(_rel(Y[c], op.apply(X[c])) for c in range(4)) <= 1e-12
