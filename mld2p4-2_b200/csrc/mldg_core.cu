@@ -367,6 +367,42 @@ struct Engine {
   }
 };
 
+// K identity columns c0 .. c0+K-1 (row-interleaved); rows past n stay zero
+template <typename T>
+__global__ void k_ident_block(int n, int c0, int K, T *x) {
+  const long long tot = (long long)n * K;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t / K), c = (int)(t % K);
+    x[t] = (i == c0 + c) ? T(1) : T(0);
+  }
+}
+// M[i*n + c0 + c] = y[i*K + c] for the columns that exist
+template <typename T>
+__global__ void k_scatter_cols(int n, int c0, int K, const T *__restrict__ y, T *__restrict__ M) {
+  const long long tot = (long long)n * K;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t / K), c = (int)(t % K);
+    if (c0 + c < n) M[(size_t)i * n + c0 + c] = y[t];
+  }
+}
+// MT = M^T (n x n), 32 x 32 tiles through shared memory
+template <typename T>
+__global__ void k_transpose_sq(int n, const T *__restrict__ M, T *__restrict__ MT) {
+  __shared__ T tile[32][33];
+  const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = by + r, j = bx + threadIdx.x;
+    if (i < n && j < n) tile[r][threadIdx.x] = M[(size_t)i * n + j];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = bx + r, j = by + threadIdx.x;
+    if (i < n && j < n) MT[(size_t)i * n + j] = tile[threadIdx.x][r];
+  }
+}
+
 // y = a*x + b*y (b = 1: an axpy as psb_geaxpby(a, x, 1, y))
 template <typename T>
 __global__ void k_axpby2(int n, T a, const T *__restrict__ x, T b, T *y) {
@@ -1117,6 +1153,71 @@ struct EngineT : Engine {
     el.ctr = ar.alloc<int>((size_t)32 * (el.S + 1));
     MLDG_CUDA(cudaMemsetAsync(el.ctr, 0, sizeof(int) * 32 * (el.S + 1), st));
     el.ok = true;
+  }
+  // Explicit inverse M^{-1} = U^{-1} diag(d) L^{-1} of a small level's ILU(0)
+  // (the operator of its solve pair), computed on the GPU 32 identity columns
+  // at a time with the multi-column solves, and its transpose.  Kept when one
+  // dense matrix-vector product beats the two dependency-bound solves.
+  bool dense_inverse(Lev &L, Arena &ar) {
+    const int n = L.n, Kw = 32, ki = 5;
+    if (n < 1 || L.minv || L.kind != MLDG_SMOOTHER_BJAC) return false;
+    Arena tmp;
+    bool ok = true;
+    for (DTri<T> *f : {&L.L, &L.U}) {
+      build_ell(*f, Kw, tmp);
+      ok = ok && f->ell[ki].ok;
+    }
+    T *M = nullptr, *MT = nullptr;
+    if (ok) {
+      const size_t nk = (size_t)n * Kw;
+      T *xm = tmp.alloc<T>(nk), *ym = tmp.alloc<T>(nk), *ba = tmp.alloc<T>(nk), *bb = tmp.alloc<T>(nk);
+      k_fill<T><<<blocks_for((int64_t)nk), 256, 0, st>>>((int)nk, Sentinel<T>::value(), ba);
+      k_fill<T><<<blocks_for((int64_t)nk), 256, 0, st>>>((int)nk, Sentinel<T>::value(), bb);
+      M = ar.alloc<T>((size_t)n * n);
+      MT = ar.alloc<T>((size_t)n * n);
+      const int sK = K;
+      K = Kw;
+      for (int c0 = 0; c0 < n; c0 += Kw) {
+        k_ident_block<T><<<blocks_for((int64_t)nk), 256, 0, st>>>(n, c0, Kw, xm);
+        trsv_m(L.L, xm, nullptr, ba, bb, nullptr, T(1), T(0));
+        trsv_m(L.U, ba, L.d, bb, ba, ym, T(1), T(0));
+        k_scatter_cols<T><<<blocks_for((int64_t)nk), 256, 0, st>>>(n, c0, Kw, ym, M);
+      }
+      K = sK;
+      dim3 tg((n + 31) / 32, (n + 31) / 32), tb(32, 8);
+      k_transpose_sq<T><<<tg, tb, 0, st>>>(n, M, MT);
+      MLDG_CUDA(cudaStreamSynchronize(st));
+    }
+    for (DTri<T> *f : {&L.L, &L.U}) f->ell[ki] = typename DTri<T>::Ell();
+    tmp.release();
+    if (!ok) return false;
+    // keep the dense form only if it is faster
+    cudaEvent_t e0, e1;
+    MLDG_CUDA(cudaEventCreate(&e0));
+    MLDG_CUDA(cudaEventCreate(&e1));
+    float t[2] = {0, 0};
+    for (int v = 0; v < 2; ++v) {
+      L.minv = v ? M : nullptr;
+      L.minvT = v ? MT : nullptr;
+      ilu_apply(L, 'N', L.x, T(0), L.ty);
+      MLDG_CUDA(cudaEventRecord(e0, st));
+      for (int r = 0; r < 3; ++r) ilu_apply(L, 'N', L.x, T(0), L.ty);
+      MLDG_CUDA(cudaEventRecord(e1, st));
+      MLDG_CUDA(cudaEventSynchronize(e1));
+      MLDG_CUDA(cudaEventElapsedTime(&t[v], e0, e1));
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const bool keep = t[1] < t[0] || std::getenv("MLDG_DENSE_INV");
+    if (!keep) {
+      L.minv = L.minvT = nullptr;  // (the matrices stay in the arena until the handle is freed)
+    }
+    if (std::getenv("MLDG_VERBOSE"))
+      std::fprintf(stderr, "mldg: dense ILU inverse n=%d: solves %.3f ms dense %.3f ms -> %s\n", n, t[0] / 3,
+                   t[1] / 3, keep ? "dense" : "solves");
+    launches = 0;
+    bytes = 0;
+    return keep;
   }
   bool ensure_multi(int Kw) override {
     bool grown = false;
@@ -2093,6 +2194,9 @@ static void set_trsv_smem_attr() {
 // (U^{-1} diag(d) L^{-1}), applied as one bandwidth-bound matrix-vector
 // product instead of a chain of dependency levels.
 constexpr int kDenseCoarseRows = 2048;
+// intermediate levels up to this size get a GPU-computed explicit inverse
+// (n^2 values, 2.1 GB at FP64 for the largest) when it applies faster
+constexpr int kDenseInvRows = 16384;
 
 // M = U^{-1} diag(d) L^{-1} (row-major) and its transpose, column by column
 static void dense_ilu_inverse(const HostCSR &Lf, const HostCSR &Uf, const std::vector<double> &d,
@@ -2301,6 +2405,12 @@ static Engine *make_engine(Handle *h) {
     if (!std::getenv("MLDG_ELL1")) e->autotune_ilu(3);
     MLDG_CUDA(cudaStreamSynchronize(h->st));
   }
+  // small intermediate levels: the explicit inverse of their ILU(0) when faster
+  if (!std::getenv("MLDG_NO_DENSE_INV"))
+    for (int l = 1; l < h->nlev; ++l) {
+      auto &L = e->lv[l];
+      if (L.kind == MLDG_SMOOTHER_BJAC && !L.minv && L.n <= kDenseInvRows) e->dense_inverse(L, ar);
+    }
   return e;
 }
 

@@ -118,3 +118,23 @@ def test_apply_large_coarse_level(mld, orc):
     for trans in ("N", "T"):
         x = rng.uniform(-1, 1, a.nrows)
         assert _rel(h.apply(x, trans=trans), op.apply(x, trans)) <= TOL_FP64
+
+
+@pytest.mark.parametrize("idim,coef", [(20, ISO), (28, ANISO)])
+def test_dense_inverse_levels_match_oracle(mld, orc, monkeypatch, idim, coef):
+    """Every BJAC level below the finest applied through the explicit inverse
+    of its ILU(0), computed on the GPU column block by column block."""
+    monkeypatch.setenv("MLDG_DENSE_INV", "1")
+    a = orc.gen_pde3d(idim, 1, coef)
+    op = orc.Prec(oracle_params(orc, "BJAC", mcs=60))
+    op.build(a)
+    assert op.nlev >= 3
+    for precision, tol in ((0, TOL_FP64), (1, TOL_FP32)):
+        h = upload_oracle_hierarchy(mld, orc, op, precision=precision)
+        rng = np.random.default_rng(idim)
+        for trans in ("N", "T"):
+            x = rng.uniform(-1, 1, a.nrows)
+            assert _rel(h.apply(x, trans=trans), op.apply(x, trans)) <= tol
+        X = rng.uniform(-1, 1, (3, a.nrows))
+        Y = h.apply_block(X)
+        assert max(_rel(Y[c], op.apply(X[c])) for c in range(3)) <= tol
