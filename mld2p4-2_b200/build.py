@@ -56,7 +56,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, os.path.basename(src) + ".o")
         if force or _stale(o, [s] + headers):
-            out = _run([nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-Werror=return-type",
+            out = _run([nvcc, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-fopenmp,-Werror=return-type",
                         "-Xptxas", "-v", "-I", INC, "-I", CSRC, "-c", s, "-o", o])
             with open(os.path.join(BUILD, os.path.basename(src) + ".ptxas.txt"), "w") as f:
                 f.write(out)

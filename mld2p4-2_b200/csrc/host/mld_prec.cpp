@@ -6,7 +6,9 @@
 // the mldg C ABI.  apply and the Krylov driver then run on the device.
 #include <algorithm>
 #include <cctype>
+#include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -255,9 +257,16 @@ extern "C" int mldp_smoothers_build(mldp_prec *p) {
   if (!p) return MLDG_ERR_ARG;
   if (!p->hier_built) return fail(p, 3112, "smoothers_build before hierarchy_build");
   std::string msg;
+  const auto t0 = std::chrono::steady_clock::now();
   int rc = mld::smoothers_build(p->lv, p->parms, msg);
   if (rc) return fail(p, rc, msg);
-  return upload_all(p);
+  const auto t1 = std::chrono::steady_clock::now();
+  rc = upload_all(p);
+  if (std::getenv("MLDG_TIMING"))
+    std::fprintf(stderr, "mldg timing: host smoothers (ILU(0), GS split) %.3f s, upload + finalize %.3f s\n",
+                 std::chrono::duration<double>(t1 - t0).count(),
+                 std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count());
+  return rc;
 }
 
 // the finished host levels -> the GPU handle (mldg_upload_level + finalize)

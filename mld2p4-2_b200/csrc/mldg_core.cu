@@ -11,7 +11,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <map>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -21,6 +23,8 @@
 #include <string>
 #include <type_traits>
 #include <vector>
+
+#include <omp.h>
 
 #include "mldg.h"
 #include "mldg_kernels.cuh"
@@ -93,13 +97,36 @@ static HostCSR transpose(const HostCSR &a) {
   t.val.resize((size_t)nnz);
   for (int64_t k = 0; k < nnz; ++k) t.irp[a.ja[k] + 1]++;
   for (int j = 0; j < t.nr; ++j) t.irp[j + 1] += t.irp[j];
-  std::vector<int> fill(t.irp.begin(), t.irp.end() - 1);
-  for (int i = 0; i < a.nr; ++i)
-    for (int k = a.irp[i]; k < a.irp[i + 1]; ++k) {
-      const int p = fill[a.ja[k]]++;
-      t.ja[p] = i;
-      t.val[p] = a.val[k];
+  // rows of the transpose in source-row order (sorted columns): each thread
+  // owns a contiguous block of source rows and fills from per-thread
+  // starting offsets computed by a column-count prefix over the blocks
+  const int nt = std::max(1, std::min(omp_get_max_threads(), a.nr / 4096 + 1));
+  std::vector<std::vector<int>> cnt((size_t)nt);
+#pragma omp parallel num_threads(nt)
+  {
+    const int tid = omp_get_thread_num();
+    const int i0 = (int)((int64_t)a.nr * tid / nt), i1 = (int)((int64_t)a.nr * (tid + 1) / nt);
+    std::vector<int> &c = cnt[(size_t)tid];
+    c.assign((size_t)t.nr, 0);
+    for (int i = i0; i < i1; ++i)
+      for (int k = a.irp[i]; k < a.irp[i + 1]; ++k) c[a.ja[k]]++;
+#pragma omp barrier
+#pragma omp for schedule(static)
+    for (int j = 0; j < t.nr; ++j) {
+      int off = t.irp[j];
+      for (int q = 0; q < nt; ++q) {
+        const int v = cnt[(size_t)q][j];
+        cnt[(size_t)q][j] = off;
+        off += v;
+      }
     }
+    for (int i = i0; i < i1; ++i)
+      for (int k = a.irp[i]; k < a.irp[i + 1]; ++k) {
+        const int p = c[a.ja[k]]++;
+        t.ja[p] = i;
+        t.val[p] = a.val[k];
+      }
+  }
   return t;
 }
 
@@ -226,15 +253,13 @@ static DCSR<T> to_dev(Arena &ar, const HostCSR &h) {
   d.irp = ar.upload(h.irp);
   d.ja = ar.upload(h.ja);
   if (h.nr == h.nc && !std::getenv("MLDG_NO_IDX16")) {
-    bool fits = true;
-    for (int i = 0; i < h.nr && fits; ++i)
-      for (int k = h.irp[i]; k < h.irp[i + 1]; ++k)
-        if (std::abs(h.ja[k] - i) > 32767) {
-          fits = false;
-          break;
-        }
-    if (fits) {
+    int bad = 0;
+#pragma omp parallel for reduction(| : bad) schedule(static, 4096)
+    for (int i = 0; i < h.nr; ++i)
+      for (int k = h.irp[i]; k < h.irp[i + 1]; ++k) bad |= std::abs(h.ja[k] - i) > 32767;
+    if (!bad) {
       std::vector<short> jd(h.ja.size());
+#pragma omp parallel for schedule(static, 4096)
       for (int i = 0; i < h.nr; ++i)
         for (int k = h.irp[i]; k < h.irp[i + 1]; ++k) jd[k] = (short)(h.ja[k] - i);
       d.jd = ar.upload(jd);
@@ -1074,35 +1099,47 @@ struct EngineT : Engine {
     }
     if (slots >= (int64_t)INT32_MAX) return;
     std::vector<int> prow((size_t)npad, -1), ej((size_t)std::max<int64_t>(slots, 1), -1),
-        ovp((size_t)npad + 1, 0), ovj;
-    std::vector<T> ev((size_t)std::max<int64_t>(slots, 1), T(0)), ovv;
-    std::vector<int> ord;
+        ovp((size_t)npad + 1, 0);
+    std::vector<T> ev((size_t)std::max<int64_t>(slots, 1), T(0));
+    // overflow offsets first (a prefix over the positions), then every
+    // position fills its slots and overflow range independently
     for (int64_t pp = 0; pp < npad; ++pp) {
       const int p = pos[pp];
-      ovp[pp + 1] = ovp[pp];
-      if (p < 0) continue;
-      const int tk = (int)(pp / rpw), g = (int)(pp % rpw), et = toff[tk].y;
-      const int i = t.h_prow[p];
-      prow[pp] = t.rev ? t.n - 1 - i : i;
-      const int k0 = t.h_pirp[p], len = t.h_pirp[p + 1] - k0;
-      ord.resize(len);
-      for (int e = 0; e < len; ++e) ord[e] = k0 + e;
-      std::stable_sort(ord.begin(), ord.end(),
-                       [&](int x, int y) { return lev_of[t.h_pja[x]] < lev_of[t.h_pja[y]]; });
-      const int nov = std::max(0, len - et);
-      for (int e = 0; e < len; ++e) {
-        const int k = ord[e], jj = t.h_pja[k];
-        const int oj = t.rev ? t.n - 1 - jj : jj;
-        if (e < nov) {
-          ovj.push_back(oj);
-          ovv.push_back((T)t.h_pval[k]);
-        } else {
-          const size_t q = (size_t)toff[tk].x + (size_t)(e - nov) * rpw + g;
-          ej[q] = oj;
-          ev[q] = (T)t.h_pval[k];
+      int nov = 0;
+      if (p >= 0) nov = std::max(0, t.h_pirp[p + 1] - t.h_pirp[p] - toff[(size_t)(pp / rpw)].y);
+      ovp[pp + 1] = ovp[pp] + nov;
+    }
+    std::vector<int> ovj((size_t)ovp[npad]);
+    std::vector<T> ovv((size_t)ovp[npad]);
+#pragma omp parallel
+    {
+      std::vector<int> ord;
+#pragma omp for schedule(static, 1024)
+      for (int64_t pp = 0; pp < npad; ++pp) {
+        const int p = pos[pp];
+        if (p < 0) continue;
+        const int tk = (int)(pp / rpw), g = (int)(pp % rpw), et = toff[tk].y;
+        const int i = t.h_prow[p];
+        prow[pp] = t.rev ? t.n - 1 - i : i;
+        const int k0 = t.h_pirp[p], len = t.h_pirp[p + 1] - k0;
+        ord.resize(len);
+        for (int e = 0; e < len; ++e) ord[e] = k0 + e;
+        std::stable_sort(ord.begin(), ord.end(),
+                         [&](int x, int y) { return lev_of[t.h_pja[x]] < lev_of[t.h_pja[y]]; });
+        const int nov = std::max(0, len - et);
+        for (int e = 0; e < len; ++e) {
+          const int k = ord[e], jj = t.h_pja[k];
+          const int oj = t.rev ? t.n - 1 - jj : jj;
+          if (e < nov) {
+            ovj[(size_t)ovp[pp] + e] = oj;
+            ovv[(size_t)ovp[pp] + e] = (T)t.h_pval[k];
+          } else {
+            const size_t q = (size_t)toff[tk].x + (size_t)(e - nov) * rpw + g;
+            ej[q] = oj;
+            ev[q] = (T)t.h_pval[k];
+          }
         }
       }
-      ovp[pp + 1] = (int)ovj.size();
     }
     el.npad = (int)npad;
     el.ntask = ntask;
@@ -2071,11 +2108,6 @@ static DTri<T> build_tri_dev(Arena &ar, const HostCSR &m, bool upper, int nsm) {
   t.n = n;
   t.rev = upper ? 1 : 0;
   t.nlevels = (int)s.lvl_ptr.size() - 1;
-  t.h_lvl = s.lvl_ptr;
-  t.h_prow = s.prow;
-  t.h_pirp = s.pirp;
-  t.h_pja = s.pja;
-  t.h_pval = s.pval;
   t.nnz = m.nnz();
   t.lvl_ptr = ar.upload(s.lvl_ptr);
   t.prow = ar.upload(s.prow);
@@ -2083,6 +2115,13 @@ static DTri<T> build_tri_dev(Arena &ar, const HostCSR &m, bool upper, int nsm) {
   t.pja = ar.upload(s.pja);
   std::vector<T> v(s.pval.begin(), s.pval.end());
   t.pval = ar.upload(v);
+  // host copies of the schedule for the ELL and multi-column plans (moved
+  // after the uploads; the staged-plan code below only reads lvl_ptr/pirp)
+  t.h_lvl = s.lvl_ptr;
+  t.h_prow = s.prow;
+  t.h_pirp = s.pirp;
+  t.h_pja = std::move(s.pja);
+  t.h_pval = std::move(s.pval);
   t.counters = ar.alloc<int>(2);
   MLDG_CUDA(cudaMemset(t.counters, 0, 2 * sizeof(int)));
   // lanes per row: smallest power of two with <= 8 entries per lane
@@ -2230,6 +2269,14 @@ static void dense_ilu_inverse(const HostCSR &Lf, const HostCSR &Uf, const std::v
 
 template <typename T>
 static Engine *make_engine(Handle *h) {
+  // MLDG_TIMING: host time of each finalize phase
+  std::map<std::string, double> tm;
+  auto clk = std::chrono::steady_clock::now();
+  auto tick = [&](const char *what) {
+    const auto now = std::chrono::steady_clock::now();
+    tm[what] += std::chrono::duration<double>(now - clk).count();
+    clk = now;
+  };
   set_trsv_smem_attr<T>();
   auto *e = new EngineT<T>();
   e->h = h;
@@ -2255,7 +2302,9 @@ static Engine *make_engine(Handle *h) {
     L.spost = H.sweeps_post;
     L.damp = H.damp;
     L.A = to_dev<T>(ar, H.A);
+    tick("A upload");
     L.AT = to_dev<T>(ar, transpose(H.A));
+    tick("A^T transpose + upload");
     if (l > 0) {
       L.P = to_dev<T>(ar, H.P);
       L.R = to_dev<T>(ar, H.R);
@@ -2275,6 +2324,7 @@ static Engine *make_engine(Handle *h) {
       }
     }
     L.nnz_nd = H.ND.nnz();
+    tick("matrices (A, A^T, P, R upload)");
     if (H.kind == MLDG_SMOOTHER_BJAC && !std::getenv("MLDG_NO_WIN")) {
       const int n = H.A.nr;
       // Single-CTA windows win on small levels; large levels stay on the
@@ -2309,12 +2359,15 @@ static Engine *make_engine(Handle *h) {
         }
       }
     }
+    tick("window plans");
     // level schedules of the four factors: the single-vector solve where no
     // window plan was taken, and always the multi-RHS solve (k_trsv_sf_m)
     if (H.kind == MLDG_SMOOTHER_BJAC) {
       L.L = build_tri_dev<T>(ar, H.L, false, h->nsm);
       L.U = build_tri_dev<T>(ar, H.U, true, h->nsm);
+      tick("L, U schedules");
       HostCSR Lt = transpose(H.L), Ut = transpose(H.U);
+      tick("L^T, U^T transposes");
       L.Ut = build_tri_dev<T>(ar, Ut, false, h->nsm);  // U^T is lower
       L.Lt = build_tri_dev<T>(ar, Lt, true, h->nsm);   // L^T is upper
       if (std::getenv("MLDG_VERBOSE") && !L.win) {
@@ -2329,6 +2382,7 @@ static Engine *make_engine(Handle *h) {
                        ts[q]->smem, ts[q]->grid);
       }
     }
+    tick("level schedules");
     std::vector<double> dh = H.d;
     if (H.kind == MLDG_SMOOTHER_FBGS) {
       // (D+L)^{-1} and (D+U)^{-1} as unit-triangular solves of the rows
@@ -2351,6 +2405,7 @@ static Engine *make_engine(Handle *h) {
       L.ND = to_dev<T>(ar, H.ND);
       L.NDT = to_dev<T>(ar, transpose(H.ND));
     }
+    tick("FBGS factors, ND");
     if (H.kind == MLDG_SMOOTHER_BJAC && l == h->nlev - 1 && h->nlev > 1 && L.n <= kDenseCoarseRows &&
         !std::getenv("MLDG_NO_DENSE_COARSE")) {
       std::vector<double> M, MT;
@@ -2359,6 +2414,7 @@ static Engine *make_engine(Handle *h) {
       L.minv = ar.upload(m);
       L.minvT = ar.upload(mt);
     }
+    tick("dense coarsest inverse");
     std::vector<T> dv(dh.begin(), dh.end());
     L.d = ar.upload(dv);
     const int n = std::max(L.n, 1);
@@ -2381,6 +2437,7 @@ static Engine *make_engine(Handle *h) {
       L.bufB = ar.alloc<T>(n);
       k_fill<T><<<64, 256, 0, h->st>>>(n, Sentinel<T>::value(), L.bufA);
       k_fill<T><<<64, 256, 0, h->st>>>(n, Sentinel<T>::value(), L.bufB);
+      tick("vectors, exchange buffers");
       if (!L.minv) {
         bool ok = true;
         for (DTri<T> *f : {&L.L, &L.U, &L.Ut, &L.Lt}) {
@@ -2388,6 +2445,7 @@ static Engine *make_engine(Handle *h) {
           e->build_ell(*f, 1, ar);
           ok = ok && f->ell[0].ok;
         }
+        tick("ELL plans (one column)");
         const char *ev = std::getenv("MLDG_ELL1");
         L.ell1 = ok && !(ev && ev[0] == '0');
       }
@@ -2401,16 +2459,22 @@ static Engine *make_engine(Handle *h) {
     e->tune_buf[0] = ar.alloc<T>(nmax);
     e->tune_buf[1] = ar.alloc<T>(nmax);
     k_fill<T><<<64, 256, 0, h->st>>>(nmax, T(1), e->tune_buf[0]);
+    tick("ELL plans");
     e->autotune_spmv(5);
+    tick("autotune SpMV");
     if (!std::getenv("MLDG_ELL1")) e->autotune_ilu(3);
     MLDG_CUDA(cudaStreamSynchronize(h->st));
   }
   // small intermediate levels: the explicit inverse of their ILU(0) when faster
+  tick("autotune solves");
   if (!std::getenv("MLDG_NO_DENSE_INV"))
     for (int l = 1; l < h->nlev; ++l) {
       auto &L = e->lv[l];
       if (L.kind == MLDG_SMOOTHER_BJAC && !L.minv && L.n <= kDenseInvRows) e->dense_inverse(L, ar);
     }
+  tick("dense level inverses");
+  if (std::getenv("MLDG_TIMING"))
+    for (auto &kv : tm) std::fprintf(stderr, "mldg timing: finalize %-32s %.3f s\n", kv.first.c_str(), kv.second);
   return e;
 }
 

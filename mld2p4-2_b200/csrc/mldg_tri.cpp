@@ -49,17 +49,23 @@ void build_tri_schedule(int n, const int *irp, const int *ja, const double *val,
   }
   s->chunk_lvl[s->nchunks] = (int)s->lvl_ptr.size();
   s->lvl_ptr.push_back(n);
+  // rows in position order: offsets by a prefix sum, then an independent copy per row
   long q = 0;
   for (int p = 0; p < n; ++p) {
     const int o = orig(s->prow[p]);
     s->pirp[p] = (int)q;
-    for (int k = irp[o]; k < irp[o + 1]; ++k) {
-      s->pja[q] = upper ? n - 1 - ja[k] : ja[k];
-      s->pval[q] = val[k];
-      ++q;
-    }
+    q += irp[o + 1] - irp[o];
   }
   s->pirp[n] = (int)q;
+#pragma omp parallel for schedule(static, 4096)
+  for (int p = 0; p < n; ++p) {
+    const int o = orig(s->prow[p]);
+    long t = s->pirp[p];
+    for (int k = irp[o]; k < irp[o + 1]; ++k, ++t) {
+      s->pja[t] = upper ? n - 1 - ja[k] : ja[k];
+      s->pval[t] = val[k];
+    }
+  }
 }
 
 }  // namespace mldg
