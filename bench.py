@@ -317,10 +317,19 @@ def time_systems(mld, args, dev, torch, nsys=64, lo=24, hi=96):
     together (mldg_krylov_batch) against solving them one after the other."""
     dims = np.random.default_rng(1).integers(lo, hi + 1, nsys)
     precs, bs, mats, rows = [], [], [], 0
+    # throughput setting: the small levels keep their triangular solves, which
+    # overlap across the concurrent systems, instead of the explicit inverses
+    # (bandwidth-bound products that a single system runs faster alone)
+    prev = os.environ.get("MLDG_NO_DENSE_INV")
+    os.environ["MLDG_NO_DENSE_INV"] = "1"
     for idim in dims:
         a = mld.gen_pde3d(int(idim), 1, ISO)
         mats.append(a)
         precs.append(make_prec(mld, a, "BJAC", "FP32", device=dev))
+    if prev is None:
+        del os.environ["MLDG_NO_DENSE_INV"]
+    else:
+        os.environ["MLDG_NO_DENSE_INV"] = prev
         bs.append(torch.tensor(a.matvec(np.ones(a.nrows)), dtype=torch.float64, device=f"cuda:{dev}"))
         rows += a.nrows
     xs = [torch.zeros_like(b) for b in bs]

@@ -489,6 +489,8 @@ struct EngineT : Engine {
     // buffer the next single solve writes (one-column and K-column forms)
     DCSR<T> GL, GU;
     int gflip = 0, gflip_m = 0;
+    // FBGS: explicit (D+L)^{-1} and (D+U)^{-1} of a small level, when faster
+    T *gsF = nullptr, *gsB = nullptr;
     DWin<T> wL, wU, wUt, wLt;
     // coarsest level: explicit inverse of its ILU(0) factorisation (and its transpose)
     T *minv = nullptr, *minvT = nullptr;
@@ -721,6 +723,13 @@ struct EngineT : Engine {
   // holding values and the other one reset); end_fbgs() restores the start
   // state at the end of a recorded cycle.
   void fbgs_solve(Lev &L, bool backward, const T *rhs, T *out, T beta) {
+    if (L.gsF) {
+      const T *M = backward ? L.gsB : L.gsF;
+      begin(MLDG_KERNEL_VEC);
+      k_gemv<T><<<blocks_for((int64_t)L.n * 32), 256, 0, st>>>(L.n, M, rhs, T(1), beta, out);
+      end((int64_t)L.n * L.n * sizeof(T) + (int64_t)L.n * sizeof(T) * (2 + (beta != T(0))));
+      return;
+    }
     const DTri<T> &t = backward ? L.U : L.L;
     T *cur = L.gflip ? L.bufB : L.bufA, *other = L.gflip ? L.bufA : L.bufB;
     L.gflip ^= 1;
@@ -1197,7 +1206,8 @@ struct EngineT : Engine {
   // dense matrix-vector product beats the two dependency-bound solves.
   bool dense_inverse(Lev &L, Arena &ar) {
     const int n = L.n, Kw = 32, ki = 5;
-    if (n < 1 || L.minv || L.kind != MLDG_SMOOTHER_BJAC) return false;
+    const bool gs = L.kind == MLDG_SMOOTHER_FBGS;
+    if (n < 1 || L.minv || L.gsF || (L.kind != MLDG_SMOOTHER_BJAC && !gs)) return false;
     Arena tmp;
     bool ok = true;
     for (DTri<T> *f : {&L.L, &L.U}) {
@@ -1216,29 +1226,56 @@ struct EngineT : Engine {
       K = Kw;
       for (int c0 = 0; c0 < n; c0 += Kw) {
         k_ident_block<T><<<blocks_for((int64_t)nk), 256, 0, st>>>(n, c0, Kw, xm);
-        trsv_m(L.L, xm, nullptr, ba, bb, nullptr, T(1), T(0));
-        trsv_m(L.U, ba, L.d, bb, ba, ym, T(1), T(0));
-        k_scatter_cols<T><<<blocks_for((int64_t)nk), 256, 0, st>>>(n, c0, Kw, ym, M);
+        if (gs) {
+          // columns of (D+L)^{-1} into M and of (D+U)^{-1} into MT (each exchange pair returns
+          // to its start state: the second solve resets the first one's buffer)
+          trsv_m(L.L, xm, L.d, ba, bb, ym, T(1), T(0));
+          k_scatter_cols<T><<<blocks_for((int64_t)nk), 256, 0, st>>>(n, c0, Kw, ym, M);
+          trsv_m(L.U, xm, L.d, bb, ba, ym, T(1), T(0));
+          k_scatter_cols<T><<<blocks_for((int64_t)nk), 256, 0, st>>>(n, c0, Kw, ym, MT);
+        } else {
+          trsv_m(L.L, xm, nullptr, ba, bb, nullptr, T(1), T(0));
+          trsv_m(L.U, ba, L.d, bb, ba, ym, T(1), T(0));
+          k_scatter_cols<T><<<blocks_for((int64_t)nk), 256, 0, st>>>(n, c0, Kw, ym, M);
+        }
       }
       K = sK;
-      dim3 tg((n + 31) / 32, (n + 31) / 32), tb(32, 8);
-      k_transpose_sq<T><<<tg, tb, 0, st>>>(n, M, MT);
+      if (!gs) {
+        dim3 tg((n + 31) / 32, (n + 31) / 32), tb(32, 8);
+        k_transpose_sq<T><<<tg, tb, 0, st>>>(n, M, MT);
+      }
       MLDG_CUDA(cudaStreamSynchronize(st));
     }
     for (DTri<T> *f : {&L.L, &L.U}) f->ell[ki] = typename DTri<T>::Ell();
     tmp.release();
     if (!ok) return false;
     // keep the dense form only if it is faster
+    auto op = [&]() {
+      if (gs) {
+        fbgs_solve(L, false, L.x, L.ty, T(0));
+        fbgs_solve(L, true, L.x, L.ty, T(0));
+      } else {
+        ilu_apply(L, 'N', L.x, T(0), L.ty);
+      }
+    };
+    auto set = [&](bool on) {
+      if (gs) {
+        L.gsF = on ? M : nullptr;
+        L.gsB = on ? MT : nullptr;
+      } else {
+        L.minv = on ? M : nullptr;
+        L.minvT = on ? MT : nullptr;
+      }
+    };
     cudaEvent_t e0, e1;
     MLDG_CUDA(cudaEventCreate(&e0));
     MLDG_CUDA(cudaEventCreate(&e1));
     float t[2] = {0, 0};
     for (int v = 0; v < 2; ++v) {
-      L.minv = v ? M : nullptr;
-      L.minvT = v ? MT : nullptr;
-      ilu_apply(L, 'N', L.x, T(0), L.ty);
+      set(v == 1);
+      op();
       MLDG_CUDA(cudaEventRecord(e0, st));
-      for (int r = 0; r < 3; ++r) ilu_apply(L, 'N', L.x, T(0), L.ty);
+      for (int r = 0; r < 3; ++r) op();
       MLDG_CUDA(cudaEventRecord(e1, st));
       MLDG_CUDA(cudaEventSynchronize(e1));
       MLDG_CUDA(cudaEventElapsedTime(&t[v], e0, e1));
@@ -1246,12 +1283,10 @@ struct EngineT : Engine {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     const bool keep = t[1] < t[0] || std::getenv("MLDG_DENSE_INV");
-    if (!keep) {
-      L.minv = L.minvT = nullptr;  // (the matrices stay in the arena until the handle is freed)
-    }
+    set(keep);  // (rejected matrices stay in the arena until the handle is freed)
     if (std::getenv("MLDG_VERBOSE"))
-      std::fprintf(stderr, "mldg: dense ILU inverse n=%d: solves %.3f ms dense %.3f ms -> %s\n", n, t[0] / 3,
-                   t[1] / 3, keep ? "dense" : "solves");
+      std::fprintf(stderr, "mldg: dense %s inverse n=%d: solves %.3f ms dense %.3f ms -> %s\n", gs ? "GS" : "ILU", n,
+                   t[0] / 3, t[1] / 3, keep ? "dense" : "solves");
     launches = 0;
     bytes = 0;
     return keep;
@@ -1443,6 +1478,16 @@ struct EngineT : Engine {
   }
   // K-wide fbgs_solve / end_fbgs / fbgs_smoother
   void fbgs_solve_m(Lev &L, bool backward, const T *rhs, T *out, T beta) {
+    if (L.gsF) {
+      const T *M = backward ? L.gsB : L.gsF;
+      begin(MLDG_KERNEL_VEC);
+      kdispatch(K, [&](auto kc) {
+        constexpr int KK = decltype(kc)::value;
+        k_gemm_m<T, KK><<<blocks_for(nk(L.n)), 256, 0, st>>>(L.n, M, rhs, T(1), beta, out);
+      });
+      end((int64_t)L.n * L.n * sizeof(T) + nk(L.n) * (int64_t)sizeof(T) * (2 + (beta != T(0))));
+      return;
+    }
     DTri<T> &t = backward ? L.U : L.L;
     T *cur = L.gflip_m ? L.bufBm : L.bufAm, *other = L.gflip_m ? L.bufAm : L.bufBm;
     L.gflip_m ^= 1;
@@ -2470,7 +2515,8 @@ static Engine *make_engine(Handle *h) {
   if (!std::getenv("MLDG_NO_DENSE_INV"))
     for (int l = 1; l < h->nlev; ++l) {
       auto &L = e->lv[l];
-      if (L.kind == MLDG_SMOOTHER_BJAC && !L.minv && L.n <= kDenseInvRows) e->dense_inverse(L, ar);
+      if ((L.kind == MLDG_SMOOTHER_BJAC || L.kind == MLDG_SMOOTHER_FBGS) && !L.minv && L.n <= kDenseInvRows)
+        e->dense_inverse(L, ar);
     }
   tick("dense level inverses");
   if (std::getenv("MLDG_TIMING"))

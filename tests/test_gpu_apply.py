@@ -120,21 +120,43 @@ def test_apply_large_coarse_level(mld, orc):
         assert _rel(h.apply(x, trans=trans), op.apply(x, trans)) <= TOL_FP64
 
 
-@pytest.mark.parametrize("idim,coef", [(20, ISO), (28, ANISO)])
-def test_dense_inverse_levels_match_oracle(mld, orc, monkeypatch, idim, coef):
-    """Every BJAC level below the finest applied through the explicit inverse
-    of its ILU(0), computed on the GPU column block by column block."""
+@pytest.mark.parametrize("idim,coef,smoother", [(20, ISO, "BJAC"), (28, ANISO, "BJAC"), (20, ANISO, "FBGS")])
+def test_dense_inverse_levels_match_oracle(mld, orc, monkeypatch, idim, coef, smoother):
+    """Every level below the finest applied through explicit inverses (of its
+    ILU(0), or of D+L and D+U for FBGS), computed on the GPU column block by
+    column block."""
     monkeypatch.setenv("MLDG_DENSE_INV", "1")
     a = orc.gen_pde3d(idim, 1, coef)
-    op = orc.Prec(oracle_params(orc, "BJAC", mcs=60))
+    op = orc.Prec(oracle_params(orc, smoother, mcs=60))
     op.build(a)
     assert op.nlev >= 3
     for precision, tol in ((0, TOL_FP64), (1, TOL_FP32)):
         h = upload_oracle_hierarchy(mld, orc, op, precision=precision)
         rng = np.random.default_rng(idim)
-        for trans in ("N", "T"):
+        for trans in (("N", "T") if smoother == "BJAC" else ("N",)):
             x = rng.uniform(-1, 1, a.nrows)
             assert _rel(h.apply(x, trans=trans), op.apply(x, trans)) <= tol
         X = rng.uniform(-1, 1, (3, a.nrows))
         Y = h.apply_block(X)
         assert max(_rel(Y[c], op.apply(X[c])) for c in range(3)) <= tol
+
+
+@pytest.mark.parametrize("idim,smoother,max_levs", [(1, "BJAC", 20), (2, "BJAC", 20), (2, "JACOBI", 1),
+                                                    (3, "FBGS", 20), (5, "BJAC", 1)])
+def test_degenerate_sizes(mld, orc, idim, smoother, max_levs):
+    """One-row and few-row systems, one-level and multilevel: same results as
+    the oracle; a zero right-hand side gives zero; nrhs = 0 is a no-op."""
+    a = orc.gen_pde3d(idim, 1, ISO)
+    par = oracle_params(orc, smoother, mcs=1)
+    par.max_levs = max_levs
+    op = orc.Prec(par)
+    op.build(a)
+    h = upload_oracle_hierarchy(mld, orc, op)
+    x = np.random.default_rng(idim).uniform(-1, 1, a.nrows)
+    assert _rel(h.apply(x), op.apply(x)) <= TOL_FP64
+    assert np.all(h.apply(np.zeros(a.nrows)) == 0.0)
+    Y = np.full((0, a.nrows), 5.0)
+    h.apply_block(np.zeros((0, a.nrows)), Y)
+    X2 = np.stack([x, -x])
+    Y2 = h.apply_block(X2)
+    assert _rel(Y2[1], -op.apply(x)) <= TOL_FP64
