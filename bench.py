@@ -326,12 +326,12 @@ def time_systems(mld, args, dev, torch, nsys=64, lo=24, hi=96):
         a = mld.gen_pde3d(int(idim), 1, ISO)
         mats.append(a)
         precs.append(make_prec(mld, a, "BJAC", "FP32", device=dev))
+        bs.append(torch.tensor(a.matvec(np.ones(a.nrows)), dtype=torch.float64, device=f"cuda:{dev}"))
+        rows += a.nrows
     if prev is None:
         del os.environ["MLDG_NO_DENSE_INV"]
     else:
         os.environ["MLDG_NO_DENSE_INV"] = prev
-        bs.append(torch.tensor(a.matvec(np.ones(a.nrows)), dtype=torch.float64, device=f"cuda:{dev}"))
-        rows += a.nrows
     xs = [torch.zeros_like(b) for b in bs]
     mld.krylov_batch("FCG", precs, bs, xs, eps=args.eps, itmax=500)  # warm: captures the graphs
     reps = max(1, min(args.steps, 3))
@@ -424,7 +424,7 @@ def run_ours(args, rank, world, local_rank):
                             dist=dist)
         others = {}
         if not args.no_variants:
-            for sm, pr in (("JACOBI", "FP64"), ("BJAC", "FP32")):
+            for sm, pr in (("JACOBI", "FP64"), ("BJAC", "FP32"), ("FBGS", "FP64")):
                 if (sm, pr) == (args.smoother, args.precision):
                     continue
                 r = time_variant(mld, a, b, sm, pr, args, dev, torch, dist=dist)

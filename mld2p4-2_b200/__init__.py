@@ -568,6 +568,8 @@ def krylov_batch(method: str, precs, bs, xs=None, eps: float = 1e-10, itmax: int
     (xs, iters[nsys], relres[nsys], device ms of the whole batch)."""
     m = {"CG": 0, "FCG": 1}[method.upper()]
     nsys = len(precs)
+    if len(bs) != nsys or (xs is not None and len(xs) != nsys):
+        raise ValueError("krylov_batch: precs, bs and xs must have one entry per system")
     if xs is None:
         xs = [np.zeros_like(b) if isinstance(b, np.ndarray) else b.new_zeros(b.shape) for b in bs]
     hs = (C.c_void_p * max(nsys, 1))()

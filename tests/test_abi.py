@@ -87,3 +87,11 @@ def test_kappa_generator_is_symmetric_and_matches_constant_case(mld):
     import scipy.sparse as sp
     m = sp.csr_matrix((a2.val, a2.ja, a2.irp))
     assert abs(m - m.T).max() <= 1e-9 * abs(m).max()
+
+
+def test_krylov_batch_rejects_mismatched_lists(mld):
+    # checked on the host before any handle is touched
+    with pytest.raises(ValueError):
+        mld.krylov_batch("FCG", [object(), object()], [np.ones(4)])
+    with pytest.raises(ValueError):
+        mld.krylov_batch("FCG", [object()], [np.ones(4)], [np.ones(4), np.ones(4)])
