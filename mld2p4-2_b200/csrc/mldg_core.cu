@@ -31,6 +31,7 @@
 #include "mldg_multi.cuh"
 #include "mldg_tri.h"
 #include "mldg_trsv_win.cuh"
+#include "mldg_trsv_rep.cuh"
 
 namespace mldg {
 
@@ -232,6 +233,34 @@ struct DWin {
   std::vector<WinDesc> h_desc;
   bool ok = false;
 };
+
+// Plan of the replicated-window cluster solve (k_trsv_rep) for one triangular
+// factor: per CTA and step one block (row descriptors, ring slots and values of
+// the entries, far entries), its descriptor, and the position maps.
+template <typename T>
+struct DRep {
+  bool ok = false, linked = false;
+  int n = 0, nsteps = 0, C = 8, R = 0, capB = 0, stage_bytes = 0, ring_bytes = 0;
+  size_t smem = 0;
+  int64_t nnz = 0, nfar = 0, block_bytes = 0;
+  int4 *desc = nullptr;
+  uint4 *blocks = nullptr;
+  T *xp = nullptr;    // position-ordered solution for far readers
+  int *orig = nullptr;
+  unsigned long long *trace = nullptr;  // MLDG_REP_TRACE: per-phase cycle counters
+  std::vector<int> h_orig, h_pos;  // position -> original row, original row -> position
+  std::vector<int> h_tail_ptr, h_tail;
+  // host schedule, released once the blocks are built
+  std::vector<int> step_ptr;       // nsteps + 1 first positions
+  std::vector<int> pirp, dep;      // entries in position order, dependency positions
+  std::vector<double> val;
+  std::vector<unsigned char> cls;  // per entry: 0 previous step, 3 two to kRepG steps back, 1 older (ring), 2 far
+  int *vbytes = nullptr;           // per step: bytes of its values (every row, one T each)
+  int *tail_ptr = nullptr, *tail = nullptr;  // far-copy positions reset after the last step, per CTA
+  std::vector<int> rst_step;       // per position read by a far entry: the step that resets its copy
+  std::vector<unsigned char> feeds;  // per position: read by a far entry
+};
+constexpr int kRepTPR = 4;
 
 static int pick_tpr(int64_t nnz, int nr) {
   const double avg = nr > 0 ? (double)nnz / nr : 0.0;
@@ -492,6 +521,10 @@ struct EngineT : Engine {
     // FBGS: explicit (D+L)^{-1} and (D+U)^{-1} of a small level, when faster
     T *gsF = nullptr, *gsB = nullptr;
     DWin<T> wL, wU, wUt, wLt;
+    // replicated-window cluster solves (k_trsv_rep): built (rep_ok) on large
+    // ILU(0) levels, used (rep) when the autotuner finds them fastest
+    bool rep = false, rep_ok = false;
+    DRep<T> rL, rU, rUt, rLt;
     // coarsest level: explicit inverse of its ILU(0) factorisation (and its transpose)
     T *minv = nullptr, *minvT = nullptr;
     T *rp0 = nullptr, *rp1 = nullptr;  // right-hand sides in position order
@@ -615,9 +648,12 @@ struct EngineT : Engine {
           ilu_apply(L, 'N', L.x, T(0), L.ty);
         }
       };
-      float best[2] = {1e30f, 1e30f};
-      for (int v = 0; v < 2; ++v) {
+      // variants: 0 the level's other solve, 1 ELL, 2 replicated-window cluster solve
+      float best[3] = {1e30f, 1e30f, 1e30f};
+      for (int v = 0; v < 3; ++v) {
+        if (v == 2 && (gs || !L.rep_ok)) continue;
         L.ell1 = v == 1;
+        L.rep = v == 2;
         op();  // warm
         MLDG_CUDA(cudaEventRecord(e0, st));
         for (int r = 0; r < reps; ++r) op();
@@ -625,10 +661,15 @@ struct EngineT : Engine {
         MLDG_CUDA(cudaEventSynchronize(e1));
         MLDG_CUDA(cudaEventElapsedTime(&best[v], e0, e1));
       }
-      L.ell1 = best[1] < best[0];
+      int pick = 0;
+      for (int v = 1; v < 3; ++v)
+        if (best[v] < best[pick]) pick = v;
+      L.ell1 = pick == 1;
+      L.rep = pick == 2;
       if (std::getenv("MLDG_VERBOSE"))
-        std::fprintf(stderr, "mldg: ilu autotune n=%d other %.3f ms ell %.3f ms -> %s\n", L.n, best[0] / reps,
-                     best[1] / reps, L.ell1 ? "ell" : "other");
+        std::fprintf(stderr, "mldg: ilu autotune n=%d other %.3f ms ell %.3f ms rep %.3f ms -> %s\n", L.n,
+                     best[0] / reps, best[1] / reps, best[2] / reps,
+                     L.rep ? "rep" : (L.ell1 ? "ell" : "other"));
     }
     launches = 0;
     bytes = 0;
@@ -636,10 +677,44 @@ struct EngineT : Engine {
     cudaEventDestroy(e1);
   }
 
-  void gather(const DWin<T> &w, const T *src, T *dst) {
+  void gather(const DWin<T> &w, const T *src, T *dst) { gather(w.n, w.orig, src, dst); }
+  void gather(int n, const int *orig, const T *src, T *dst) {
     begin(MLDG_KERNEL_VEC);
-    k_gather<T><<<blocks_for(w.n), 256, 0, st>>>(w.n, w.orig, src, (const T *)nullptr, dst);
-    end((int64_t)w.n * (4 + 2 * sizeof(T)));
+    k_gather<T><<<blocks_for(n), 256, 0, st>>>(n, orig, src, (const T *)nullptr, dst);
+    end((int64_t)n * (4 + 2 * sizeof(T)));
+  }
+  // one replicated-window solve; rhs in the plan's position order
+  void rsolve(const DRep<T> &w, const T *rhs, T *next, T *out, T beta, T *tpos = nullptr) {
+    RepArgs<T> a;
+    a.nsteps = w.nsteps;
+    a.rmask = w.R - 1;
+    a.capB = w.capB;
+    a.stage_bytes = w.stage_bytes;
+    a.ring_bytes = w.ring_bytes;
+    a.linked = w.linked ? 1 : 0;
+    a.desc = w.desc;
+    a.blocks = w.blocks;
+    a.rhs = rhs;
+    a.next = w.linked ? next : nullptr;
+    a.out = (beta == T(0)) ? out : nullptr;
+    a.tpos = (out && beta != T(0)) ? tpos : nullptr;
+    a.xp = w.xp;
+    a.tail_ptr = w.tail_ptr;
+    a.tail = w.tail;
+    a.alpha = T(1);
+    a.off_bar = w.ring_bytes + kRepD * w.stage_bytes;
+    a.vbytes = w.vbytes;
+    a.err = err;
+    a.trace = w.trace;
+    begin(MLDG_KERNEL_TRSV);
+    launch_rep(w, a, st);
+    end(w.nnz * (int64_t)(sizeof(T) + 4) + 4 * (2 * (int64_t)w.n + 1) +
+        (int64_t)w.n * sizeof(T) * (1 + (next ? 2 : 0) + (out ? 1 : 0)) + (next ? 4 * (int64_t)w.n : 0));
+    if (out && beta != T(0)) {
+      begin(MLDG_KERNEL_VEC);
+      k_combine<T><<<blocks_for(w.n), 256, 0, st>>>(w.n, w.orig, tpos, T(1), beta, out);
+      end((int64_t)w.n * (4 + 3 * sizeof(T)));
+    }
   }
   void wsolve(const DWin<T> &w, const T *rhs, T *next, T *out, T beta, T *tpos = nullptr) {
     WinArgs<T> a;
@@ -698,6 +773,14 @@ struct EngineT : Engine {
         trsv_ell1(L.Ut, x, nullptr, L.bufA, L.bufB, nullptr, T(1), T(0));
         trsv_ell1(L.Lt, L.bufA, L.d, L.bufB, L.bufA, y, T(1), beta);
       }
+      return;
+    }
+    if (L.rep) {
+      const DRep<T> &f = (trans == 'N') ? L.rL : L.rUt;
+      const DRep<T> &g = (trans == 'N') ? L.rU : L.rLt;
+      gather(f.n, f.orig, x, L.rp0);
+      rsolve(f, L.rp0, L.rp1, nullptr, T(0));
+      rsolve(g, L.rp1, nullptr, y, beta, L.rp0);  // rp0 is free again: results in position order
       return;
     }
     if (L.win) {
@@ -1704,6 +1787,25 @@ struct EngineT : Engine {
   void dump_trace() override {
     dump_ell_trace();
     for (size_t l = 0; l < lv.size(); ++l) {
+      const DRep<T> *rs[4] = {&lv[l].rL, &lv[l].rU, &lv[l].rUt, &lv[l].rLt};
+      for (int q = 0; q < 4; ++q) {
+        if (!rs[q]->trace) continue;
+        unsigned long long t[20] = {0};
+        cudaMemcpy(t, rs[q]->trace, 20 * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+        for (int th = 0; th < 2; ++th) {
+          const unsigned long long *u = t + 10 * th;
+          if (!u[7]) continue;
+          const double k = (double)u[7];
+          std::fprintf(stderr,
+                       "mldg trace: level %zu rep%d C=%d group %d steps %llu: cycles/step wait(s-2) %.0f mid %.0f "
+                       "wait(s-1) %.0f critical %.0f outputs %.0f sync %.0f prepare %.0f | kernel cycles/step %.0f "
+                       "ns/step %.0f\n",
+                       l, q, rs[q]->C, th, u[7], u[0] / k, u[1] / k, u[2] / k, u[3] / k, u[4] / k, u[5] / k,
+                       u[6] / k, u[8] / k, u[9] / k);
+        }
+      }
+    }
+    for (size_t l = 0; l < lv.size(); ++l) {
       if (!lv[l].win) continue;
       const DWin<T> *ws[4] = {&lv[l].wL, &lv[l].wU, &lv[l].wUt, &lv[l].wLt};
       for (int q = 0; q < 4; ++q) {
@@ -2143,6 +2245,480 @@ static void launch_win(const DWin<T> &w, const WinArgs<T> &a, cudaStream_t st) {
   }
 }
 
+// ---- replicated-window cluster solve (k_trsv_rep): plans and launch ----
+
+// Step schedule and entry classes of one factor for a cluster of C CTAs;
+// ok == false when a row exceeds the per-lane register capacities or a
+// dependency beyond the ring is fewer than kRepFarMin steps back.
+template <typename T>
+static DRep<T> build_rep_sched(const HostCSR &m, bool upper, int C) {
+  DRep<T> w;
+  const int n = m.nr;
+  if (n <= 0) return w;
+  TriSchedule s;
+  build_tri_schedule(n, m.irp.data(), m.ja.data(), m.val.data(), upper, n, &s);
+  const int nlev = (int)s.lvl_ptr.size() - 1;
+  std::vector<int> posof((size_t)n);
+  for (int p = 0; p < n; ++p) posof[s.prow[p]] = p;
+  w.n = n;
+  w.C = C;
+  w.nnz = m.nnz();
+  w.R = (int)(128 * 1024 / sizeof(T));
+  // MLDG_REP_R: a smaller ring (power of two), so that small tests reach the far path
+  if (const char *ev = std::getenv("MLDG_REP_R")) {
+    const int r = std::atoi(ev);
+    if (r >= 1024 && r <= w.R && (r & (r - 1)) == 0) w.R = r;
+  }
+  w.h_orig.resize((size_t)n);
+  w.h_pos.resize((size_t)n);
+  for (int p = 0; p < n; ++p) {
+    w.h_orig[p] = upper ? n - 1 - s.prow[p] : s.prow[p];
+    w.h_pos[w.h_orig[p]] = p;
+  }
+  // steps: levels, split where wider than the cluster's row slots
+  const int maxstep = C * rep_rows<kRepTPR>();
+  if (w.R < 2 * maxstep) return w;
+  w.step_ptr.push_back(0);
+  for (int L = 0; L < nlev; ++L) {
+    const int p0 = s.lvl_ptr[L], p1 = s.lvl_ptr[L + 1], nr = p1 - p0;
+    const int k = (nr + maxstep - 1) / maxstep;
+    for (int j = 1; j <= k; ++j) w.step_ptr.push_back(p0 + (int)((int64_t)nr * j / k));
+  }
+  w.nsteps = (int)w.step_ptr.size() - 1;
+  std::vector<int> step_of((size_t)n);
+  for (int st = 0; st < w.nsteps; ++st)
+    for (int p = w.step_ptr[st]; p < w.step_ptr[st + 1]; ++p) step_of[p] = st;
+  w.pirp = std::move(s.pirp);
+  w.val = std::move(s.pval);
+  w.dep.resize(s.pja.size());
+  w.cls.resize(s.pja.size());
+  w.feeds.assign((size_t)n, 0);
+  bool ok = true;
+#pragma omp parallel for schedule(static) reduction(&& : ok)
+  for (int p = 0; p < n; ++p) {
+    const int sp = step_of[p], end = w.step_ptr[sp + 1];
+    int n1 = 0, nm = 0, no = 0, nf = 0;
+    for (int k = w.pirp[p]; k < w.pirp[p + 1]; ++k) {
+      const int q = posof[s.pja[k]], sq = step_of[q], dist = sp - sq;
+      w.dep[k] = q;
+      if (dist < 1) ok = false;
+      if (end - q <= w.R) {
+        w.cls[k] = dist == 1 ? 0 : (dist <= kRepG ? 3 : 1);
+        (dist == 1 ? n1 : (dist <= kRepG ? nm : no))++;
+      } else {
+        w.cls[k] = 2;
+        ++nf;
+        if (dist < kRepFarMin) ok = false;
+      }
+    }
+    if (n1 > kRepN1 * kRepTPR || nf > kRepNF * kRepTPR || nm > 255 || no > 255) ok = false;
+  }
+  if (!ok) return w;
+  int64_t nfar = 0;
+  // a far copy is reset one step after its last reader's step
+  w.rst_step.assign((size_t)n, -1);
+  for (int p = 0; p < n; ++p)
+    for (int k = w.pirp[p]; k < w.pirp[p + 1]; ++k)
+      if (w.cls[k] == 2) {
+        w.feeds[w.dep[k]] = 1;
+        w.rst_step[w.dep[k]] = std::max(w.rst_step[w.dep[k]], step_of[p] + 1);
+        ++nfar;
+      }
+  w.nfar = nfar;
+  w.ok = true;
+  return w;
+}
+
+// Per-CTA blocks of a scheduled factor (host memory); with `next`, each row
+// also writes the following solve's right-hand side: next[pos'(orig)] = d[orig] * t.
+// Sets w.ok = false when the stages and the ring do not fit in shared memory.
+template <typename T>
+static void build_rep_blocks_host(DRep<T> &w, const DRep<T> *next, const std::vector<double> *d,
+                                  std::vector<uint4> &blocks, std::vector<int4> &desc) {
+  const int C = w.C, ns = w.nsteps;
+  w.linked = next != nullptr;
+  desc.assign((size_t)C * ns, make_int4(0, 0, 0, 0));
+  auto slice = [&](int c, int st, int &a, int &b) {
+    const int P0 = w.step_ptr[st], P1 = w.step_ptr[st + 1];
+    a = P0 + (int)((int64_t)(P1 - P0) * c / C);
+    b = P0 + (int)((int64_t)(P1 - P0) * (c + 1) / C);
+  };
+  // far-copy resets of each (CTA, step): position q goes to CTA q % C at its reset step
+  std::vector<std::vector<int>> rst((size_t)C * ns);
+  std::vector<std::vector<int>> tailv((size_t)C);
+  for (int q = 0; q < w.n; ++q)
+    if (w.feeds[q]) {
+      const int r = w.rst_step[q];
+      if (r < ns)
+        rst[(size_t)(q % C) * ns + r].push_back(q);
+      else
+        tailv[(size_t)(q % C)].push_back(q);
+    }
+  w.h_tail_ptr.assign((size_t)C + 1, 0);
+  w.h_tail.clear();
+  for (int c = 0; c < C; ++c) {
+    w.h_tail.insert(w.h_tail.end(), tailv[c].begin(), tailv[c].end());
+    w.h_tail_ptr[c + 1] = (int)w.h_tail.size();
+  }
+  // ring and far entries of each (CTA, step) slice
+  std::vector<int> ne_of((size_t)C * ns), nf_of((size_t)C * ns);
+  for (int c = 0; c < C; ++c)
+    for (int st = 0; st < ns; ++st) {
+      int a, b, ne = 0, nf = 0;
+      slice(c, st, a, b);
+      for (int p = a; p < b; ++p)
+        for (int k = w.pirp[p]; k < w.pirp[p + 1]; ++k) (w.cls[k] == 2 ? nf : ne)++;
+      ne_of[(size_t)c * ns + st] = ne;
+      nf_of[(size_t)c * ns + st] = nf;
+    }
+  // block sizes (the block of step t lists the far entries of step t + 2), offsets per CTA in step order
+  std::vector<int64_t> boff((size_t)C * ns + 1, 0);
+  int capB = 16, maxnr = 0;
+  for (int c = 0; c < C; ++c)
+    for (int st = 0; st < ns; ++st) {
+      const size_t i = (size_t)c * ns + st;
+      int a, b, a2 = 0, b2 = 0;
+      slice(c, st, a, b);
+      if (st + kRepG < ns) slice(c, st + kRepG, a2, b2);
+      const int nf2 = st + kRepG < ns ? nf_of[i + kRepG] : 0;
+      const RepLayout L = rep_layout<T>(b - a, ne_of[i], b2 - a2, nf2, (int)rst[i].size(), w.linked);
+      desc[i] = make_int4((int)(boff[i] / 16), L.bytes / 16, a, b - a);
+      boff[i + 1] = boff[i] + L.bytes;
+      capB = std::max(capB, L.bytes);
+      maxnr = std::max(maxnr, b - a);
+    }
+  w.block_bytes = boff[(size_t)C * ns];
+  blocks.assign((size_t)(w.block_bytes / 16), make_uint4(0, 0, 0, 0));
+  unsigned char *base = reinterpret_cast<unsigned char *>(blocks.data());
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t i = 0; i < (int64_t)C * ns; ++i) {
+    const int st = (int)(i % ns), c = (int)(i / ns);
+    const int4 dd = desc[(size_t)i];
+    const int a = dd.z, nr = dd.w;
+    int a2 = 0, b2 = 0;
+    if (st + kRepG < ns) slice(c, st + kRepG, a2, b2);
+    const int nr2 = b2 - a2, nf2 = st + kRepG < ns ? nf_of[(size_t)i + kRepG] : 0;
+    unsigned char *blk = base + boff[(size_t)i];
+    const int nrst = (int)rst[(size_t)i].size();
+    const RepLayout L = rep_layout<T>(nr, ne_of[(size_t)i], nr2, nf2, nrst, w.linked);
+    int4 *hdr = reinterpret_cast<int4 *>(blk);
+    hdr[0] = make_int4(nr, ne_of[(size_t)i], nf2, a);
+    // the blocks this CTA copies and prefetches while this one is staged
+    hdr[1] = st + kRepD - 1 < ns ? desc[(size_t)i + kRepD - 1] : make_int4(0, 0, 0, 0);
+    hdr[2] = st + kRepPF < ns ? desc[(size_t)i + kRepPF] : make_int4(0, 0, 0, 0);
+    hdr[3] = make_int4(nr2, nrst, 0, 0);
+    std::copy(rst[(size_t)i].begin(), rst[(size_t)i].end(), reinterpret_cast<int *>(blk + L.o_rst));
+    int4 *row = reinterpret_cast<int4 *>(blk + L.o_row);
+    int *npos = reinterpret_cast<int *>(blk + L.o_npos);
+    T *nsc = reinterpret_cast<T *>(blk + L.o_nsc);
+    unsigned short *slot = reinterpret_cast<unsigned short *>(blk + L.o_slot);
+    T *val = reinterpret_cast<T *>(blk + L.o_val);
+    int2 *fr = reinterpret_cast<int2 *>(blk + L.o_fr);
+    int *fq = reinterpret_cast<int *>(blk + L.o_fq);
+    T *fv = reinterpret_cast<T *>(blk + L.o_fv);
+    int e = 0;
+    for (int r = 0; r < nr; ++r) {
+      const int p = a + r, o = w.h_orig[p];
+      const int e0 = e;
+      int cnt[4] = {0, 0, 0, 0};
+      for (int pass : {0, 3, 1})  // previous step, two to kRepG steps back, older
+        for (int k = w.pirp[p]; k < w.pirp[p + 1]; ++k)
+          if (w.cls[k] == pass) {
+            slot[e] = (unsigned short)(w.dep[k] & (w.R - 1));
+            val[e] = (T)w.val[k];
+            ++e;
+            ++cnt[pass];
+          }
+      row[r] = make_int4(e0, cnt[0] | (cnt[3] << 8) | (cnt[1] << 16) | ((int)w.feeds[p] << 24), 0, o);
+      if (w.linked) {
+        npos[r] = next->h_pos[o];
+        nsc[r] = (T)(*d)[o];
+      }
+    }
+    int f = 0;
+    for (int r = 0; r < nr2; ++r) {
+      const int p = a2 + r, f0 = f;
+      for (int k = w.pirp[p]; k < w.pirp[p + 1]; ++k)
+        if (w.cls[k] == 2) {
+          fq[f] = w.dep[k];
+          fv[f] = (T)w.val[k];
+          ++f;
+        }
+      fr[r] = make_int2(f0, f - f0);
+    }
+  }
+  constexpr int PER = 16 / (int)sizeof(T);
+  w.capB = capB;
+  w.stage_bytes = capB + rep_al16((maxnr + 2 * PER) * (int)sizeof(T));
+  w.ring_bytes = w.R * (int)sizeof(T);
+  w.smem = (size_t)w.ring_bytes + (size_t)kRepD * w.stage_bytes + 256;  // + the mbarriers
+  if (w.smem > (size_t)kWinSmemMax) w.ok = false;
+}
+
+template <typename T>
+static void build_rep_blocks(Arena &ar, DRep<T> &w, const DRep<T> *next, const std::vector<double> *d) {
+  std::vector<uint4> blocks;
+  std::vector<int4> desc;
+  build_rep_blocks_host(w, next, d, blocks, desc);
+  if (!w.ok) return;
+  w.desc = ar.upload(desc);
+  w.blocks = ar.upload(blocks);
+  std::vector<int> vb((size_t)w.nsteps);
+  for (int st = 0; st < w.nsteps; ++st) vb[st] = (int)sizeof(T) * (w.step_ptr[st + 1] - w.step_ptr[st]);
+  w.vbytes = ar.upload(vb);
+  std::vector<int> orig(w.h_orig);
+  orig.resize((size_t)w.n + 4, 0);
+  w.orig = ar.upload(orig);
+  if (w.nfar) {
+    // the far copy holds the sentinel until a value is written
+    std::vector<T> xs((size_t)w.n + 8, Sentinel<T>::value());
+    w.xp = ar.upload(xs);
+    w.tail_ptr = ar.upload(w.h_tail_ptr);
+    std::vector<int> tl(w.h_tail);
+    tl.push_back(0);
+    w.tail = ar.upload(tl);
+  }
+  if (std::getenv("MLDG_REP_TRACE")) {
+    w.trace = ar.alloc<unsigned long long>(20);
+    MLDG_CUDA(cudaMemset(w.trace, 0, 20 * sizeof(unsigned long long)));
+  }
+}
+
+// drops the host schedule of a plan (after its blocks and those of the plan
+// linked to it are built)
+template <typename T>
+static void rep_release_sched(DRep<T> &w) {
+  std::vector<int>().swap(w.step_ptr);
+  std::vector<int>().swap(w.pirp);
+  std::vector<int>().swap(w.dep);
+  std::vector<double>().swap(w.val);
+  std::vector<unsigned char>().swap(w.cls);
+  std::vector<unsigned char>().swap(w.feeds);
+  std::vector<int>().swap(w.rst_step);
+}
+
+template <typename T, int C>
+static cudaLaunchConfig_t rep_config(const DRep<T> &w, cudaStream_t st, cudaLaunchAttribute *at) {
+  static bool attr = false;
+  if (!attr) {
+    MLDG_CUDA(cudaFuncSetAttribute(k_trsv_rep<T, kRepTPR, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   kWinSmemMax));
+    if (C > 8)
+      MLDG_CUDA(cudaFuncSetAttribute(k_trsv_rep<T, kRepTPR, C>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    attr = true;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(C);
+  cfg.blockDim = dim3(kRepThreads);
+  cfg.dynamicSmemBytes = w.smem;
+  cfg.stream = st;
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = C;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+
+// can a cluster of this plan's shape be resident at all
+template <typename T>
+static bool rep_fits(const DRep<T> &w) {
+  cudaLaunchAttribute at[1];
+  int ncl = 0;
+  cudaError_t e;
+  if (w.C == 8) {
+    cudaLaunchConfig_t cfg = rep_config<T, 8>(w, 0, at);
+    e = cudaOccupancyMaxActiveClusters(&ncl, k_trsv_rep<T, kRepTPR, 8>, &cfg);
+  } else {
+    cudaLaunchConfig_t cfg = rep_config<T, 16>(w, 0, at);
+    e = cudaOccupancyMaxActiveClusters(&ncl, k_trsv_rep<T, kRepTPR, 16>, &cfg);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return ncl > 0;
+}
+
+template <typename T>
+static void launch_rep(const DRep<T> &w, const RepArgs<T> &a, cudaStream_t st) {
+  cudaLaunchAttribute at[1];
+  if (w.C == 8) {
+    cudaLaunchConfig_t cfg = rep_config<T, 8>(w, st, at);
+    MLDG_CUDA(cudaLaunchKernelEx(&cfg, k_trsv_rep<T, kRepTPR, 8>, a));
+  } else {
+    cudaLaunchConfig_t cfg = rep_config<T, 16>(w, st, at);
+    MLDG_CUDA(cudaLaunchKernelEx(&cfg, k_trsv_rep<T, kRepTPR, 16>, a));
+  }
+}
+
+// Host emulation of k_trsv_rep over a plan, in the kernel's order (the rows
+// of a step from the ring state after the previous step, values published at
+// the end of the step).  Every ring read is checked against the position the
+// schedule says it holds, every ring read against the window bound of its
+// step, every far read against its kRepFarMin-step distance, and every block
+// against its descriptor and the stage capacity; returns the violations.
+// rhs_pos: right-hand side in the plan's position order; out[orig] = t;
+// next_pos[npos] = nsc * t for a linked plan.
+template <typename T>
+static int64_t rep_emulate(const DRep<T> &w, const std::vector<uint4> &blocks, const std::vector<int4> &desc,
+                           const std::vector<T> &rhs_pos, std::vector<T> &out, std::vector<T> *next_pos) {
+  const int R = w.R, C = w.C, ns = w.nsteps, n = w.n;
+  constexpr int PER = 16 / (int)sizeof(T);
+  std::vector<T> ring((size_t)R, T(0)), xp((size_t)n, T(0));
+  std::vector<int> tag((size_t)R, -1), tstep((size_t)R, -1), xstep((size_t)n, 1 << 30);
+  std::vector<unsigned char> xvalid((size_t)n, 0);  // far copy written and not yet reset
+  std::vector<std::pair<int, T>> pub;
+  const unsigned char *base = reinterpret_cast<const unsigned char *>(blocks.data());
+  int64_t bad = 0;
+  for (int s = 0; s < ns; ++s) {
+    pub.clear();
+    const int end = w.step_ptr[s + 1];
+    for (int c = 0; c < C; ++c) {
+      const int4 dd = desc[(size_t)c * ns + s];
+      const unsigned char *blk = base + (size_t)dd.x * 16;
+      const int4 hdr = *reinterpret_cast<const int4 *>(blk);
+      const int4 h3 = reinterpret_cast<const int4 *>(blk)[3];
+      const RepLayout L = rep_layout<T>(hdr.x, hdr.y, h3.x, hdr.z, h3.y, w.linked);
+      if (hdr.x != dd.w || hdr.w != dd.z || L.bytes != dd.y * 16 || L.bytes > w.capB) ++bad;
+      if (s + kRepG < ns && h3.x != desc[(size_t)c * ns + s + kRepG].w) ++bad;
+      for (int h = 1; h <= 2; ++h) {
+        const int ahead = h == 1 ? kRepD - 1 : kRepPF;
+        const int4 want = s + ahead < ns ? desc[(size_t)c * ns + s + ahead] : make_int4(0, 0, 0, 0);
+        const int4 got = reinterpret_cast<const int4 *>(blk)[h];
+        if (got.x != want.x || got.y != want.y || got.z != want.z || got.w != want.w) ++bad;
+      }
+      if (hdr.x > rep_rows<kRepTPR>()) ++bad;
+      const int r0a = dd.z & ~(PER - 1);
+      const int nrc = dd.w > 0 ? (dd.z + dd.w - r0a + PER - 1) / PER : 0;
+      if (16 * nrc > w.stage_bytes - w.capB) ++bad;
+      const int4 *row = reinterpret_cast<const int4 *>(blk + L.o_row);
+      const int *npos = reinterpret_cast<const int *>(blk + L.o_npos);
+      const T *nsc = reinterpret_cast<const T *>(blk + L.o_nsc);
+      const unsigned short *slot = reinterpret_cast<const unsigned short *>(blk + L.o_slot);
+      const T *val = reinterpret_cast<const T *>(blk + L.o_val);
+      // far entries of this step's rows: listed in the block of step s - kRepG
+      const int2 *fr = nullptr;
+      const int *fq = nullptr;
+      const T *fv = nullptr;
+      if (s >= kRepG) {
+        const unsigned char *b2 = base + (size_t)desc[(size_t)c * ns + s - kRepG].x * 16;
+        const int4 g0 = *reinterpret_cast<const int4 *>(b2);
+        const int4 g3 = reinterpret_cast<const int4 *>(b2)[3];
+        if (g3.x != hdr.x) ++bad;
+        const RepLayout L2 = rep_layout<T>(g0.x, g0.y, g3.x, g0.z, g3.y, w.linked);
+        fr = reinterpret_cast<const int2 *>(b2 + L2.o_fr);
+        fq = reinterpret_cast<const int *>(b2 + L2.o_fq);
+        fv = reinterpret_cast<const T *>(b2 + L2.o_fv);
+      }
+      for (int r = 0; r < hdr.x; ++r) {
+        const int p = hdr.w + r;
+        const int4 ri = row[r];
+        const int n1 = ri.y & 0xff, nm = (ri.y >> 8) & 0xff, no = (ri.y >> 16) & 0xff;
+        const int nf = fr ? fr[r].y : 0, f0 = fr ? fr[r].x : 0;
+        int nfs = 0;
+        for (int k = w.pirp[p]; k < w.pirp[p + 1]; ++k) nfs += w.cls[k] == 2;
+        if (n1 > kRepN1 * kRepTPR || nf > kRepNF * kRepTPR || nf != nfs) ++bad;
+        if (ri.w != w.h_orig[p] || ((ri.y >> 24) & 1) != (int)w.feeds[p]) ++bad;
+        // the schedule's ring dependencies of p, in block order, and the step
+        // distance each class allows: previous step, 2..kRepG back, older
+        std::vector<int> qs;
+        std::vector<int> lo, hi;
+        for (int pass : {0, 3, 1})
+          for (int k = w.pirp[p]; k < w.pirp[p + 1]; ++k)
+            if (w.cls[k] == pass) {
+              qs.push_back(w.dep[k]);
+              lo.push_back(pass == 0 ? 1 : (pass == 3 ? 2 : kRepG + 1));
+              hi.push_back(pass == 0 ? 1 : (pass == 3 ? kRepG : 1 << 30));
+            }
+        if ((int)qs.size() != n1 + nm + no) ++bad;
+        T acc = T(0);
+        for (int e = 0; e < n1 + nm + no; ++e) {
+          const int k = ri.x + e, sl = slot[k];
+          const int q = e < (int)qs.size() ? qs[e] : -1;
+          if (q < 0 || tag[sl] != q || q < end - R) {
+            ++bad;
+          } else {
+            const int dist = s - tstep[sl];
+            if (dist < lo[e] || dist > hi[e]) ++bad;
+          }
+          acc = acc + val[k] * ring[sl];
+        }
+        for (int f = 0; f < nf; ++f) {
+          const int q = fq[f0 + f];
+          // written in this solve, not yet reset, far enough back
+          if (q < 0 || q >= n || !xvalid[q] || xstep[q] > s - kRepFarMin) ++bad;
+          acc = acc + fv[f0 + f] * xp[q];
+        }
+        const T t = rhs_pos[p] - acc;
+        pub.emplace_back(p, t);
+        out[ri.w] = t;
+        if (w.linked) (*next_pos)[npos[r]] = nsc[r] * t;
+        if ((ri.y >> 24) & 1) {
+          xp[p] = t;
+          xstep[p] = s;
+          xvalid[p] = 1;
+        }
+      }
+    }
+    for (auto &pv : pub) {
+      ring[pv.first & (R - 1)] = pv.second;
+      tag[pv.first & (R - 1)] = pv.first;
+      tstep[pv.first & (R - 1)] = s;
+    }
+    // far-copy resets of this step (every reader of them is in an earlier step)
+    for (int c = 0; c < C; ++c) {
+      const unsigned char *blk = base + (size_t)desc[(size_t)c * ns + s].x * 16;
+      const int4 hdr = *reinterpret_cast<const int4 *>(blk);
+      const int4 h3 = reinterpret_cast<const int4 *>(blk)[3];
+      const RepLayout L = rep_layout<T>(hdr.x, hdr.y, h3.x, hdr.z, h3.y, w.linked);
+      const int *rs = reinterpret_cast<const int *>(blk + L.o_rst);
+      for (int i = 0; i < h3.y; ++i) {
+        const int q = rs[i];
+        if (q < 0 || q >= n || !xvalid[q] || q % C != c) ++bad;
+        else xvalid[q] = 0;
+      }
+    }
+  }
+  // the tail resets leave the far copy clean for the next solve
+  for (int c = 0; c < C; ++c)
+    for (int i = w.h_tail_ptr[c]; i < w.h_tail_ptr[c + 1]; ++i) {
+      const int q = w.h_tail[i];
+      if (q < 0 || q >= n || !xvalid[q] || q % C != c) ++bad;
+      else xvalid[q] = 0;
+    }
+  for (int q = 0; q < n; ++q) bad += xvalid[q];
+  return bad;
+}
+
+// y = U^{-1} diag(d) L^{-1} x through the emulated pair of plans; stats: violations,
+// steps of the first plan, far entries of both, plans usable (1/0).
+template <typename T>
+static void rep_check_pair(const HostCSR &Lf, bool lupper, const HostCSR &Uf, bool uupper,
+                           const std::vector<double> &d, int C, const double *x, double *y, long long *stats) {
+  DRep<T> f = build_rep_sched<T>(Lf, lupper, C);
+  DRep<T> g = build_rep_sched<T>(Uf, uupper, C);
+  stats[0] = 0;
+  stats[1] = f.nsteps;
+  stats[2] = f.nfar + g.nfar;
+  stats[3] = 0;
+  if (!f.ok || !g.ok) return;
+  std::vector<uint4> bf, bg;
+  std::vector<int4> df, dg;
+  build_rep_blocks_host(f, &g, &d, bf, df);
+  build_rep_blocks_host(g, (const DRep<T> *)nullptr, (const std::vector<double> *)nullptr, bg, dg);
+  if (!f.ok || !g.ok) return;
+  const int n = f.n;
+  std::vector<T> rp((size_t)n), nx((size_t)n, T(0)), o1((size_t)n), o2((size_t)n);
+  for (int p = 0; p < n; ++p) rp[p] = (T)x[f.h_orig[p]];
+  int64_t bad = rep_emulate(f, bf, df, rp, o1, &nx);
+  bad += rep_emulate(g, bg, dg, nx, o2, (std::vector<T> *)nullptr);
+  for (int i = 0; i < n; ++i) y[i] = (double)o2[i];
+  stats[0] = bad;
+  stats[3] = 1;
+}
+
 template <typename T>
 static DTri<T> build_tri_dev(Arena &ar, const HostCSR &m, bool upper, int nsm) {
   DTri<T> t;
@@ -2460,6 +3036,47 @@ static Engine *make_engine(Handle *h) {
       L.minvT = ar.upload(mt);
     }
     tick("dense coarsest inverse");
+    // replicated-window cluster solves (k_trsv_rep) for the large ILU(0) levels
+    {
+      int rep_min = 65536;
+      if (const char *ev = std::getenv("MLDG_REP_MIN")) rep_min = std::atoi(ev);
+      if (H.kind == MLDG_SMOOTHER_BJAC && !L.minv && !L.win && L.n > rep_min && !std::getenv("MLDG_NO_REP")) {
+        int C = 16;
+        if (const char *ev = std::getenv("MLDG_REP_C")) C = std::atoi(ev) == 8 ? 8 : 16;
+        HostCSR Lt = transpose(H.L), Ut = transpose(H.U);
+        L.rL = build_rep_sched<T>(H.L, false, C);
+        L.rU = build_rep_sched<T>(H.U, true, C);
+        L.rUt = build_rep_sched<T>(Ut, false, C);
+        L.rLt = build_rep_sched<T>(Lt, true, C);
+        DRep<T> *rs[4] = {&L.rL, &L.rU, &L.rUt, &L.rLt};
+        bool ok = L.rL.ok && L.rU.ok && L.rUt.ok && L.rLt.ok;
+        if (ok) {
+          build_rep_blocks(ar, L.rL, &L.rU, &H.d);
+          build_rep_blocks(ar, L.rU, (const DRep<T> *)nullptr, (const std::vector<double> *)nullptr);
+          build_rep_blocks(ar, L.rUt, &L.rLt, &H.d);
+          build_rep_blocks(ar, L.rLt, (const DRep<T> *)nullptr, (const std::vector<double> *)nullptr);
+          for (DRep<T> *r : rs) ok = ok && r->ok && rep_fits(*r);
+        }
+        for (DRep<T> *r : rs) rep_release_sched(*r);
+        L.rep_ok = ok;
+        if (ok && !L.rp0) {
+          L.rp0 = ar.alloc<T>((size_t)L.n + 8);
+          L.rp1 = ar.alloc<T>((size_t)L.n + 8);
+          MLDG_CUDA(cudaMemset(L.rp0, 0, sizeof(T) * ((size_t)L.n + 8)));
+          MLDG_CUDA(cudaMemset(L.rp1, 0, sizeof(T) * ((size_t)L.n + 8)));
+        }
+        if (std::getenv("MLDG_VERBOSE")) {
+          const char *nm[4] = {"L", "U", "Ut", "Lt"};
+          for (int q = 0; q < 4; ++q)
+            std::fprintf(stderr,
+                         "mldg: level %d rep %-2s n=%d C=%d steps=%d R=%d far=%lld capB=%d stage=%d smem=%zu "
+                         "blocks=%.1f MB ok=%d\n",
+                         l, nm[q], rs[q]->n, rs[q]->C, rs[q]->nsteps, rs[q]->R, (long long)rs[q]->nfar,
+                         rs[q]->capB, rs[q]->stage_bytes, rs[q]->smem, rs[q]->block_bytes / 1e6, (int)rs[q]->ok);
+        }
+      }
+    }
+    tick("replicated-window plans");
     std::vector<T> dv(dh.begin(), dh.end());
     L.d = ar.upload(dv);
     const int n = std::max(L.n, 1);
@@ -2511,6 +3128,14 @@ static Engine *make_engine(Handle *h) {
     MLDG_CUDA(cudaStreamSynchronize(h->st));
   }
   // small intermediate levels: the explicit inverse of their ILU(0) when faster
+  // MLDG_REP_FORCE: every level with replicated-window plans uses them
+  if (std::getenv("MLDG_REP_FORCE"))
+    for (auto &L : e->lv)
+      if (L.rep_ok) {
+        L.rep = true;
+        L.ell1 = false;
+        if (std::getenv("MLDG_VERBOSE")) std::fprintf(stderr, "mldg: level n=%d uses rep (forced)\n", L.n);
+      }
   tick("autotune solves");
   if (!std::getenv("MLDG_NO_DENSE_INV"))
     for (int l = 1; l < h->nlev; ++l) {
@@ -3595,7 +4220,8 @@ extern "C" void mldg_destroy(mldg_handle *hp) {
   Handle &h = hp->h;
   cudaSetDevice(h.opts.device);
   if (h.st) cudaStreamSynchronize(h.st);
-  if (h.eng && (std::getenv("MLDG_WIN_TRACE") || std::getenv("MLDG_ELL_TRACE"))) h.eng->dump_trace();
+  if (h.eng && (std::getenv("MLDG_WIN_TRACE") || std::getenv("MLDG_ELL_TRACE") || std::getenv("MLDG_REP_TRACE")))
+    h.eng->dump_trace();
   for (int t = 0; t < 2; ++t)
     if (h.gexec[t]) cudaGraphExecDestroy(h.gexec[t]);
   mldg::drop_multi_graphs(&h);
@@ -3611,4 +4237,33 @@ extern "C" void mldg_destroy(mldg_handle *hp) {
   if (h.pev1) cudaEventDestroy(h.pev1);
   if (h.st) cudaStreamDestroy(h.st);
   delete hp;
+}
+
+// Test hook (host only, no GPU): builds the replicated-window plans of an
+// ILU(0) pair for a cluster of `cluster` CTAs and runs the pair through the
+// host emulation of k_trsv_rep.  trans 'N': y = U^{-1} diag(d) L^{-1} x;
+// 'T': y = L^{-T} diag(d) U^{-T} x.  stats[4]: plan violations, steps of the
+// first solve, far entries, plans usable.
+extern "C" int mldg_rep_plan_check(const mldg_csr *Lc, const mldg_csr *Uc, const double *d, const double *x,
+                                   double *y, int cluster, int fp32, char trans, long long *stats) {
+  if (!Lc || !Uc || !d || !x || !y || !stats || (cluster != 8 && cluster != 16)) return MLDG_ERR_ARG;
+  try {
+    mldg::HostCSR L = mldg::copy_csr(*Lc, 0, "L", 0), U = mldg::copy_csr(*Uc, 0, "U", 0);
+    std::vector<double> dv(d, d + L.nr);
+    if (trans == 'N') {
+      if (fp32)
+        mldg::rep_check_pair<float>(L, false, U, true, dv, cluster, x, y, stats);
+      else
+        mldg::rep_check_pair<double>(L, false, U, true, dv, cluster, x, y, stats);
+    } else {
+      mldg::HostCSR Ut = mldg::transpose(U), Lt = mldg::transpose(L);
+      if (fp32)
+        mldg::rep_check_pair<float>(Ut, false, Lt, true, dv, cluster, x, y, stats);
+      else
+        mldg::rep_check_pair<double>(Ut, false, Lt, true, dv, cluster, x, y, stats);
+    }
+  } catch (const mldg::Error &e) {
+    return e.code;
+  }
+  return MLDG_SUCCESS;
 }
