@@ -212,6 +212,7 @@ __global__ void __launch_bounds__(kRepThreads, 1) k_trsv_rep(RepArgs<T> a) {
   const unsigned ring_s = rep_smem_u32(ring);
   const unsigned vbar_s = rep_smem_u32(vbar);
   const int4 zero4 = make_int4(0, 0, 0, 0);
+  auto load_desc = [&](int t) { return t < a.nsteps ? desc[t] : zero4; };
 
   // After a wait that gave up (error 4021) a thread reads and writes nothing
   // more; it only keeps the cluster barriers, so the kernel still ends.
@@ -239,13 +240,14 @@ __global__ void __launch_bounds__(kRepThreads, 1) k_trsv_rep(RepArgs<T> a) {
 
   if (producer) {
     // ---- producer warp: lane 0 copies the plan and arms the value barriers ----
-    auto issue = [&](int t) {
+    // Descriptors and value bytes come 32 steps at a time, one step per lane,
+    // loaded a chunk ahead; lane 0 takes each step's entries by shuffle.
+    auto issue = [&](int t, int4 d) {
       if (lane != 0 || !live || t >= a.nsteps) return;
       if (t >= D && !mbar_wait(&empty[t % D], (unsigned)(((t - D) / D) & 1))) {
         give_up();
         return;
       }
-      const int4 d = desc[t];
       unsigned char *dst = stg + (size_t)(t % D) * a.stage_bytes;
       const int r0a = d.z & ~(PER - 1);
       const int nrc = d.w > 0 ? (d.z + d.w - r0a + PER - 1) / PER : 0;
@@ -253,9 +255,8 @@ __global__ void __launch_bounds__(kRepThreads, 1) k_trsv_rep(RepArgs<T> a) {
       tma_bulk_g2s(dst, a.blocks + d.x, 16u * (unsigned)d.y, &full[t % D]);
       if (nrc) tma_bulk_g2s(dst + a.capB, a.rhs + r0a, 16u * (unsigned)nrc, &full[t % D]);
     };
-    auto prefetch = [&](int t) {
+    auto prefetch = [&](int t, int4 d) {
       if (lane != 0 || t >= a.nsteps) return;
-      const int4 d = desc[t];
       rep_prefetch_l2(a.blocks + d.x, 16u * (unsigned)d.y);
       const int r0a = d.z & ~(PER - 1);
       const int nrc = d.w > 0 ? (d.z + d.w - r0a + PER - 1) / PER : 0;
@@ -263,21 +264,46 @@ __global__ void __launch_bounds__(kRepThreads, 1) k_trsv_rep(RepArgs<T> a) {
     };
     // expect the values of step t (every row of the cluster, one T each) once
     // the barrier's previous phase (step t - MV) has completed
-    auto arm = [&](int t) {
+    auto arm = [&](int t, int bytes) {
       if (lane != 0 || !live || t >= a.nsteps) return;
       if (t >= MV && !rep_wait_cluster(&vbar[t % MV], (unsigned)(((t - MV) / MV) & 1))) {
         give_up();
         return;
       }
-      mbar_expect_tx(&vbar[t % MV], (unsigned)a.vbytes[t]);
+      mbar_expect_tx(&vbar[t % MV], (unsigned)bytes);
     };
-    for (int t = 0; t < kRepAR; ++t) arm(t);
-    for (int t = 0; t < D - 1; ++t) issue(t);
-    for (int t = D - 1; t < kRepPF; ++t) prefetch(t);
+    auto vbytes_of = [&](int t) { return t < a.nsteps ? a.vbytes[t] : 0; };
+    for (int t = 0; t < kRepAR; ++t) arm(t, vbytes_of(t));
+    for (int t = 0; t < D - 1; ++t) issue(t, load_desc(t));
+    for (int t = D - 1; t < kRepPF; ++t) prefetch(t, load_desc(t));
+    // lane j of chunk c: the steps 32c + j + (D-1, kRepPF, kRepAR)
+    int4 ci = load_desc(D - 1 + lane), cp = load_desc(kRepPF + lane);
+    int cv = vbytes_of(kRepAR + lane);
+    int4 ni = load_desc(32 + D - 1 + lane), np = load_desc(32 + kRepPF + lane);
+    int nv = vbytes_of(32 + kRepAR + lane);
     for (int t = 0; t < a.nsteps; ++t) {
-      arm(t + kRepAR);
-      issue(t + D - 1);
-      prefetch(t + kRepPF);
+      const int j = t & 31;
+      if (j == 0 && t > 0) {
+        ci = ni;
+        cp = np;
+        cv = nv;
+        ni = load_desc(t + 32 + D - 1 + lane);
+        np = load_desc(t + 32 + kRepPF + lane);
+        nv = vbytes_of(t + 32 + kRepAR + lane);
+      }
+      const int vb = __shfl_sync(0xffffffffu, cv, j);
+      int4 di, dp;
+      di.x = __shfl_sync(0xffffffffu, ci.x, j);
+      di.y = __shfl_sync(0xffffffffu, ci.y, j);
+      di.z = __shfl_sync(0xffffffffu, ci.z, j);
+      di.w = __shfl_sync(0xffffffffu, ci.w, j);
+      dp.x = __shfl_sync(0xffffffffu, cp.x, j);
+      dp.y = __shfl_sync(0xffffffffu, cp.y, j);
+      dp.z = __shfl_sync(0xffffffffu, cp.z, j);
+      dp.w = __shfl_sync(0xffffffffu, cp.w, j);
+      arm(t + kRepAR, vb);
+      issue(t + D - 1, di);
+      prefetch(t + kRepPF, dp);
     }
     cluster_sync();
     return;
