@@ -319,9 +319,12 @@ def time_systems(mld, args, dev, torch, nsys=64, lo=24, hi=96):
     precs, bs, mats, rows = [], [], [], 0
     # throughput setting: the small levels keep their triangular solves, which
     # overlap across the concurrent systems, instead of the explicit inverses
-    # (bandwidth-bound products that a single system runs faster alone)
+    # (bandwidth-bound products that a single system runs faster alone) or
+    # the 16-SM cluster solves (which hold SMs the other systems would use)
     prev = os.environ.get("MLDG_NO_DENSE_INV")
+    prev_rep = os.environ.get("MLDG_NO_REP")
     os.environ["MLDG_NO_DENSE_INV"] = "1"
+    os.environ["MLDG_NO_REP"] = "1"
     for idim in dims:
         a = mld.gen_pde3d(int(idim), 1, ISO)
         mats.append(a)
@@ -332,6 +335,10 @@ def time_systems(mld, args, dev, torch, nsys=64, lo=24, hi=96):
         del os.environ["MLDG_NO_DENSE_INV"]
     else:
         os.environ["MLDG_NO_DENSE_INV"] = prev
+    if prev_rep is None:
+        del os.environ["MLDG_NO_REP"]
+    else:
+        os.environ["MLDG_NO_REP"] = prev_rep
     xs = [torch.zeros_like(b) for b in bs]
     mld.krylov_batch("FCG", precs, bs, xs, eps=args.eps, itmax=500)  # warm: captures the graphs
     reps = max(1, min(args.steps, 3))

@@ -3128,10 +3128,11 @@ static Engine *make_engine(Handle *h) {
     MLDG_CUDA(cudaStreamSynchronize(h->st));
   }
   // small intermediate levels: the explicit inverse of their ILU(0) when faster
-  // MLDG_REP_FORCE: every level with replicated-window plans uses them
-  if (std::getenv("MLDG_REP_FORCE"))
+  // MLDG_REP_FORCE: every level with replicated-window plans uses them (a
+  // value above 1: only the levels of at most that many rows)
+  if (const char *ev = std::getenv("MLDG_REP_FORCE"))
     for (auto &L : e->lv)
-      if (L.rep_ok) {
+      if (L.rep_ok && (std::atol(ev) <= 1 || L.n <= std::atol(ev))) {
         L.rep = true;
         L.ell1 = false;
         if (std::getenv("MLDG_VERBOSE")) std::fprintf(stderr, "mldg: level n=%d uses rep (forced)\n", L.n);
