@@ -67,3 +67,18 @@ def test_rep_krylov_iterations_match(mld, orc, monkeypatch, capfd):
     assert abs(it - it_ref) <= 1, (it, it_ref)
     assert rr <= 1e-10
     assert np.linalg.norm(x - 1) / np.sqrt(a.nrows) < 1e-6
+
+
+@pytest.mark.parametrize("idim,cluster", [(3, 16), (12, 8), (12, 16)])
+def test_rep_few_steps(mld, orc, monkeypatch, capfd, idim, cluster):
+    """Levels of 7 to 74 steps: fewer steps than the step groups, the stage
+    lookahead or one 32-step descriptor chunk of the producer."""
+    _force(monkeypatch, None, cluster)
+    a = orc.gen_pde3d(idim, 1, ISO)
+    op = orc.Prec(oracle_params(orc, "BJAC", mcs=20))
+    op.build(a)
+    h = upload_oracle_hierarchy(mld, orc, op)
+    assert "uses rep" in capfd.readouterr().err
+    x = np.random.default_rng(idim).uniform(-1, 1, a.nrows)
+    for trans in ("N", "T"):
+        assert _rel(h.apply(x, trans=trans), op.apply(x, trans)) <= TOL_FP64
