@@ -577,7 +577,6 @@ __global__ void __launch_bounds__(512) k_trsv_stg(TriArgs<T> a, StageCfg c, cons
 
 template <typename T, int TPR, int E>
 __global__ void __launch_bounds__(256) k_trsv_sf(TriArgs<T> a) {
-  constexpr int RPW = 32 / TPR;
   const int lane = threadIdx.x & 31;
   const int sub = lane % TPR;
   const int grp = lane / TPR;

@@ -115,7 +115,6 @@ __global__ void __launch_bounds__(256) k_gemm_m(int n, const T *__restrict__ M, 
 // sentinel until produced; a lane waits only on its own column.
 template <typename T, int K>
 __global__ void __launch_bounds__(256) k_trsv_sf_m(TriArgs<T> a, int nblk_m, const int2 *blk_m) {
-  constexpr int RPW = 32 / K;
   const int lane = threadIdx.x & 31;
   const int c = lane % K;
   const int grp = lane / K;
