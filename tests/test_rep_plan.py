@@ -85,3 +85,50 @@ def test_rep_plan_far_path_and_split_steps(mld, orc, monkeypatch):
     st, err = _check(mld, Lm, Um, d, 8, 0, "N")
     nlev = 3 * 40 - 2  # dependency levels of the 7-point lower triangle
     assert st[3] == 1 and st[1] > nlev and st[0] == 0 and err <= 1e-13
+
+
+def _random_pair(seed, n, reach, per_row):
+    """Random strict triangles with a mix of short and long dependencies."""
+    rng = np.random.default_rng(seed)
+
+    def tri(lower):
+        irp, ja, val = [0], [], []
+        for i in range(n):
+            cand = []
+            for _ in range(rng.integers(0, per_row + 1)):
+                back = int(rng.integers(1, reach)) if rng.random() < 0.8 else int(rng.integers(1, n))
+                j = i - back if lower else i + back
+                if 0 <= j < n:
+                    cand.append(j)
+            cols = sorted(set(cand))
+            ja += cols
+            val += list(rng.uniform(-0.3, 0.3, len(cols)))
+            irp.append(len(ja))
+        return (np.array(irp, np.int32), np.array(ja if ja else [0], np.int32)[:len(ja)],
+                np.array(val if val else [0.0])[:len(val)])
+
+    class M:
+        pass
+    Lm, Um = M(), M()
+    Lm.irp, Lm.ja, Lm.val = tri(True)
+    Um.irp, Um.ja, Um.val = tri(False)
+    d = rng.uniform(0.5, 1.5, n)
+    return Lm, Um, d
+
+
+@pytest.mark.parametrize("seed,n,reach,per_row,ring", [(1, 3000, 40, 6, None), (2, 5000, 400, 4, "2048"),
+                                                      (3, 2000, 8, 30, None), (4, 6000, 3000, 3, "1024")])
+def test_rep_plan_random_structures(mld, monkeypatch, seed, n, reach, per_row, ring):
+    """Irregular triangles: plans are either rejected or replay without a
+    single violation and match a direct solve, for both cluster sizes, both
+    precisions and both triangle orders."""
+    if ring:
+        monkeypatch.setenv("MLDG_REP_R", ring)
+    Lm, Um, d = _random_pair(seed, n, reach, per_row)
+    for cluster in (8, 16):
+        for fp32, tol in ((0, 1e-12), (1, 1e-5)):
+            for trans in ("N", "T"):
+                st, err = _check(mld, Lm, Um, d, cluster, fp32, trans)
+                assert st[0] == 0, "plan violations"
+                if st[3]:
+                    assert err <= tol, (cluster, fp32, trans, err)
