@@ -2403,7 +2403,7 @@ static void build_rep_blocks_host(DRep<T> &w, const DRep<T> *next, const std::ve
     const RepLayout L = rep_layout<T>(nr, ne_of[(size_t)i], nr2, nf2, nrst, w.linked);
     int4 *hdr = reinterpret_cast<int4 *>(blk);
     hdr[0] = make_int4(nr, ne_of[(size_t)i], nf2, a);
-    // the blocks this CTA copies and prefetches while this one is staged
+    // copies of the descriptors of the blocks copied and prefetched while this one is staged
     hdr[1] = st + kRepD - 1 < ns ? desc[(size_t)i + kRepD - 1] : make_int4(0, 0, 0, 0);
     hdr[2] = st + kRepPF < ns ? desc[(size_t)i + kRepPF] : make_int4(0, 0, 0, 0);
     hdr[3] = make_int4(nr2, nrst, 0, 0);

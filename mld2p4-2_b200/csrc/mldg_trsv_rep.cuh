@@ -52,8 +52,8 @@ namespace mldg {
 
 // Byte layout of the plan block of one CTA for step t (arrays 16-byte aligned):
 //   int4 hdr  {nr, ne, nf2, r0}
-//   int4 cp   descriptor of the block this CTA copies while this one is staged (t + D - 1)
-//   int4 pf   descriptor of the block it prefetches into L2 then (t + RP)
+//   int4 cp   copy of the descriptor of step t + D - 1 (checked by the host emulation; the
+//   int4 pf   producer warp reads the descriptor table) and of step t + RP
 //   int4 h3   {nrG, nrst, 0, 0}: rows of this CTA in step t + kRepG, far-copy positions to reset
 //   int4 row[nr]  {ebeg, cnt, 0, orig}      cnt = n1 | nm << 8 | no << 16 | feeds_far << 24
 //   int  npos[nr], T nsc[nr]                (linked solves only)
@@ -114,7 +114,7 @@ struct RepArgs {
   int off_bar;      // byte offset of the mbarriers in shared memory: full[D], empty[D], values[MV]
   const int *vbytes;  // [nsteps] bytes of the values of each step (every row of the cluster)
   int *err;
-  unsigned long long *trace;  // optional [20]: cycles per phase, steps, kernel cycles and ns of threads 0 and 511 of CTA 0
+  unsigned long long *trace;  // optional [20]: per-phase cycles, steps, kernel cycles and ns of the first thread of groups 0 and 1 in CTA 0
 };
 
 __device__ __forceinline__ unsigned rep_smem_u32(const void *p) {
