@@ -41,6 +41,12 @@ int mldp_hierarchy_build(mldp_prec *p, int n, const int32_t *irp, const int32_t 
 /* prec%smoothers_build(a, desc_a, info) (impl/mld_d_smoothers_bld.f90) and
  * upload of the hierarchy to the GPU (mldg_upload_level + mldg_finalize) */
 int mldp_smoothers_build(mldp_prec *p);
+/* The host half of mldp_smoothers_build: the smoother and solver data of
+ * every level (ILU(0) factors L, U and pivots, the GS split, the Jacobi
+ * off-diagonal part and inverse diagonal) without the upload to the GPU, so
+ * that they can be read back (mldp_level_csr / mldp_level_vec) and compared
+ * on a machine without a GPU.  No counterpart in the reference. */
+int mldp_smoothers_build_host(mldp_prec *p);
 /* prec%build = hierarchy_build + smoothers_build (impl/mld_dprecbld.f90) */
 int mldp_build(mldp_prec *p, int n, const int32_t *irp, const int32_t *ja, const double *val);
 /* prec%apply(x, y, desc_a, info, trans) */

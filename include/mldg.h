@@ -3,7 +3,8 @@
  *
  * This is the drop-in boundary for MLD2P4 2.1's `prec%apply`: a Fortran
  * 2003 extension of mld_dprec_type overrides psb_d_apply2_vect and reaches
- * these entry points through ISO_C_BINDING.  The level
+ * these entry points through ISO_C_BINDING (the module mldg_cbind in
+ * mld2p4-2_b200/fortran/mldg_cbind.f90).  The level
  * hierarchy built on the host by mld_dprecbld (aggregation, smoothed
  * prolongators, Galerkin products, ILU(0)/diagonal factors) is uploaded
  * unchanged, level by level; the V-cycle then runs on the GPU.
@@ -223,10 +224,18 @@ int mldg_level_info(const mldg_handle *h, int lev, int64_t *info);
  * events on the handle's stream, and the number of kernel launches it made. */
 int mldg_last_timing(const mldg_handle *h, double *ms, int64_t *launches);
 
-/* Bytes an FP64 (or the finalized precision's) V-cycle apply must move at
- * least: every CSR operand once + every dense vector operand once (the
- * roofline numerator). */
+/* Algorithmic bytes of one V-cycle apply (trans 'N') in the finalized
+ * precision: every sparse operand of the reference's operation sequence
+ * (mld_dmlprec_aply.f90:590-809) once, CSR bytes nnz*(value + index size) +
+ * 4*(rows+1), plus every dense vector operand read once and every output
+ * written once (the roofline numerator).  A level whose ILU(0) or GS solves
+ * run as products with an explicit dense inverse counts the sparse factors
+ * it stands for.  Valid after the first apply. */
 int mldg_apply_bytes(const mldg_handle *h, int64_t *bytes);
+/* Bytes the chosen kernels of one V-cycle apply move: as mldg_apply_bytes,
+ * except that a dense-inverse product counts its n*n matrix.  No counterpart
+ * in the reference. */
+int mldg_apply_impl_bytes(const mldg_handle *h, int64_t *bytes);
 
 /* ---- diagnostics: per-kernel device time ------------------------------- */
 #define MLDG_KERNEL_TRSV 1    /* sparse unit-triangular solve (ILU factors)   */
@@ -260,10 +269,10 @@ int mldg_profile_multi(mldg_handle *h, char trans, int nrhs, int max, mldg_kerne
 
 /* ---- allocation-free relative residual --------------------------------- */
 /* No counterpart in the reference.  For callers that must not allocate
- * device memory: code that runs while a CUDA graph is being captured (where
- * cudaMalloc is not allowed), applications whose memory pool owns every
- * device byte, and convergence checks in tight loops where cudaMalloc /
- * cudaFree would synchronise the device.
+ * device memory: applications whose memory pool or allocator owns every
+ * device byte (a second allocator would fragment or overcommit it), and
+ * convergence checks in tight host loops, where cudaMalloc / cudaFree would
+ * synchronise the whole device on every call.
  *
  * Computes *relres = ||b - A x||_2 / ||b||_2 (1 when ||b|| = 0).  A's arrays
  * and x, b are DEVICE pointers, 0-based CSR, nrows == ncols == n.  The
@@ -274,8 +283,9 @@ int mldg_profile_multi(mldg_handle *h, char trans, int nrhs, int max, mldg_kerne
  * up the array's device address (cudaGetSymbolAddress) once, so make that
  * first call before any stream capture.  All calls share the array and it
  * keeps the last call's contents; calls that overlap on the GPU (other
- * streams, other threads) race on it.  Runs on the handle's stream and
- * returns after the result is on the host. */
+ * streams, other threads) race on it.  Runs on the handle's stream, copies
+ * the result to the host and waits for it: the call returns with *relres
+ * set. */
 #define MLDG_NOALLOC_MAX_N 524288
 int mldg_relres_noalloc(mldg_handle *h, const mldg_csr *A, const double *x, const double *b,
                         double *relres);

@@ -155,8 +155,15 @@ class _GpuDiag:
         return X, np.array(it[:nrhs]), np.array(rr[:nrhs])
 
     def apply_bytes(self) -> int:
+        """Algorithmic bytes of one V-cycle apply (mldg_apply_bytes)."""
         b = C.c_int64(0)
         lib().mldg_apply_bytes(self._gpu(), C.byref(b))
+        return b.value
+
+    def apply_impl_bytes(self) -> int:
+        """Bytes the chosen kernels of one V-cycle apply move (dense inverses at full size)."""
+        b = C.c_int64(0)
+        lib().mldg_apply_impl_bytes(self._gpu(), C.byref(b))
         return b.value
 
 
@@ -186,6 +193,7 @@ def lib():
         L.mldg_level_info.argtypes = [vp, C.c_int, C.POINTER(C.c_int64)]
         L.mldg_last_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
         L.mldg_apply_bytes.argtypes = [vp, C.POINTER(C.c_int64)]
+        L.mldg_apply_impl_bytes.argtypes = [vp, C.POINTER(C.c_int64)]
         L.mldg_probe_set.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         L.mldg_probe_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                       C.POINTER(C.c_int64)]
@@ -209,6 +217,7 @@ def lib():
         L.mldp_setc.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_int]
         L.mldp_hierarchy_build.argtypes = [vp, C.c_int, ip, ip, dp]
         L.mldp_smoothers_build.argtypes = [vp]
+        L.mldp_smoothers_build_host.argtypes = [vp]
         L.mldp_build.argtypes = [vp, C.c_int, ip, ip, dp]
         L.mldp_apply.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_char, C.c_int]
         L.mldp_krylov.argtypes = [vp, C.c_char_p, C.c_int, ip, ip, dp, C.c_void_p, C.c_void_p,
@@ -452,6 +461,10 @@ class MldPrec(_GpuDiag):
 
     def smoothers_build(self):
         self._check(lib().mldp_smoothers_build(self._p))
+
+    def smoothers_build_host(self):
+        """Smoother/solver data on the host only (no GPU upload), for checking."""
+        self._check(lib().mldp_smoothers_build_host(self._p))
 
     def build(self, a: CSR):
         self.hierarchy_build(a)

@@ -269,6 +269,14 @@ extern "C" int mldp_smoothers_build(mldp_prec *p) {
   return rc;
 }
 
+extern "C" int mldp_smoothers_build_host(mldp_prec *p) {
+  if (!p) return MLDG_ERR_ARG;
+  if (!p->hier_built) return fail(p, 3112, "smoothers_build before hierarchy_build");
+  std::string msg;
+  const int rc = mld::smoothers_build(p->lv, p->parms, msg);
+  return rc ? fail(p, rc, msg) : 0;
+}
+
 // the finished host levels -> the GPU handle (mldg_upload_level + finalize)
 static int upload_all(mldp_prec *p) {
   int rc = 0;

@@ -365,7 +365,12 @@ struct Engine {
   int mcap = 0;
   virtual void dump_trace() {}
   int64_t launches = 0;
-  int64_t bytes = 0;
+  // bytes: algorithmic bytes of the recorded launches (each sparse operand of
+  // the reference's operation once, each dense vector operand once);
+  // impl_bytes: what the chosen implementation reads and writes, which
+  // differs where a level's ILU(0) or GS solves run as products with an
+  // explicit dense inverse
+  int64_t bytes = 0, impl_bytes = 0;
   cudaStream_t st = nullptr;
   int cycle = MLDG_CYCLE_V;  // MLDG_CYCLE_V / _W / _K / _KSYM
   // ---- launch accounting, probe and profile hooks ----
@@ -405,17 +410,20 @@ struct Engine {
       prof->push_back(e);
     }
   }
-  void end(int64_t b) {
+  // b: bytes the launch moves; alg: its algorithmic bytes when they differ
+  void end(int64_t b, int64_t alg = -1) {
+    if (alg < 0) alg = b;
     launches++;
-    bytes += b;
+    bytes += alg;
+    impl_bytes += b;
     if (pmatch) {
       rec(pev1);
-      probe_bytes = b;
+      probe_bytes = alg;
       probe_armed = true;
       pmatch = false;
     }
     if (prof) {
-      prof->back().bytes = b;
+      prof->back().bytes = alg;
       MLDG_CUDA(cudaEventRecord(prof->back().e1, st));
     }
   }
@@ -501,6 +509,10 @@ struct EngineT : Engine {
     int n = 0, kind = 0, spre = 1, spost = 1;
     double damp = 1.0;
     int64_t nnz_nd = 0;
+    // stored entries of the two triangular factors (ILU(0) L, U or the GS
+    // strict triangles): the algorithmic bytes of a level whose solves run
+    // as dense products
+    int64_t nnz_l = 0, nnz_u = 0;
     DCSR<T> A, AT, P, R, ND, NDT;
     DTri<T> L, U, Lt, Ut;
     T *d = nullptr;
@@ -673,6 +685,7 @@ struct EngineT : Engine {
     }
     launches = 0;
     bytes = 0;
+    impl_bytes = 0;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
   }
@@ -762,7 +775,10 @@ struct EngineT : Engine {
       const T *M = (trans == 'N') ? L.minv : L.minvT;
       begin(MLDG_KERNEL_VEC);
       k_gemv<T><<<blocks_for((int64_t)L.n * 32), 256, 0, st>>>(L.n, M, x, T(1), beta, y);
-      end((int64_t)L.n * L.n * sizeof(T) + (int64_t)L.n * sizeof(T) * (2 + (beta != T(0))));
+      // algorithmic: the two sparse solves and the pivot scaling it replaces
+      end((int64_t)L.n * L.n * sizeof(T) + (int64_t)L.n * sizeof(T) * (2 + (beta != T(0))),
+          (L.nnz_l + L.nnz_u) * (int64_t)(sizeof(T) + 4) + 8 * ((int64_t)L.n + 1) +
+              (int64_t)L.n * sizeof(T) * (3 + (beta != T(0))));
       return;
     }
     if (L.ell1) {
@@ -810,7 +826,10 @@ struct EngineT : Engine {
       const T *M = backward ? L.gsB : L.gsF;
       begin(MLDG_KERNEL_VEC);
       k_gemv<T><<<blocks_for((int64_t)L.n * 32), 256, 0, st>>>(L.n, M, rhs, T(1), beta, out);
-      end((int64_t)L.n * L.n * sizeof(T) + (int64_t)L.n * sizeof(T) * (2 + (beta != T(0))));
+      // algorithmic: the sparse triangular solve (with its diagonal) it replaces
+      end((int64_t)L.n * L.n * sizeof(T) + (int64_t)L.n * sizeof(T) * (2 + (beta != T(0))),
+          (backward ? L.nnz_u : L.nnz_l) * (int64_t)(sizeof(T) + 4) + 4 * ((int64_t)L.n + 1) +
+              (int64_t)L.n * sizeof(T) * (3 + (beta != T(0))));
       return;
     }
     const DTri<T> &t = backward ? L.U : L.L;
@@ -1099,6 +1118,7 @@ struct EngineT : Engine {
     }
     launches = 0;
     bytes = 0;
+    impl_bytes = 0;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
   }
@@ -1372,6 +1392,7 @@ struct EngineT : Engine {
                    t[0] / 3, t[1] / 3, keep ? "dense" : "solves");
     launches = 0;
     bytes = 0;
+    impl_bytes = 0;
     return keep;
   }
   bool ensure_multi(int Kw) override {
@@ -1548,7 +1569,9 @@ struct EngineT : Engine {
         constexpr int KK = decltype(kc)::value;
         k_gemm_m<T, KK><<<blocks_for(nk(L.n)), 256, 0, st>>>(L.n, M, x, T(1), beta, y);
       });
-      end((int64_t)L.n * L.n * sizeof(T) + nk(L.n) * (int64_t)sizeof(T) * (2 + (beta != T(0))));
+      end((int64_t)L.n * L.n * sizeof(T) + nk(L.n) * (int64_t)sizeof(T) * (2 + (beta != T(0))),
+          (L.nnz_l + L.nnz_u) * (int64_t)(sizeof(T) + 4) + 8 * ((int64_t)L.n + 1) +
+              (int64_t)L.n * sizeof(T) + nk(L.n) * (int64_t)sizeof(T) * (2 + (beta != T(0))));
       return;
     }
     if (trans == 'N') {
@@ -1568,7 +1591,9 @@ struct EngineT : Engine {
         constexpr int KK = decltype(kc)::value;
         k_gemm_m<T, KK><<<blocks_for(nk(L.n)), 256, 0, st>>>(L.n, M, rhs, T(1), beta, out);
       });
-      end((int64_t)L.n * L.n * sizeof(T) + nk(L.n) * (int64_t)sizeof(T) * (2 + (beta != T(0))));
+      end((int64_t)L.n * L.n * sizeof(T) + nk(L.n) * (int64_t)sizeof(T) * (2 + (beta != T(0))),
+          (backward ? L.nnz_u : L.nnz_l) * (int64_t)(sizeof(T) + 4) + 4 * ((int64_t)L.n + 1) +
+              (int64_t)L.n * sizeof(T) + nk(L.n) * (int64_t)sizeof(T) * (2 + (beta != T(0))));
       return;
     }
     DTri<T> &t = backward ? L.U : L.L;
@@ -1708,6 +1733,7 @@ struct EngineT : Engine {
     if (kcycle_mode()) fail(MLDG_ERR_ARG, "the K-cycle has no multi-column form");
     launches = 0;
     bytes = 0;
+    impl_bytes = 0;
     cur_lev = 0;
     probe_armed = false;
     std::memset(seen, 0, sizeof seen);
@@ -1826,6 +1852,7 @@ struct EngineT : Engine {
   void record(char trans) override {
     launches = 0;
     bytes = 0;
+    impl_bytes = 0;
     cur_lev = 0;
     probe_armed = false;
     std::memset(seen, 0, sizeof seen);
@@ -1914,11 +1941,15 @@ struct Handle {
   int n0 = 0;
   // graphs per trans
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
-  int64_t glaunch[2] = {0, 0}, gbytes[2] = {0, 0};
+  int64_t glaunch[2] = {0, 0}, gbytes[2] = {0, 0}, gimpl[2] = {0, 0};
   // Krylov state (FP64)
   DCSR<double> A0, A0T;
-  double *kb = nullptr, *kx = nullptr, *kd = nullptr, *kq = nullptr, *kpart = nullptr;
-  KrylovScalars *ksc = nullptr;
+  // FP64 Krylov state: b, x, the two alternating direction buffers, q = A d,
+  // per-block partial sums, the device scalars (KState) and the parameters
+  // of the current solve, with pinned host mirrors of both
+  double *kb = nullptr, *kx = nullptr, *kd = nullptr, *kd1 = nullptr, *kq = nullptr, *kpart = nullptr;
+  KState *kst = nullptr, *hkst = nullptr;
+  KParams *kpar = nullptr, *hkpar = nullptr;
   double *hpin = nullptr;  // pinned host scalar mirror
   double last_ms = 0;
   int64_t last_launches = 0;
@@ -1938,9 +1969,12 @@ struct Handle {
   int kcap = 0;
   double *kb_m = nullptr, *kx_m = nullptr, *kd_m = nullptr, *kq_m = nullptr, *kpart_m = nullptr;
   KrylovM *ksc_m = nullptr, *hksc_m = nullptr;  // device state, pinned host mirror
-  // one captured CG/FCG iteration per [method][first] (systems solved in a batch)
-  cudaGraphExec_t kgraph[2][2] = {};
-  int64_t kglaunch[2][2] = {};
+  // one whole CG/FCG solve per [method][trans] as a CUDA graph: the initial
+  // residual, then a conditional WHILE node repeating V-cycle + iteration
+  // until the device-side stopping test clears it; launches of the prefix and
+  // of one loop body
+  cudaGraphExec_t sgraph[2][2] = {};
+  int64_t sglaunch_pre[2][2] = {}, sglaunch_body[2][2] = {};
 };
 
 // the GS solvers accept trans = 'N' only (mld_d_gs_solver_apply_vect.f90:68-75)
@@ -1951,10 +1985,10 @@ static void check_trans(const Handle *h, char trans) {
 
 static void drop_krylov_graphs(Handle *h) {
   for (int m = 0; m < 2; ++m)
-    for (int f = 0; f < 2; ++f)
-      if (h->kgraph[m][f]) {
-        cudaGraphExecDestroy(h->kgraph[m][f]);
-        h->kgraph[m][f] = nullptr;
+    for (int t = 0; t < 2; ++t)
+      if (h->sgraph[m][t]) {
+        cudaGraphExecDestroy(h->sgraph[m][t]);
+        h->sgraph[m][t] = nullptr;
       }
 }
 
@@ -2945,6 +2979,10 @@ static Engine *make_engine(Handle *h) {
       }
     }
     L.nnz_nd = H.ND.nnz();
+    if (H.kind == MLDG_SMOOTHER_BJAC || H.kind == MLDG_SMOOTHER_FBGS) {
+      L.nnz_l = H.L.nnz();
+      L.nnz_u = H.U.nnz();
+    }
     tick("matrices (A, A^T, P, R upload)");
     if (H.kind == MLDG_SMOOTHER_BJAC && !std::getenv("MLDG_NO_WIN")) {
       const int n = H.A.nr;
@@ -3180,6 +3218,8 @@ static void check_level(const HostLevel &H, int l, const HostLevel *prev) {
   if (H.sweeps_pre < 0 || H.sweeps_post < 0) fail(MLDG_ERR_ARG, "level %d: negative sweeps", l);
 }
 
+static void tune_krylov_spmv(Handle *h);
+
 static void finalize(Handle *h, int nlev, int precision) {
   if (nlev < 1 || nlev > (int)h->host.size()) fail(MLDG_ERR_ARG, "nlev %d: %zu levels uploaded", nlev, h->host.size());
   for (int l = 0; l < nlev; ++l)
@@ -3216,14 +3256,20 @@ static void finalize(Handle *h, int nlev, int precision) {
   h->kb = h->arena.alloc<double>(n0);
   h->kx = h->arena.alloc<double>(n0);
   h->kd = h->arena.alloc<double>(n0);
+  h->kd1 = h->arena.alloc<double>(n0);
   h->kq = h->arena.alloc<double>(n0);
-  h->kpart = h->arena.alloc<double>(3 * kRedBlocks);
-  h->ksc = h->arena.alloc<KrylovScalars>(1);
+  // partials: 3 per reduction block, or 2 per block of the fused SpMV
+  h->kpart = h->arena.alloc<double>(std::max(3 * kRedBlocks, 2 * 16 * h->nsm));
+  h->kst = h->arena.alloc<KState>(1);
+  h->kpar = h->arena.alloc<KParams>(1);
+  if (!h->hkst) MLDG_CUDA(cudaMallocHost(&h->hkst, sizeof(KState)));
+  if (!h->hkpar) MLDG_CUDA(cudaMallocHost(&h->hkpar, sizeof(KParams)));
   if (precision == MLDG_PREC_FP64)
     h->eng.reset(make_engine<double>(h));
   else
     h->eng.reset(make_engine<float>(h));
   h->finalized = true;
+  if (h->opts.autotune) tune_krylov_spmv(h);
 }
 
 static bool kcycle_handle(const Handle *h) { return h->cycle == MLDG_CYCLE_K || h->cycle == MLDG_CYCLE_KSYM; }
@@ -3248,6 +3294,7 @@ static void run_vcycle(Handle *h, char trans) {
       cudaGraphDestroy(g);
       h->glaunch[t] = h->eng->launches;
       h->gbytes[t] = h->eng->bytes;
+      h->gimpl[t] = h->eng->impl_bytes;
       h->gprobe[t] = h->eng->probe_armed;
       if (h->eng->probe_armed) h->probe_bytes = h->eng->probe_bytes;
     }
@@ -3258,6 +3305,7 @@ static void run_vcycle(Handle *h, char trans) {
     h->eng->record(trans);
     h->glaunch[t] = h->eng->launches;
     h->gbytes[t] = h->eng->bytes;
+    h->gimpl[t] = h->eng->impl_bytes;
     h->last_launches += h->eng->launches;
     h->pending = h->eng->probe_armed;
     if (h->eng->probe_armed) h->probe_bytes = h->eng->probe_bytes;
@@ -3407,13 +3455,6 @@ static void apply(Handle *h, const double *x, double *y, char trans, int nrhs, i
 }
 
 // ---------------------------------------------------------------------------
-static void dots(Handle *h, int n, int np, const double *x0, const double *y0, const double *x1,
-                 const double *y1, const double *x2, const double *y2) {
-  k_dots<<<kRedBlocks, kRedThreads, 0, h->st>>>(n, np, x0, y0, x1, y1, x2, y2, h->kpart);
-  k_dots_final<<<1, kRedThreads, 0, h->st>>>(kRedBlocks, h->kpart, h->ksc->dots);
-  h->last_launches += 2;
-}
-
 static void spmv64(Handle *h, const DCSR<double> &A, const double *v, double a1, const double *b,
                    double a0, double *out) {
   const int64_t thr = (int64_t)A.nr * A.tpr;
@@ -3433,32 +3474,174 @@ static void spmv64(Handle *h, const DCSR<double> &A, const double *v, double a1,
   h->last_launches++;
 }
 
-// One CG/FCG iteration after the preconditioner apply z = M^{-1} r: the
-// direction update, q = A d, the step and ||r||^2 into sc->dots[0]
-// (psb_dcg / psb_dfcg, one iteration; all scalars stay on the device).
-static void krylov_body(Handle *h, const DCSR<double> &A, int method, bool first) {
-  const int n = h->n0, nb = kRedBlocks;
-  double *r = h->xin, *z = h->yout, *d = h->kd, *q = h->kq, *xx = h->kx;
-  KrylovScalars *sc = h->ksc;
-  if (method == 1) {
-    if (!first) {
-      dots(h, n, 1, z, q, nullptr, nullptr, nullptr, nullptr);
-      k_scal_store<<<1, 32, 0, h->st>>>(sc, 0);
-      h->last_launches++;
-    }
-  } else {
-    dots(h, n, 1, r, z, nullptr, nullptr, nullptr, nullptr);
-    k_scal_store<<<1, 32, 0, h->st>>>(sc, 0);
-    h->last_launches++;
+// The initial residual r = b - A x and the Krylov state (k_kry_init) from
+// the parameters in h->kpar; hc != 0 also sets the graph conditional.
+static void krylov_prefix(Handle *h, const DCSR<double> &A, cudaGraphConditionalHandle hc) {
+  const int n = h->n0;
+  spmv64(h, A, h->kx, -1.0, h->kb, 1.0, h->xin);  // r = b - A x
+  k_dots<<<kRedBlocks, kRedThreads, 0, h->st>>>(n, 2, h->kb, h->kb, h->xin, h->xin, nullptr, nullptr,
+                                                h->kpart);
+  k_kry_init<<<1, kRedThreads, 0, h->st>>>(kRedBlocks, h->kpart, h->kpar, h->kst, hc);
+  h->last_launches += 2;
+}
+
+// One CG/FCG iteration after the preconditioner apply z = M^{-1} r (in yout):
+// three fused kernels (mldg_kernels.cuh, k_kry_*); every kernel returns at
+// once when the device state says the solve is done.
+static void kry_spmv(Handle *h, const DCSR<double> &A) {
+  double *r = h->xin, *z = h->yout;
+  const int64_t thr = (int64_t)A.nr * A.tpr;
+  const int g = (int)std::max<int64_t>(1, std::min<int64_t>((thr + 255) / 256, (int64_t)h->nsm * 16));
+  switch (A.tpr) {
+#define CASE(K)                                                                                  \
+  case K:                                                                                        \
+    if (A.jd)                                                                                    \
+      k_kry_spmv<K, short><<<g, 256, 0, h->st>>>(A.nr, A.irp, A.jd, A.val, z, h->kd, h->kd1, h->kq, r, \
+                                                 h->kst, h->kpart);                              \
+    else                                                                                         \
+      k_kry_spmv<K, int><<<g, 256, 0, h->st>>>(A.nr, A.irp, A.ja, A.val, z, h->kd, h->kd1, h->kq, r,   \
+                                               h->kst, h->kpart);                                \
+    break;
+    CASE(1) CASE(2) CASE(4) CASE(8) CASE(16) CASE(32)
+#undef CASE
+    default: fail(MLDG_ERR_INTERNAL, "bad tpr");
   }
-  k_dir_update<<<nb, 256, 0, h->st>>>(n, method, first ? 1 : 0, z, d, sc);
-  spmv64(h, A, d, 1.0, nullptr, 0.0, q);  // q = A d
-  dots(h, n, 2, d, q, d, r, nullptr, nullptr);
-  k_scal_store<<<1, 32, 0, h->st>>>(sc, 1);
-  k_xr_update<<<nb, kRedThreads, 0, h->st>>>(n, method, d, q, xx, r, sc, h->kpart);
-  k_dots_final<<<1, kRedThreads, 0, h->st>>>(nb, h->kpart, sc->dots);
-  k_scal_store<<<1, 32, 0, h->st>>>(sc, 2);
-  h->last_launches += 6;
+}
+
+static void krylov_iteration(Handle *h, const DCSR<double> &A, cudaGraphConditionalHandle hc) {
+  const int n = h->n0;
+  double *r = h->xin, *z = h->yout;
+  k_kry_beta<<<kRedBlocks, kRedThreads, 0, h->st>>>(n, z, h->kq, r, h->kst, h->kpart);
+  kry_spmv(h, A);
+  k_kry_update<<<kRedBlocks, kRedThreads, 0, h->st>>>(n, h->kd, h->kd1, h->kq, h->kx, r, h->kst, h->kpart,
+                                                      hc);
+  h->last_launches += 3;
+}
+
+// Lanes per row of the finest matrix in the fused Krylov SpMV, picked by
+// timing (finalize): the state is set to a mid-solve iteration on zero
+// vectors, and the kernel is timed for each width.
+static void tune_krylov_spmv(Handle *h) {
+  DCSR<double> &A = h->A0;
+  if (!A.present() || A.nr == 0) return;
+  KState s0 = {};
+  s0.bn2 = 1.0;
+  s0.it = 1;
+  s0.itmax = 1 << 30;
+  s0.method = 1;
+  s0.beta = 0.5;
+  cudaEvent_t e0, e1;
+  MLDG_CUDA(cudaEventCreate(&e0));
+  MLDG_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int best_t = A.tpr;
+  for (double *v : {h->kd, h->kd1, h->kq}) MLDG_CUDA(cudaMemsetAsync(v, 0, sizeof(double) * (size_t)h->n0, h->st));
+  for (int t : {1, 2, 4, 8, 16, 32}) {
+    A.tpr = t;
+    *h->hkst = s0;
+    MLDG_CUDA(cudaMemcpyAsync(h->kst, h->hkst, sizeof(KState), cudaMemcpyHostToDevice, h->st));
+    kry_spmv(h, A);  // warm
+    MLDG_CUDA(cudaEventRecord(e0, h->st));
+    for (int r = 0; r < 5; ++r) kry_spmv(h, A);
+    MLDG_CUDA(cudaEventRecord(e1, h->st));
+    MLDG_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    MLDG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best) {
+      best = ms;
+      best_t = t;
+    }
+  }
+  A.tpr = best_t;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // leave clean vectors behind
+  MLDG_CUDA(cudaMemsetAsync(h->kd, 0, sizeof(double) * (size_t)h->n0, h->st));
+  MLDG_CUDA(cudaMemsetAsync(h->kd1, 0, sizeof(double) * (size_t)h->n0, h->st));
+  MLDG_CUDA(cudaMemsetAsync(h->kq, 0, sizeof(double) * (size_t)h->n0, h->st));
+  MLDG_CUDA(cudaStreamSynchronize(h->st));
+}
+
+// Captures a whole solve (method, trans) on the handle's own matrix A as one
+// graph: prefix, then a WHILE node whose body is the V-cycle and one
+// iteration.  The stopping test runs on the device, so the solve makes no
+// host round trip; the iteration count is read back afterwards.
+static void capture_solve(Handle *h, int method, char trans, const DCSR<double> &A) {
+  const int t = trans == 'N' ? 0 : 1;
+  if (h->sgraph[method][t]) return;
+  cudaGraph_t g = nullptr;
+  MLDG_CUDA(cudaGraphCreate(&g, 0));
+  const int64_t l0 = h->last_launches;
+  try {
+    cudaGraphConditionalHandle hc;
+    MLDG_CUDA(cudaGraphConditionalHandleCreate(&hc, g, 0, cudaGraphCondAssignDefault));
+    // prefix, captured into g (a linear chain)
+    MLDG_CUDA(cudaStreamBeginCaptureToGraph(h->st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    try {
+      krylov_prefix(h, A, hc);
+    } catch (...) {
+      cudaGraph_t tmp;
+      cudaStreamEndCapture(h->st, &tmp);
+      throw;
+    }
+    cudaGraph_t gout = nullptr;
+    MLDG_CUDA(cudaStreamEndCapture(h->st, &gout));
+    const int64_t lpre = h->last_launches - l0;
+    // the sink of the prefix chain
+    size_t nn = 0;
+    MLDG_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    MLDG_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+    cudaGraphNode_t sink = nullptr;
+    for (cudaGraphNode_t nd : nodes) {
+      size_t nd_out = 0;
+      MLDG_CUDA(cudaGraphNodeGetDependentNodes(nd, nullptr, &nd_out));
+      if (nd_out == 0) {
+        if (sink) fail(MLDG_ERR_INTERNAL, "solve graph: prefix is not a chain");
+        sink = nd;
+      }
+    }
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = hc;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cn;
+    MLDG_CUDA(cudaGraphAddNode(&cn, g, sink ? &sink : nullptr, sink ? 1 : 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    const int64_t l1 = h->last_launches;
+    MLDG_CUDA(cudaStreamBeginCaptureToGraph(h->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    h->eng->capturing = true;
+    try {
+      h->eng->record(trans);
+      krylov_iteration(h, A, hc);
+    } catch (...) {
+      h->eng->capturing = false;
+      cudaGraph_t tmp;
+      cudaStreamEndCapture(h->st, &tmp);
+      throw;
+    }
+    h->eng->capturing = false;
+    MLDG_CUDA(cudaStreamEndCapture(h->st, &gout));
+    const int64_t lbody = h->eng->launches + (h->last_launches - l1);
+    MLDG_CUDA(cudaGraphInstantiate(&h->sgraph[method][t], g, 0));
+    h->sglaunch_pre[method][t] = lpre;
+    h->sglaunch_body[method][t] = lbody;
+  } catch (...) {
+    h->last_launches = l0;
+    cudaGraphDestroy(g);
+    throw;
+  }
+  cudaGraphDestroy(g);
+  h->last_launches = l0;
+}
+
+// Whole solves run as one captured graph unless the handle's V-cycle is not
+// graph-captured (K-cycle, use_graphs = 0), a probe brackets a V-cycle launch
+// (event nodes cannot sit in a conditional body), or the caller passed its
+// own matrix; those run the same kernels with one host check per iteration.
+static bool solve_graphable(const Handle *h, bool own_matrix) {
+  return own_matrix && h->opts.use_graphs && !kcycle_handle(h) && h->probe_kind == 0;
 }
 
 static void krylov(Handle *h, int method, const mldg_csr *Acsr, const double *b, double *x,
@@ -3483,39 +3666,44 @@ static void krylov(Handle *h, int method, const mldg_csr *Acsr, const double *b,
   }
   const cudaMemcpyKind h2d = mem == MLDG_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   const cudaMemcpyKind d2h = mem == MLDG_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
-  double *r = h->xin, *xx = h->kx, *bb = h->kb;
-  KrylovScalars *sc = h->ksc;
+  const bool graphed = solve_graphable(h, Acsr == nullptr);
+  const int t = trans == 'N' ? 0 : 1;
+  if (graphed) capture_solve(h, method, trans, A);  // first use: capture (not timed)
   h->last_launches = 0;
+  h->hkpar->tol = tol;
+  h->hkpar->itmax = itmax;
+  h->hkpar->method = method;
   MLDG_CUDA(cudaEventRecord(h->ev0, h->st));
-  MLDG_CUDA(cudaMemcpyAsync(bb, b, sizeof(double) * n, h2d, h->st));
-  MLDG_CUDA(cudaMemcpyAsync(xx, x, sizeof(double) * n, h2d, h->st));
-  spmv64(h, A, xx, -1.0, bb, 1.0, r);  // r = b - A x
-  dots(h, n, 2, bb, bb, r, r, nullptr, nullptr);
-  MLDG_CUDA(cudaMemcpyAsync(h->hpin, sc->dots, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
-  MLDG_CUDA(cudaStreamSynchronize(h->st));
-  double bn2 = std::sqrt(h->hpin[0]);
-  if (bn2 == 0.0) bn2 = 1.0;
-  double err = std::sqrt(h->hpin[1]) / bn2;
-  int it = 0;
-  while (err > tol && it < itmax) {
-    ++it;
-    run_vcycle(h, trans);  // z = M^{-1} r (or M^{-T} r)
-    krylov_body(h, A, method, it == 1);
-    MLDG_CUDA(cudaMemcpyAsync(h->hpin, sc->dots, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  MLDG_CUDA(cudaMemcpyAsync(h->kb, b, sizeof(double) * n, h2d, h->st));
+  MLDG_CUDA(cudaMemcpyAsync(h->kx, x, sizeof(double) * n, h2d, h->st));
+  MLDG_CUDA(cudaMemcpyAsync(h->kpar, h->hkpar, sizeof(KParams), cudaMemcpyHostToDevice, h->st));
+  KState *hs = h->hkst;
+  if (graphed) {
+    MLDG_CUDA(cudaGraphLaunch(h->sgraph[method][t], h->st));
+    MLDG_CUDA(cudaMemcpyAsync(hs, h->kst, sizeof(KState), cudaMemcpyDeviceToHost, h->st));
+  } else {
+    krylov_prefix(h, A, 0);
+    MLDG_CUDA(cudaMemcpyAsync(hs, h->kst, sizeof(KState), cudaMemcpyDeviceToHost, h->st));
     MLDG_CUDA(cudaStreamSynchronize(h->st));
-    probe_collect(h);
-    err = std::sqrt(std::max(h->hpin[0], 0.0)) / bn2;
-    if (std::isnan(err)) break;
+    while (!hs->done) {
+      run_vcycle(h, trans);  // z = M^{-1} r (or M^{-T} r)
+      krylov_iteration(h, A, 0);
+      MLDG_CUDA(cudaMemcpyAsync(hs, h->kst, sizeof(KState), cudaMemcpyDeviceToHost, h->st));
+      MLDG_CUDA(cudaStreamSynchronize(h->st));
+      probe_collect(h);
+    }
   }
-  MLDG_CUDA(cudaMemcpyAsync(x, xx, sizeof(double) * n, d2h, h->st));
+  MLDG_CUDA(cudaMemcpyAsync(x, h->kx, sizeof(double) * n, d2h, h->st));
   MLDG_CUDA(cudaEventRecord(h->ev1, h->st));
   MLDG_CUDA(cudaStreamSynchronize(h->st));
+  if (graphed)
+    h->last_launches = h->sglaunch_pre[method][t] + (int64_t)hs->it * h->sglaunch_body[method][t];
   float ms = 0;
   MLDG_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
   h->last_ms = ms;
   tmp.release();
-  if (iters) *iters = it;
-  if (relres) *relres = err;
+  if (iters) *iters = hs->it;
+  if (relres) *relres = hs->err;
   check_device_error(h);
 }
 
@@ -3667,35 +3855,12 @@ static void krylov_multi(Handle *h, int method, const mldg_csr *Acsr, int nrhs, 
 
 // ---------------------------------------------------------------------------
 // Independent systems solved together: every handle keeps its own hierarchy,
-// stream and FP64 Krylov state; one CG/FCG iteration of a system (V-cycle +
-// Krylov kernels + the D2H copy of ||r||^2) is one CUDA graph captured once
-// per handle, and an iteration of the batch launches the graphs of all
-// still-active systems on their own streams so that they run concurrently.
-// Each system follows exactly the kernel sequence of krylov() (same results).
-
-static void capture_iteration(Handle *h, int method, int first) {
-  if (h->kgraph[method][first]) return;
-  cudaGraph_t g;
-  MLDG_CUDA(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
-  h->eng->capturing = true;
-  const int64_t l0 = h->last_launches;
-  try {
-    h->eng->record('N');
-    krylov_body(h, h->A0, method, first != 0);
-    MLDG_CUDA(cudaMemcpyAsync(h->hpin, h->ksc->dots, sizeof(double), cudaMemcpyDeviceToHost, h->st));
-  } catch (...) {
-    h->eng->capturing = false;
-    cudaStreamEndCapture(h->st, &g);
-    throw;
-  }
-  h->eng->capturing = false;
-  MLDG_CUDA(cudaStreamEndCapture(h->st, &g));
-  MLDG_CUDA(cudaGraphInstantiate(&h->kgraph[method][first], g, 0));
-  cudaGraphDestroy(g);
-  h->kglaunch[method][first] = h->eng->launches + (h->last_launches - l0);
-  h->last_launches = l0;
-}
-
+// stream, FP64 Krylov state and whole-solve graph (capture_solve: initial
+// residual + a device-controlled WHILE loop of V-cycle and iteration).  The
+// batch launches every system's graph on its own stream once; the systems
+// then run concurrently to their own convergence with no host involvement
+// until all have finished.  Each system runs exactly the graph mldg_krylov
+// runs for it, so the results are the same bits.
 static void krylov_batch(int nsys, Handle **hs, int method, const double *const *b, double *const *x, double tol,
                          int itmax, int *iters, double *relres, int mem, double *ms_out) {
   if (nsys < 0) fail(MLDG_ERR_ARG, "nsys < 0");
@@ -3709,7 +3874,9 @@ static void krylov_batch(int nsys, Handle **hs, int method, const double *const 
     if (!hs[i]) fail(MLDG_ERR_ARG, "system %d: null handle", i);
     if (!hs[i]->finalized) fail(MLDG_ERR_NOT_BUILT, "system %d: krylov before build", i);
     if (hs[i]->opts.device != dev) fail(MLDG_ERR_ARG, "system %d: handles on different devices", i);
-    if (kcycle_handle(hs[i])) fail(MLDG_ERR_ARG, "system %d: K-cycle iterations are not captured; use mldg_krylov", i);
+    if (!solve_graphable(hs[i], true))
+      fail(MLDG_ERR_ARG, "system %d: its solve cannot be one graph (K-cycle, use_graphs = 0 or a probe set); "
+                         "use mldg_krylov", i);
     if (!b[i] || !x[i]) fail(MLDG_ERR_ARG, "system %d: null vector", i);
     for (int k = 0; k < i; ++k)
       if (hs[k] == hs[i]) fail(MLDG_ERR_ARG, "system %d: handle repeated", i);
@@ -3722,60 +3889,26 @@ static void krylov_batch(int nsys, Handle **hs, int method, const double *const 
   MLDG_CUDA(cudaStreamCreateWithFlags(&ms, cudaStreamNonBlocking));
   MLDG_CUDA(cudaEventCreate(&e0));
   MLDG_CUDA(cudaEventCreate(&e1));
-  std::vector<double> bn(nsys, 1.0), err(nsys, 0.0);
-  std::vector<char> active(nsys, 0);
   try {
     // graphs first (capture is not timed)
     for (int i = 0; i < nsys; ++i) {
       hs[i]->last_launches = 0;
-      capture_iteration(hs[i], method, 1);
-      capture_iteration(hs[i], method, 0);
+      capture_solve(hs[i], method, 'N', hs[i]->A0);
     }
     MLDG_CUDA(cudaEventRecord(e0, ms));
     for (int i = 0; i < nsys; ++i) {
       Handle *h = hs[i];
       const int n = h->n0;
+      h->hkpar->tol = tol;
+      h->hkpar->itmax = itmax;
+      h->hkpar->method = method;
       MLDG_CUDA(cudaStreamWaitEvent(h->st, e0, 0));
       MLDG_CUDA(cudaMemcpyAsync(h->kb, b[i], sizeof(double) * n, h2d, h->st));
       MLDG_CUDA(cudaMemcpyAsync(h->kx, x[i], sizeof(double) * n, h2d, h->st));
-      spmv64(h, h->A0, h->kx, -1.0, h->kb, 1.0, h->xin);  // r = b - A x
-      dots(h, n, 2, h->kb, h->kb, h->xin, h->xin, nullptr, nullptr);
-      MLDG_CUDA(cudaMemcpyAsync(h->hpin, h->ksc->dots, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
-    }
-    for (int i = 0; i < nsys; ++i) {
-      MLDG_CUDA(cudaStreamSynchronize(hs[i]->st));
-      bn[i] = std::sqrt(hs[i]->hpin[0]);
-      if (bn[i] == 0.0) bn[i] = 1.0;
-      err[i] = std::sqrt(hs[i]->hpin[1]) / bn[i];
-      active[i] = err[i] > tol && itmax > 0;
-      iters[i] = 0;
-    }
-    int it = 0;
-    auto any = [&]() {
-      for (char a : active)
-        if (a) return true;
-      return false;
-    };
-    while (any() && it < itmax) {
-      ++it;
-      const int f = it == 1 ? 1 : 0;
-      for (int i = 0; i < nsys; ++i)
-        if (active[i]) {
-          MLDG_CUDA(cudaGraphLaunch(hs[i]->kgraph[method][f], hs[i]->st));
-          hs[i]->last_launches += hs[i]->kglaunch[method][f];
-        }
-      for (int i = 0; i < nsys; ++i)
-        if (active[i]) {
-          MLDG_CUDA(cudaStreamSynchronize(hs[i]->st));
-          err[i] = std::sqrt(std::max(hs[i]->hpin[0], 0.0)) / bn[i];
-          iters[i] = it;
-          if (!(err[i] > tol)) active[i] = 0;
-        }
-    }
-    for (int i = 0; i < nsys; ++i) {
-      Handle *h = hs[i];
-      relres[i] = err[i];
-      MLDG_CUDA(cudaMemcpyAsync(x[i], h->kx, sizeof(double) * h->n0, d2h, h->st));
+      MLDG_CUDA(cudaMemcpyAsync(h->kpar, h->hkpar, sizeof(KParams), cudaMemcpyHostToDevice, h->st));
+      MLDG_CUDA(cudaGraphLaunch(h->sgraph[method][0], h->st));
+      MLDG_CUDA(cudaMemcpyAsync(h->hkst, h->kst, sizeof(KState), cudaMemcpyDeviceToHost, h->st));
+      MLDG_CUDA(cudaMemcpyAsync(x[i], h->kx, sizeof(double) * n, d2h, h->st));
       MLDG_CUDA(cudaEventRecord(h->ev1, h->st));
       MLDG_CUDA(cudaStreamWaitEvent(ms, h->ev1, 0));
     }
@@ -3785,8 +3918,12 @@ static void krylov_batch(int nsys, Handle **hs, int method, const double *const 
     MLDG_CUDA(cudaEventElapsedTime(&t, e0, e1));
     if (ms_out) *ms_out = t;
     for (int i = 0; i < nsys; ++i) {
-      hs[i]->last_ms = t;
-      check_device_error(hs[i]);
+      Handle *h = hs[i];
+      iters[i] = h->hkst->it;
+      relres[i] = h->hkst->err;
+      h->last_ms = t;
+      h->last_launches = h->sglaunch_pre[method][0] + (int64_t)h->hkst->it * h->sglaunch_body[method][0];
+      check_device_error(h);
     }
   } catch (...) {
     cudaStreamSynchronize(ms);
@@ -4035,6 +4172,13 @@ extern "C" int mldg_apply_bytes(const mldg_handle *hp, int64_t *bytes) {
   return MLDG_SUCCESS;
 }
 
+extern "C" int mldg_apply_impl_bytes(const mldg_handle *hp, int64_t *bytes) {
+  if (!hp || !bytes) return MLDG_ERR_ARG;
+  if (!hp->h.finalized) return MLDG_ERR_NOT_BUILT;
+  *bytes = hp->h.gimpl[0];
+  return MLDG_SUCCESS;
+}
+
 extern "C" int mldg_probe_set(mldg_handle *hp, int kind, int lev, int index) {
   if (!hp) return MLDG_ERR_ARG;
   MLDG_GUARD(hp, {
@@ -4231,6 +4375,8 @@ extern "C" void mldg_destroy(mldg_handle *hp) {
   h.arena.release();
   h.karena.release();
   if (h.hpin) cudaFreeHost(h.hpin);
+  if (h.hkst) cudaFreeHost(h.hkst);
+  if (h.hkpar) cudaFreeHost(h.hkpar);
   if (h.hksc_m) cudaFreeHost(h.hksc_m);
   if (h.ev0) cudaEventDestroy(h.ev0);
   if (h.ev1) cudaEventDestroy(h.ev1);

@@ -698,36 +698,197 @@ __global__ void __launch_bounds__(kRedThreads) k_dots_final(int nblocks, const d
   }
 }
 
-// Krylov scalar state kept on the device (no host round trip per kernel).
-struct KrylovScalars {
-  double dots[3];     // scratch results of the last k_dots_final
-  double beta_num;    // (z, q_prev)
-  double dq_prev;     // (d_prev, q_prev)
-  double dq;          // (d, q)
-  double dr;          // (d, r)
-  double rr;          // (r, r)
-  double rho, rho_old;
+// ---------------------------------------------------------------------------
+// One CG/FCG iteration after the preconditioner apply z = M^{-1} r (psb_dcg /
+// psb_dfcg with istop = 2; FCG is Notay's flexible CG with truncation 1) in
+// three kernels, every scalar kept on the device:
+//   k_kry_beta   (z, q_prev) [FCG] or (r, z) [CG] -> beta
+//   k_kry_spmv   d = z + beta d_prev (d = z on the first iteration), q = A d,
+//                (d, q) and (d, r) -> alpha
+//   k_kry_update x += alpha d, r -= alpha q, ||r||^2 -> ||r|| / ||b||, and the
+//                stopping test, which also sets the CUDA-graph conditional
+//                that repeats the iteration (a whole solve is one graph launch)
+// Each kernel reduces deterministically: every block writes its partial sums,
+// and the last block to finish (a ticket counter) adds them in block order.
+// The direction lives in two buffers used alternately (d0 on even, d1 on odd
+// iterations), so q = A d reads the previous direction while the new one is
+// written.
+struct KState {
+  double bn2;           // ||b||_2 (1 when b = 0)
+  double tol;           // relative residual to reach
+  double err;           // ||r||_2 / ||b||_2 after the last iteration
+  double rr;            // ||r||_2^2
+  double beta;          // direction coefficient of the current iteration
+  double dq, dr;        // (d, A d), (d, r)
+  double dq_prev;       // (d, A d) of the previous iteration (FCG)
+  double rho, rho_old;  // (r, z) of this and the previous iteration (CG)
+  double alpha;         // step of the current iteration
+  int it;               // iterations done
+  int itmax;
+  int done;             // 1 once converged, at itmax or on a NaN residual
+  int method;           // 0 CG, 1 FCG
+  unsigned int ticket[4];
 };
 
-// FCG direction update: d = z - beta*d with beta = beta_num/dq_prev
-// (first iteration: d = z).  CG: d = z + (rho/rho_old) d.
-__global__ void k_dir_update(int n, int method, int first, const double *__restrict__ z,
-                             double *d, const KrylovScalars *sc) {
-  double beta = 0.0;
-  if (!first) beta = (method == 1) ? -(sc->beta_num / sc->dq_prev) : (sc->rho / sc->rho_old);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    d[i] = first ? z[i] : fma(beta, d[i], z[i]);
+// True in exactly one block of the grid: the last one to arrive (after every
+// block has written its partials).  The ticket is reset by that block.
+__device__ __forceinline__ bool kry_last_block(unsigned int *ticket) {
+  __shared__ int amlast;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) amlast = (atomicAdd(ticket, 1u) == gridDim.x - 1) ? 1 : 0;
+  __syncthreads();
+  if (amlast) __threadfence();
+  return amlast != 0;
+}
+// sum of partial[b*np + k] over the blocks, in a fixed order (one block)
+__device__ __forceinline__ double kry_sum_partials(const double *partial, int nb, int np, int k,
+                                                   double *sh) {
+  double s = 0;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) s += __ldcg(partial + (size_t)b * np + k);
+  return block_sum(s, sh);
 }
 
-// x += alpha d ; r -= alpha q ; alpha = num/dq, plus partial ||r||^2
-__global__ void __launch_bounds__(kRedThreads) k_xr_update(int n, int method,
-                                                          const double *__restrict__ d,
-                                                          const double *__restrict__ q,
-                                                          double *x, double *r,
-                                                          const KrylovScalars *sc,
-                                                          double *partial) {
+// Initial state after r = b - A x and the partials of (b, b), (r, r) from
+// k_dots (one block).  ps: tol / itmax / method from the host.
+struct KParams {
+  double tol;
+  int itmax;
+  int method;
+};
+__global__ void __launch_bounds__(kRedThreads) k_kry_init(int nblocks, const double *partial,
+                                                         const KParams *ps, KState *st,
+                                                         cudaGraphConditionalHandle hc) {
   __shared__ double sh[32];
-  const double alpha = (method == 1) ? sc->dr / sc->dq : sc->rho / sc->dq;
+  const double bb = kry_sum_partials(partial, nblocks, 3, 0, sh);
+  const double rr = kry_sum_partials(partial, nblocks, 3, 1, sh);
+  if (threadIdx.x == 0) {
+    double bn2 = sqrt(bb);
+    if (bn2 == 0.0) bn2 = 1.0;
+    const double err = sqrt(rr) / bn2;
+    st->bn2 = bn2;
+    st->tol = ps->tol;
+    st->itmax = ps->itmax;
+    st->method = ps->method;
+    st->err = err;
+    st->rr = rr;
+    st->it = 0;
+    st->beta = st->dq = st->dr = st->dq_prev = st->rho = st->rho_old = st->alpha = 0.0;
+    for (int k = 0; k < 4; ++k) st->ticket[k] = 0u;
+    const int done = (err > ps->tol && ps->itmax > 0) ? 0 : 1;
+    st->done = done;
+    if (hc) cudaGraphSetConditional(hc, done ? 0u : 1u);
+  }
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_kry_beta(int n, const double *__restrict__ z,
+                                                         const double *__restrict__ q,
+                                                         const double *__restrict__ r, KState *st,
+                                                         double *partial) {
+  __shared__ double sh[32];
+  if (st->done) return;
+  const int it = st->it, method = st->method;
+  double s = 0;
+  if (method == 1) {
+    if (it > 0)
+      for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        s = fma(z[i], q[i], s);
+  } else {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+      s = fma(r[i], z[i], s);
+  }
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  if (kry_last_block(&st->ticket[0])) {
+    const double t = kry_sum_partials(partial, gridDim.x, 1, 0, sh);
+    if (threadIdx.x == 0) {
+      if (method == 1) {
+        st->beta = it > 0 ? -(t / st->dq_prev) : 0.0;
+      } else {
+        st->rho_old = st->rho;
+        st->rho = t;
+        st->beta = it > 0 ? t / st->rho_old : 0.0;
+      }
+      st->ticket[0] = 0u;
+    }
+  }
+}
+
+// q = A d with d = z + beta*d_prev formed on the fly for every entry (the
+// same fma as the stored d, so both agree bit for bit); TPR lanes per row as
+// in k_spmv.  partial[2*b + {0,1}] = block sums of d_i q_i and d_i r_i.
+template <int TPR, typename CI>
+__global__ void __launch_bounds__(256) k_kry_spmv(int nr, const int *__restrict__ irp,
+                                                  const CI *__restrict__ ja,
+                                                  const double *__restrict__ val,
+                                                  const double *__restrict__ z, double *d0, double *d1,
+                                                  double *__restrict__ q, const double *__restrict__ r,
+                                                  KState *st, double *partial) {
+  __shared__ double sh[32];
+  if (st->done) return;
+  constexpr int RPW = 32 / TPR;
+  const int it = st->it;
+  const bool first = it == 0;
+  const double beta = st->beta;
+  const double *dold = (it & 1) ? d0 : d1;
+  double *dnew = (it & 1) ? d1 : d0;
+  const int lane = threadIdx.x & 31;
+  const int sub = lane % TPR;
+  const int grp = lane / TPR;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  double sdq = 0, sdr = 0;
+  for (int r0 = warp * RPW; r0 < nr; r0 += nwarps * RPW) {
+    const int row = r0 + grp;
+    double s = 0;
+    if (row < nr) {
+      const int e = irp[row + 1];
+      if (first) {
+        for (int k = irp[row] + sub; k < e; k += TPR) s = fma(val[k], __ldg(z + colof(ja, k, row)), s);
+      } else {
+        for (int k = irp[row] + sub; k < e; k += TPR) {
+          const int j = colof(ja, k, row);
+          s = fma(val[k], fma(beta, dold[j], __ldg(z + j)), s);
+        }
+      }
+    }
+#pragma unroll
+    for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, TPR);
+    if (row < nr && sub == 0) {
+      const double di = first ? z[row] : fma(beta, dold[row], z[row]);
+      dnew[row] = di;
+      q[row] = s;
+      sdq = fma(di, s, sdq);
+      sdr = fma(di, r[row], sdr);
+    }
+  }
+  sdq = block_sum(sdq, sh);
+  sdr = block_sum(sdr, sh);
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = sdq;
+    partial[2 * blockIdx.x + 1] = sdr;
+  }
+  if (kry_last_block(&st->ticket[1])) {
+    const double dq = kry_sum_partials(partial, gridDim.x, 2, 0, sh);
+    const double dr = kry_sum_partials(partial, gridDim.x, 2, 1, sh);
+    if (threadIdx.x == 0) {
+      st->dq = dq;
+      st->dr = dr;
+      st->alpha = (st->method == 1) ? dr / dq : st->rho / dq;
+      st->ticket[1] = 0u;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_kry_update(int n, const double *d0, const double *d1,
+                                                           const double *__restrict__ q, double *x,
+                                                           double *r, KState *st, double *partial,
+                                                           cudaGraphConditionalHandle hc) {
+  __shared__ double sh[32];
+  if (st->done) return;
+  const int it = st->it;
+  const double *__restrict__ d = (it & 1) ? d1 : d0;
+  const double alpha = st->alpha;
   double s = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     x[i] = fma(alpha, d[i], x[i]);
@@ -736,30 +897,20 @@ __global__ void __launch_bounds__(kRedThreads) k_xr_update(int n, int method,
     s = fma(ri, ri, s);
   }
   s = block_sum(s, sh);
-  if (threadIdx.x == 0) {
-    partial[blockIdx.x * 3 + 0] = s;
-    partial[blockIdx.x * 3 + 1] = 0;
-    partial[blockIdx.x * 3 + 2] = 0;
-  }
-}
-
-// copy reduction results into named scalar slots
-__global__ void k_scal_store(KrylovScalars *sc, int what) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  switch (what) {
-    case 0:  // after (z,q_prev) [FCG] or (r,z) [CG]
-      sc->beta_num = sc->dots[0];
-      sc->rho_old = sc->rho;
-      sc->rho = sc->dots[0];
-      break;
-    case 1:  // after (d,q),(d,r)
-      sc->dq = sc->dots[0];
-      sc->dr = sc->dots[1];
-      break;
-    case 2:  // after ||r||^2
-      sc->rr = sc->dots[0];
-      sc->dq_prev = sc->dq;
-      break;
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  if (kry_last_block(&st->ticket[2])) {
+    const double rr = kry_sum_partials(partial, gridDim.x, 1, 0, sh);
+    if (threadIdx.x == 0) {
+      const double err = sqrt(rr < 0.0 ? 0.0 : rr) / st->bn2;  // NaN stays NaN
+      st->rr = rr;
+      st->err = err;
+      st->it = it + 1;
+      st->dq_prev = st->dq;
+      const int done = (err > st->tol && it + 1 < st->itmax) ? 0 : 1;
+      st->done = done;
+      st->ticket[2] = 0u;
+      if (hc) cudaGraphSetConditional(hc, done ? 0u : 1u);
+    }
   }
 }
 

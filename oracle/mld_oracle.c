@@ -218,12 +218,25 @@ static void spmv_op(const csr *a, char trans, double alpha, const double *x,
 }
 
 static void axpby(int n, double a, const double *x, double b, double *y) {
+#pragma omp parallel for schedule(static) if (n > 20000)
   for (int i = 0; i < n; i++) y[i] = (b == 0.0) ? a * x[i] : a * x[i] + b * y[i];
 }
 
+/* Dot product summed in ORC_DOT_CHUNKS fixed chunks (each from zero in index
+ * order), the chunk sums then added in chunk order: the same result for any
+ * number of threads. */
+#define ORC_DOT_CHUNKS 64
 static double dot(int n, const double *x, const double *y) {
+  double part[ORC_DOT_CHUNKS];
+#pragma omp parallel for schedule(static) if (n > 20000)
+  for (int c = 0; c < ORC_DOT_CHUNKS; c++) {
+    const int lo = (int)((long)n * c / ORC_DOT_CHUNKS), hi = (int)((long)n * (c + 1) / ORC_DOT_CHUNKS);
+    double s = 0.0;
+    for (int i = lo; i < hi; i++) s = s + x[i] * y[i];
+    part[c] = s;
+  }
   double s = 0.0;
-  for (int i = 0; i < n; i++) s = s + x[i] * y[i];
+  for (int c = 0; c < ORC_DOT_CHUNKS; c++) s = s + part[c];
   return s;
 }
 
@@ -545,6 +558,7 @@ static void ilu_apply(const level *lv, char trans, double alpha, const double *x
 static void diag_apply(const level *lv, double alpha, const double *x,
                        double beta, double *y) {
   int n = lv->A.nr;
+#pragma omp parallel for schedule(static) if (n > 20000)
   for (int i = 0; i < n; i++)
     y[i] = (beta == 0.0) ? alpha * (lv->dinv[i] * x[i])
                          : alpha * (lv->dinv[i] * x[i]) + beta * y[i];
@@ -1153,11 +1167,13 @@ int orc_krylov(int method, int n, const int *irp, const int *ja,
         memcpy(d, z, sizeof(double) * (size_t)n);
       else {
         double beta = rho / rho_old;
+#pragma omp parallel for schedule(static) if (n > 20000)
         for (int i = 0; i < n; i++) d[i] = z[i] + beta * d[i];
       }
       orc_spmv(n, irp, ja, val, 1.0, d, 0.0, q);
       double sigma = dot(n, d, q);
       double alpha = rho / sigma;
+#pragma omp parallel for schedule(static) if (n > 20000)
       for (int i = 0; i < n; i++) {
         x[i] = x[i] + alpha * d[i];
         r[i] = r[i] - alpha * q[i];
@@ -1167,11 +1183,13 @@ int orc_krylov(int method, int n, const int *irp, const int *ja,
         memcpy(d, z, sizeof(double) * (size_t)n);
       } else {
         double beta = dot(n, z, q) / dq_prev; /* (z, A d_prev)/(d_prev, A d_prev) */
+#pragma omp parallel for schedule(static) if (n > 20000)
         for (int i = 0; i < n; i++) d[i] = z[i] - beta * d[i];
       }
       orc_spmv(n, irp, ja, val, 1.0, d, 0.0, q);
       double dq = dot(n, d, q);
       double alpha = dot(n, d, r) / dq;
+#pragma omp parallel for schedule(static) if (n > 20000)
       for (int i = 0; i < n; i++) {
         x[i] = x[i] + alpha * d[i];
         r[i] = r[i] - alpha * q[i];

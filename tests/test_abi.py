@@ -95,3 +95,41 @@ def test_krylov_batch_rejects_mismatched_lists(mld):
         mld.krylov_batch("FCG", [object(), object()], [np.ones(4)])
     with pytest.raises(ValueError):
         mld.krylov_batch("FCG", [object()], [np.ones(4)], [np.ones(4), np.ones(4)])
+
+
+def test_header_compiles_as_c99_and_links(mld, tmp_path):
+    """include/mldg.h as a C caller sees it: a C99 program that includes the
+    header, links libmldgpu.so and checks the host-side error paths (null
+    handle, error text), with no GPU."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    mld.lib()  # built
+    src = tmp_path / "abi_c99.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include <string.h>
+#include "mldg.h"
+int main(void) {
+  mldg_level_desc d;
+  memset(&d, 0, sizeof d);
+  if (mldg_upload_level(NULL, 0, &d) != MLDG_ERR_ARG) return 1;
+  if (mldg_finalize(NULL, 1, MLDG_PREC_FP64) != MLDG_ERR_ARG) return 2;
+  if (mldg_apply(NULL, NULL, NULL, 'N', 1, 0, MLDG_MEM_HOST) != MLDG_ERR_ARG) return 3;
+  if (mldg_krylov(NULL, 1, NULL, NULL, NULL, 1e-10, 10, NULL, NULL, MLDG_MEM_HOST) != MLDG_ERR_ARG) return 4;
+  if (strcmp(mldg_last_error(NULL), "null handle") != 0) return 5;
+  mldg_destroy(NULL);
+  puts("c99 ok");
+  return 0;
+}
+''')
+    exe = tmp_path / "abi_c99"
+    libdir = os.path.join(ROOT, "mld2p4-2_b200")
+    r = subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I",
+                        os.path.join(ROOT, "include"), str(src), "-o", str(exe), "-L", libdir,
+                        "-lmldgpu", f"-Wl,-rpath,{libdir}"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and "c99 ok" in r.stdout, (r.returncode, r.stdout, r.stderr)

@@ -1,9 +1,10 @@
 """Batching of independent systems: several hierarchies solved together.
 
-mldg_krylov_batch runs one captured CG/FCG iteration graph per system and
-launches the graphs of all unconverged systems concurrently.  Every system
-follows exactly the kernel sequence of its own mldg_krylov, so iterations
-and solutions must be identical to solving the systems one by one.
+mldg_krylov_batch launches every system's whole-solve graph (initial
+residual, then a device-controlled loop of V-cycle and CG/FCG iteration) on
+the system's own stream, once; the systems run concurrently to their own
+convergence.  Every system runs exactly the graph of its own mldg_krylov, so
+iterations and solutions must be identical to solving the systems one by one.
 """
 import numpy as np
 import pytest

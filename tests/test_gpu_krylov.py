@@ -47,3 +47,42 @@ def test_fp32_vcycle_inside_fp64_fcg(mld, orc):
     assert rr <= 1e-10
     assert it <= it_ref + 2
     assert np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref) < 1e-8
+
+
+@pytest.mark.parametrize("method", ["CG", "FCG"])
+def test_graph_solve_equals_host_stepped_solve(mld, orc, method):
+    """A solve without a probe is one graph launch (device-side stopping
+    test in a conditional WHILE node); with a probe set, the same kernels run
+    with one host check per iteration.  Both must give the same bits."""
+    a = orc.gen_pde3d(20, 1, ISO)
+    op = orc.Prec(oracle_params(orc, "JACOBI", 2, 0.8, mcs=300))
+    op.build(a)
+    b = np.random.default_rng(5).uniform(-1, 1, a.nrows)
+    h = upload_oracle_hierarchy(mld, orc, op)
+    x1, it1, r1 = h.krylov(method, b.copy(), eps=1e-10)
+    _, nl1 = h.last_timing()
+    h.probe_set(mld.KERNEL_SPMV, 0, 0)  # forces the host-stepped loop
+    x2, it2, r2 = h.krylov(method, b.copy(), eps=1e-10)
+    h.probe_set(0, 0, 0)
+    x3, it3, r3 = h.krylov(method, b.copy(), eps=1e-10)  # graph again
+    assert it1 == it2 == it3 and r1 == r2 == r3
+    assert np.array_equal(x1, x2) and np.array_equal(x1, x3)
+    assert r1 <= 1e-10 and nl1 > it1
+
+
+def test_itmax_and_zero_rhs(mld, orc):
+    """itmax stops the device loop exactly; a zero right-hand side or an
+    exact initial guess stops before the first iteration."""
+    a = orc.gen_pde3d(12, 1, ISO)
+    op = orc.Prec(oracle_params(orc, "BJAC", mcs=200))
+    op.build(a)
+    h = upload_oracle_hierarchy(mld, orc, op)
+    b = orc.spmv(a, np.ones(a.nrows))
+    _, it, rr = h.krylov("FCG", b.copy(), eps=1e-14, itmax=3)
+    _, it_ref, rr_ref, _ = orc.krylov("FCG", a, op, b, eps=1e-14, itmax=3)
+    assert it == 3 and it_ref == 3 and rr > 1e-14
+    assert abs(rr - rr_ref) <= 1e-6 * rr_ref
+    x, it, rr = h.krylov("FCG", np.zeros(a.nrows), eps=1e-10)
+    assert it == 0 and np.all(x == 0)
+    x, it, rr = h.krylov("FCG", b.copy(), x=np.ones(a.nrows), eps=1e-10)
+    assert it == 0 and rr <= 1e-10

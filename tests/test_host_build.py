@@ -50,19 +50,32 @@ def test_hierarchy_identical(mld, orc, idim, coef, smoother, mcs):
             assert np.array_equal(mo.val, mp.val), (l, w)
 
 
-@pytest.mark.parametrize("smoother", ["BJAC", "JACOBI"])
-def test_smoother_data_identical(mld, orc, smoother):
-    idim = 14
-    ao = orc.gen_pde3d(idim, 1, ISO)
-    sm = orc.BJAC if smoother == "BJAC" else orc.JACOBI
+@pytest.mark.parametrize("idim,coef,smoother,mcs", [(14, ISO, "BJAC", 150), (16, ANISO, "BJAC", 200),
+                                                    (14, ISO, "JACOBI", 150), (12, ISO, "FBGS", 100)])
+def test_smoother_data_identical(mld, orc, idim, coef, smoother, mcs):
+    """The smoother/solver data of every level -- ILU(0) factors L, U and
+    pivots (mld_dilu0_fact.f90), the Jacobi off-diagonal part and inverse
+    diagonal, the GS split -- bit for bit between the product's host build
+    and the oracle."""
+    ao = orc.gen_pde3d(idim, 1, coef)
+    sm = {"BJAC": orc.BJAC, "JACOBI": orc.JACOBI, "FBGS": orc.FBGS}[smoother]
     op = orc.Prec(orc.default_params(smoother=sm, coarse_solver=orc.BJAC, coarse_sweeps=4,
-                                     min_coarse_size=150))
+                                     min_coarse_size=mcs))
     op.build(ao)
-    pp = _product(mld, mld.gen_pde3d(idim, 1, ISO), smoother, 150)
-    # smoothers_build needs no GPU up to the upload; compare through the
-    # oracle-side factorisation of the product's level matrices instead
+    pp = _product(mld, mld.gen_pde3d(idim, 1, coef), smoother, mcs)
+    pp.smoothers_build_host()
+    assert pp.nlev == op.nlev
+    compared = 0
     for l in range(op.nlev):
         io = op.level_info(l)
-        if io["smoother"] == orc.BJAC:
-            from mld2p4_2_b200 import CSR  # noqa: F401  (package loaded by fixture)
-        assert io["n"] == pp.level_info(l)["n"]
+        names = {orc.BJAC: ["L", "U"], orc.FBGS: ["L", "U"], orc.JACOBI: ["ND"]}[io["smoother"]]
+        for w in names:
+            mo, mp = op.level_csr(l, w), pp.level_csr(l, w)
+            assert mo is not None and mp is not None, (l, w)
+            assert np.array_equal(mo.irp, mp.irp), (l, w)
+            assert np.array_equal(mo.ja, mp.ja), (l, w)
+            assert np.array_equal(mo.val, mp.val), (l, w)
+            compared += mo.nnz
+        vo = op.level_vec(l, "dinv" if io["smoother"] == orc.JACOBI else "d")
+        assert np.array_equal(vo, pp.level_vec(l, "d")), l
+    assert compared > 0

@@ -1,9 +1,9 @@
 """GPU: the allocation-free relative residual (mldg_relres_noalloc).
 
-Some callers cannot allocate device memory -- code running while a CUDA
-graph is being captured, applications whose own memory pool owns every
-device byte, tight convergence loops where cudaMalloc/cudaFree would
-synchronise the device.  For them the library computes ||b - A x|| / ||b||
+Some callers cannot allocate device memory: applications whose own memory
+pool or allocator owns every device byte, and tight host-side convergence
+loops where each cudaMalloc/cudaFree would synchronise the whole device.
+For them the library computes ||b - A x|| / ||b||
 with its scratch in a fixed file-scope device array instead of memory it
 allocates.  This test calls that entry point through the C ABI twice in a
 row and checks each result against the regular path (mldg_krylov with
