@@ -1,13 +1,14 @@
 /*
- * mldg_test.h -- host-only test hook of libmldgpu.so.
+ * mldg_test.h -- test hooks of libmldgpu.so (no counterparts in the reference).
  *
- * No counterpart in the reference: it checks the plans of the replicated-
- * window cluster solve (the kernel that runs the large ILU(0) levels) without
- * a GPU.  It builds the plans of an ILU(0) pair exactly as mldg_finalize
- * would and replays them through a host emulation of the kernel, in the
- * kernel's step order, checking every ring read against the position its
- * slot holds, every far read and reset, and every plan block against its
- * descriptor.
+ * mldg_rep_plan_check checks the plans of the replicated-window cluster
+ * solve (the kernel that runs the large ILU(0) levels) without a GPU: it
+ * builds the plans of an ILU(0) pair exactly as mldg_finalize would and
+ * replays them through a host emulation of the kernel, in the kernel's step
+ * order, checking every ring read against the position its slot holds, every
+ * far read and reset, and every plan block against its descriptor.
+ * mldg_test_set_spin_limit makes dependency waits run out on purpose
+ * (failure detection without a GPU fault).
  */
 #ifndef MLDG_TEST_H
 #define MLDG_TEST_H
@@ -26,6 +27,16 @@ extern "C" {
  * y untouched).  Returns MLDG_SUCCESS or MLDG_ERR_ARG. */
 int mldg_rep_plan_check(const mldg_csr *L, const mldg_csr *U, const double *d, const double *x,
                         double *y, int cluster, int fp32, char trans, long long *stats);
+
+/* Polls a sentinel wait of the sync-free and ELL triangular solves makes
+ * before it gives up with MLDG_ERR_TIMEOUT, on `device`; polls < 0 restores
+ * the default (2^22).  A test lowers it (0: give up at the first poll that
+ * finds a dependency not yet written) to make a solve's waits run out on
+ * purpose, then checks that the call returns MLDG_ERR_TIMEOUT, that the
+ * kernel ends, and that the next apply on the same handle is correct.  The
+ * mbarrier waits of the window and cluster solves keep their own limit.
+ * Returns MLDG_SUCCESS or MLDG_ERR_CUDA. */
+int mldg_test_set_spin_limit(int device, int polls);
 
 #ifdef __cplusplus
 }

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <map>
@@ -32,6 +33,7 @@
 #include "mldg_tri.h"
 #include "mldg_trsv_win.cuh"
 #include "mldg_trsv_rep.cuh"
+#include "mldg_trsv_blk.cuh"
 
 namespace mldg {
 
@@ -176,8 +178,25 @@ struct DCSR {
   short *jd = nullptr;  // int16 column offsets from the row (square, |j - i| <= 32767), or null
   T *val = nullptr;
   int tpr = 1;
+  // sliced-ELL copy (SELL-32, see k_spmv_sell): slice offsets, values and
+  // column indices (int16 offsets from the row when jd is set, else int32),
+  // built when the padding stays small; used when the autotuner finds it faster
+  int *soff = nullptr;
+  T *sval = nullptr;
+  short *sjd = nullptr;
+  int *sja = nullptr;
+  int64_t slots = 0;
+  bool sell = false;
   bool present() const { return irp != nullptr; }
   int64_t idx_bytes() const { return jd ? 2 : 4; }
+  int nslice() const { return (nr + 31) / 32; }
+  // bytes of the matrix as the chosen kernel reads it
+  int64_t mat_bytes() const {
+    return sell ? slots * (int64_t)(sizeof(T) + idx_bytes()) + 4 * ((int64_t)nslice() + 1)
+                : nnz * (int64_t)(sizeof(T) + idx_bytes()) + 4 * ((int64_t)nr + 1);
+  }
+  // algorithmic CSR bytes nnz*(value + index) + 4*(rows + 1)
+  int64_t alg_bytes() const { return nnz * (int64_t)(sizeof(T) + idx_bytes()) + 4 * ((int64_t)nr + 1); }
 };
 
 template <typename T>
@@ -262,6 +281,19 @@ struct DRep {
 };
 constexpr int kRepTPR = 4;
 
+// Plan of the partitioned solve (k_trsv_blk) for one triangular factor.
+template <typename T>
+struct DBlk {
+  bool ok = false;
+  int n = 0, nblocks = 0, nsteps = 0, W = 0, stage_bytes = 0;
+  size_t smem = 0;
+  int64_t nnz = 0, plan_bytes = 0;
+  int *bstep = nullptr;
+  int2 *sdesc = nullptr;
+  uint4 *plan = nullptr;
+  int *ticket = nullptr;
+};
+
 static int pick_tpr(int64_t nnz, int nr) {
   const double avg = nr > 0 ? (double)nnz / nr : 0.0;
   if (avg <= 8) return 1;
@@ -270,6 +302,55 @@ static int pick_tpr(int64_t nnz, int nr) {
   if (avg <= 64) return 8;
   if (avg <= 128) return 16;
   return 32;
+}
+
+// The SELL-32 copy of a CSR matrix (k_spmv_sell): skipped when padding would
+// add more than a quarter of the entries, or with MLDG_NO_SELL.  Padding
+// slots hold a zero value on an in-range column (the row itself, or the last
+// row for the rows past the end of the last slice).
+template <typename T>
+static void build_sell(Arena &ar, const HostCSR &h, DCSR<T> &d) {
+  if (std::getenv("MLDG_NO_SELL") || h.nr == 0 || h.nnz() == 0) return;
+  const int ns = (h.nr + 31) / 32;
+  std::vector<int> soff((size_t)ns + 1, 0);
+  for (int s = 0; s < ns; ++s) {
+    int w = 0;
+    for (int i = s * 32; i < std::min(h.nr, s * 32 + 32); ++i) w = std::max(w, h.irp[i + 1] - h.irp[i]);
+    const int64_t next = (int64_t)soff[s] + 32 * (int64_t)w;
+    if (next > INT32_MAX) return;
+    soff[s + 1] = (int)next;
+  }
+  const int64_t slots = soff[ns];
+  if (slots * 4 > h.nnz() * 5) return;
+  std::vector<T> sv((size_t)slots, T(0));
+  const bool rel = d.jd != nullptr;
+  std::vector<short> sjd(rel ? (size_t)slots : 0);
+  std::vector<int> sja(rel ? 0 : (size_t)slots);
+#pragma omp parallel for schedule(static, 256)
+  for (int s = 0; s < ns; ++s) {
+    const int w = (soff[s + 1] - soff[s]) / 32;
+    for (int lane = 0; lane < 32; ++lane) {
+      const int i = s * 32 + lane;
+      const int len = i < h.nr ? h.irp[i + 1] - h.irp[i] : 0;
+      const int pad_col = i < h.nr ? (h.nr == h.nc ? i : 0) : (h.nr == h.nc ? h.nr - 1 : 0);
+      for (int k = 0; k < w; ++k) {
+        const size_t e = (size_t)soff[s] + 32 * (size_t)k + lane;
+        const int col = k < len ? h.ja[h.irp[i] + k] : pad_col;
+        if (k < len) sv[e] = (T)h.val[h.irp[i] + k];
+        if (rel)
+          sjd[e] = (short)(col - i);
+        else
+          sja[e] = col;
+      }
+    }
+  }
+  d.soff = ar.upload(soff);
+  d.sval = ar.upload(sv);
+  if (rel)
+    d.sjd = ar.upload(sjd);
+  else
+    d.sja = ar.upload(sja);
+  d.slots = slots;
 }
 
 template <typename T>
@@ -297,6 +378,7 @@ static DCSR<T> to_dev(Arena &ar, const HostCSR &h) {
   std::vector<T> v(h.val.begin(), h.val.end());
   d.val = ar.upload(v);
   d.tpr = pick_tpr(d.nnz, d.nr);
+  build_sell(ar, h, d);
   return d;
 }
 
@@ -364,6 +446,10 @@ struct Engine {
   double *xin_m = nullptr, *yout_m = nullptr, *col_m = nullptr;
   int mcap = 0;
   virtual void dump_trace() {}
+  // After a solve gave up on a dependency wait: put every exchange buffer
+  // back to the sentinel and every ticket counter back to zero, as finalize
+  // left them, so that the next apply on the handle starts clean.
+  virtual void reset_solve_state() = 0;
   int64_t launches = 0;
   // bytes: algorithmic bytes of the recorded launches (each sparse operand of
   // the reference's operation once, each dense vector operand once);
@@ -537,6 +623,10 @@ struct EngineT : Engine {
     // ILU(0) levels, used (rep) when the autotuner finds them fastest
     bool rep = false, rep_ok = false;
     DRep<T> rL, rU, rUt, rLt;
+    // partitioned solves (k_trsv_blk): built (blk_ok) on ILU(0) levels, used
+    // (blk) when the autotuner finds them fastest
+    bool blk = false, blk_ok = false;
+    DBlk<T> kL, kU, kUt, kLt;
     // coarsest level: explicit inverse of its ILU(0) factorisation (and its transpose)
     T *minv = nullptr, *minvT = nullptr;
     T *rp0 = nullptr, *rp1 = nullptr;  // right-hand sides in position order
@@ -556,6 +646,17 @@ struct EngineT : Engine {
     return (int)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)nsm * 16));
   }
   void spmv(const DCSR<T> &A, const T *v, T a1, const T *b, T a0, T *out, T a2) {
+    const int64_t vec = (int64_t)A.nc * sizeof(T) + (int64_t)A.nr * sizeof(T) * (1 + (b ? 1 : 0) + (a2 != T(0) ? 1 : 0));
+    if (A.sell) {
+      begin(MLDG_KERNEL_SPMV);
+      const int g = blocks_for((int64_t)A.nslice() * 32);
+      if (A.sjd)
+        k_spmv_sell<T, short><<<g, 256, 0, st>>>(A.nr, A.soff, A.sjd, A.sval, v, a1, b, a0, out, a2);
+      else
+        k_spmv_sell<T, int><<<g, 256, 0, st>>>(A.nr, A.soff, A.sja, A.sval, v, a1, b, a0, out, a2);
+      end(A.mat_bytes() + vec, A.alg_bytes() + vec);
+      return;
+    }
     const int g = blocks_for((int64_t)A.nr * A.tpr);
     begin(MLDG_KERNEL_SPMV);
     switch (A.tpr) {
@@ -575,6 +676,19 @@ struct EngineT : Engine {
   }
   void jacobi(const DCSR<T> &ND, const T *d, const T *x, const T *ty, int first, T omega,
               T alpha, T beta, T *out) {
+    if (ND.sell) {
+      const int64_t vec = (int64_t)ND.nr * sizeof(T) * (3 + (first ? 0 : 1) + (beta != T(0) ? 1 : 0));
+      begin(MLDG_KERNEL_JACOBI);
+      const int g = blocks_for((int64_t)ND.nslice() * 32);
+      if (ND.sjd)
+        k_jacobi_sell<T, short><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sjd, ND.sval, d, x, ty, first, omega,
+                                                   alpha, beta, out);
+      else
+        k_jacobi_sell<T, int><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sja, ND.sval, d, x, ty, first, omega,
+                                                 alpha, beta, out);
+      end(ND.mat_bytes() + vec, ND.alg_bytes() + vec);
+      return;
+    }
     const int g = blocks_for((int64_t)ND.nr * ND.tpr);
     begin(MLDG_KERNEL_JACOBI);
     switch (ND.tpr) {
@@ -660,12 +774,15 @@ struct EngineT : Engine {
           ilu_apply(L, 'N', L.x, T(0), L.ty);
         }
       };
-      // variants: 0 the level's other solve, 1 ELL, 2 replicated-window cluster solve
-      float best[3] = {1e30f, 1e30f, 1e30f};
-      for (int v = 0; v < 3; ++v) {
+      // variants: 0 the level's other solve, 1 ELL, 2 replicated-window cluster
+      // solve, 3 partitioned solve
+      float best[4] = {1e30f, 1e30f, 1e30f, 1e30f};
+      for (int v = 0; v < 4; ++v) {
         if (v == 2 && (gs || !L.rep_ok)) continue;
+        if (v == 3 && (gs || !L.blk_ok)) continue;
         L.ell1 = v == 1;
         L.rep = v == 2;
+        L.blk = v == 3;
         op();  // warm
         MLDG_CUDA(cudaEventRecord(e0, st));
         for (int r = 0; r < reps; ++r) op();
@@ -674,14 +791,15 @@ struct EngineT : Engine {
         MLDG_CUDA(cudaEventElapsedTime(&best[v], e0, e1));
       }
       int pick = 0;
-      for (int v = 1; v < 3; ++v)
+      for (int v = 1; v < 4; ++v)
         if (best[v] < best[pick]) pick = v;
       L.ell1 = pick == 1;
       L.rep = pick == 2;
+      L.blk = pick == 3;
       if (std::getenv("MLDG_VERBOSE"))
-        std::fprintf(stderr, "mldg: ilu autotune n=%d other %.3f ms ell %.3f ms rep %.3f ms -> %s\n", L.n,
-                     best[0] / reps, best[1] / reps, best[2] / reps,
-                     L.rep ? "rep" : (L.ell1 ? "ell" : "other"));
+        std::fprintf(stderr, "mldg: ilu autotune n=%d other %.3f ms ell %.3f ms rep %.3f ms blk %.3f ms -> %s\n",
+                     L.n, best[0] / reps, best[1] / reps, best[2] / reps, best[3] / reps,
+                     L.blk ? "blk" : (L.rep ? "rep" : (L.ell1 ? "ell" : "other")));
     }
     launches = 0;
     bytes = 0;
@@ -769,6 +887,32 @@ struct EngineT : Engine {
     }
   }
 
+  // one partitioned solve: cur = T^{-1}(scale o rhs); other reset; out = alpha*t + beta*out
+  void bsolve(const DBlk<T> &w, const T *rhs, const T *scale, T *cur, T *other, T *out, T alpha, T beta) {
+    BlkArgs<T> a;
+    a.nblocks = w.nblocks;
+    a.wmask = w.W - 1;
+    a.stage_bytes = w.stage_bytes;
+    a.bstep = w.bstep;
+    a.sdesc = w.sdesc;
+    a.plan = w.plan;
+    a.src = rhs;
+    a.scale = scale;
+    a.cur = cur;
+    a.other = other;
+    a.out = out;
+    a.alpha = alpha;
+    a.beta = beta;
+    a.ticket = w.ticket;
+    a.err = err;
+    begin(MLDG_KERNEL_TRSV);
+    launch_blk(w, a, st);
+    const int64_t vec = (int64_t)w.n * sizeof(T) *
+                        (1 + (scale ? 1 : 0) + 1 + (other ? 1 : 0) + (out ? 1 + (beta != T(0)) : 0));
+    end(w.plan_bytes + 4 * ((int64_t)w.nsteps + 1) + vec,
+        w.nnz * (int64_t)(sizeof(T) + 4) + 4 * ((int64_t)w.n + 1) + vec);
+  }
+
   // ILU solver apply: y = alpha*U^{-1}(d o L^{-1} x) + beta*y, or the 'T' form
   void ilu_apply(Lev &L, char trans, const T *x, T beta, T *y) {
     if (L.minv) {
@@ -779,6 +923,16 @@ struct EngineT : Engine {
       end((int64_t)L.n * L.n * sizeof(T) + (int64_t)L.n * sizeof(T) * (2 + (beta != T(0))),
           (L.nnz_l + L.nnz_u) * (int64_t)(sizeof(T) + 4) + 8 * ((int64_t)L.n + 1) +
               (int64_t)L.n * sizeof(T) * (3 + (beta != T(0))));
+      return;
+    }
+    if (L.blk) {
+      if (trans == 'N') {
+        bsolve(L.kL, x, nullptr, L.bufA, L.bufB, nullptr, T(1), T(0));
+        bsolve(L.kU, L.bufA, L.d, L.bufB, L.bufA, y, T(1), beta);
+      } else {
+        bsolve(L.kUt, x, nullptr, L.bufA, L.bufB, nullptr, T(1), T(0));
+        bsolve(L.kLt, L.bufA, L.d, L.bufB, L.bufA, y, T(1), beta);
+      }
       return;
     }
     if (L.ell1) {
@@ -840,6 +994,31 @@ struct EngineT : Engine {
     else
       trsv(t, rhs, L.d, cur, other, out, T(1), beta);
   }
+  void reset_solve_state() override {
+    const T sent = Sentinel<T>::value();
+    auto refill = [&](T *b, int64_t cnt) {
+      if (b && cnt > 0) k_fill<T><<<blocks_for(cnt), 256, 0, st>>>((int)cnt, sent, b);
+    };
+    for (auto &L : lv) {
+      const int n = std::max(L.n, 1);
+      refill(L.bufA, n);
+      refill(L.bufB, n);
+      refill(L.bufAm, (int64_t)n * mcap);
+      refill(L.bufBm, (int64_t)n * mcap);
+      for (DTri<T> *f : {&L.L, &L.U, &L.Ut, &L.Lt}) {
+        if (f->counters) MLDG_CUDA(cudaMemsetAsync(f->counters, 0, 2 * sizeof(int), st));
+        for (auto &el : f->ell)
+          if (el.ok && el.ctr) MLDG_CUDA(cudaMemsetAsync(el.ctr, 0, sizeof(int) * 32 * (el.S + 1), st));
+      }
+      for (DRep<T> *r : {&L.rL, &L.rU, &L.rUt, &L.rLt}) refill(r->xp, (int64_t)r->n + 8);
+      for (DBlk<T> *k : {&L.kL, &L.kU, &L.kUt, &L.kLt})
+        if (k->ticket) MLDG_CUDA(cudaMemsetAsync(k->ticket, 0, 2 * sizeof(int), st));
+      L.gflip = 0;
+      L.gflip_m = 0;
+    }
+    MLDG_CUDA(cudaStreamSynchronize(st));
+  }
+
   void end_fbgs() {
     for (auto &L : lv)
       if (L.kind == MLDG_SMOOTHER_FBGS && L.gflip) {
@@ -1099,8 +1278,12 @@ struct EngineT : Engine {
         T *v = scratch_for(nmax, 0), *o = scratch_for(nmax, 1);
         float best = 1e30f;
         int best_t = op->tpr;
-        for (int t : {1, 2, 4, 8, 16, 32}) {
-          op->tpr = t;
+        bool best_sell = false;
+        // candidates: CSR with 1..32 lanes per row, then the SELL copy (t = 0)
+        for (int t : {1, 2, 4, 8, 16, 32, 0}) {
+          if (t == 0 && !op->soff) continue;
+          op->sell = t == 0;
+          if (t) op->tpr = t;
           spmv(*op, v, T(1), nullptr, T(0), o, T(0));  // warm
           MLDG_CUDA(cudaEventRecord(e0, st));
           for (int r = 0; r < reps; ++r) spmv(*op, v, T(1), nullptr, T(0), o, T(0));
@@ -1110,10 +1293,12 @@ struct EngineT : Engine {
           MLDG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
           if (ms < best) {
             best = ms;
-            best_t = t;
+            best_t = t ? t : best_t;
+            best_sell = t == 0;
           }
         }
         op->tpr = best_t;
+        op->sell = best_sell;
       }
     }
     launches = 0;
@@ -1925,6 +2110,9 @@ void EngineT<float>::prolong(Lev &C, float *y) {
 // ---------------------------------------------------------------------------
 struct Handle {
   mldg_opts opts{};
+  // changes at every finalize and destroy: identifies the finalized state
+  // that a cached batch graph was captured from
+  uint64_t serial = 0;
   int cycle = MLDG_CYCLE_V;
   bool has_fbgs = false;  // a Gauss-Seidel level: trans 'T' is rejected
   std::string last_error;
@@ -2753,6 +2941,163 @@ static void rep_check_pair(const HostCSR &Lf, bool lupper, const HostCSR &Uf, bo
   stats[3] = 1;
 }
 
+// ---- partitioned solve (k_trsv_blk): plan and launch ----
+// The factor in lower form (an upper factor with rows and columns reversed)
+// is cut into P contiguous blocks of about equal rows + entries.  A block's
+// rows are ordered by (global dependency level, row) and grouped into steps
+// of one level each, split where a step's plan would exceed kBlkStageCap
+// bytes.  A dependency on a row of the same block whose ring slot is still
+// intact at the end of the reading step reads the ring, every other one the
+// exchange vector.  The ring holds W values: the smallest power of two that
+// covers every local dependency's reach, at most kBlkWMax.
+constexpr int kBlkStageCap = 24 * 1024;
+constexpr int kBlkWMax = 8192;
+
+template <typename T>
+static DBlk<T> build_blk_plan(Arena &ar, const HostCSR &m, bool upper, int P) {
+  DBlk<T> w;
+  const int n = m.nr;
+  if (n == 0 || P < 1) return w;
+  P = std::min(P, n);
+  auto orig = [&](int ip) { return upper ? n - 1 - ip : ip; };
+  auto lowcol = [&](int j) { return upper ? n - 1 - j : j; };
+  std::vector<int> lev((size_t)n, 0);
+  for (int ip = 0; ip < n; ++ip) {
+    const int o = orig(ip);
+    int l = 0;
+    for (int k = m.irp[o]; k < m.irp[o + 1]; ++k) {
+      const int jp = lowcol(m.ja[k]);
+      if (jp >= ip) return w;  // not triangular in this direction
+      l = std::max(l, lev[jp] + 1);
+    }
+    lev[ip] = l;
+  }
+  // blocks of about equal rows + entries
+  const int64_t total = (int64_t)n + m.nnz();
+  std::vector<int> bnd((size_t)P + 1, n);
+  bnd[0] = 0;
+  {
+    int64_t acc = 0;
+    int b = 1;
+    for (int ip = 0; ip < n && b < P; ++ip) {
+      const int o = orig(ip);
+      acc += 1 + (m.irp[o + 1] - m.irp[o]);
+      if (acc * P >= total * b) bnd[b++] = ip + 1;
+    }
+    for (; b < P; ++b) bnd[b] = n;
+  }
+  std::vector<int> blk((size_t)n), lpos((size_t)n);
+  // per block: positions in (level, row) order
+  std::vector<std::vector<int>> order((size_t)P);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int b = 0; b < P; ++b) {
+    auto &ord = order[b];
+    ord.resize((size_t)(bnd[b + 1] - bnd[b]));
+    for (int ip = bnd[b]; ip < bnd[b + 1]; ++ip) ord[ip - bnd[b]] = ip;
+    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return lev[x] < lev[y]; });
+    for (size_t q = 0; q < ord.size(); ++q) {
+      blk[ord[q]] = b;
+      lpos[ord[q]] = (int)q;
+    }
+  }
+  // steps: (block, first local position) ; split on level change or capacity
+  struct Step {
+    int b, p0, p1, nent;
+  };
+  std::vector<Step> steps;
+  std::vector<int> bstep((size_t)P + 1, 0);
+  for (int b = 0; b < P; ++b) {
+    bstep[b] = (int)steps.size();
+    const auto &ord = order[b];
+    int p = 0;
+    while (p < (int)ord.size()) {
+      Step st{b, p, p, 0};
+      const int l = lev[ord[p]];
+      while (st.p1 < (int)ord.size() && lev[ord[st.p1]] == l) {
+        const int o = orig(ord[st.p1]);
+        const int len = m.irp[o + 1] - m.irp[o];
+        if (st.p1 > st.p0 && blk_bytes<T>(st.p1 - st.p0 + 1, st.nent + len) > kBlkStageCap) break;
+        st.nent += len;
+        ++st.p1;
+      }
+      steps.push_back(st);
+      p = st.p1;
+    }
+  }
+  bstep[P] = (int)steps.size();
+  const int ns = (int)steps.size();
+  // ring size: the reach of the local dependencies (capped)
+  std::vector<int> step_end((size_t)n);
+  for (const Step &st : steps)
+    for (int q = st.p0; q < st.p1; ++q) step_end[order[st.b][q]] = st.p1;
+  int reach = 1;
+  for (int ip = 0; ip < n; ++ip) {
+    const int o = orig(ip);
+    for (int k = m.irp[o]; k < m.irp[o + 1]; ++k) {
+      const int jp = lowcol(m.ja[k]);
+      if (blk[jp] == blk[ip]) reach = std::max(reach, step_end[ip] - lpos[jp]);
+    }
+  }
+  int W = 16;
+  while (W < reach && W < kBlkWMax) W *= 2;
+  // plan blocks
+  std::vector<int64_t> boff((size_t)ns + 1, 0);
+  int capB = 16;
+  for (int s = 0; s < ns; ++s) {
+    const int bytes = blk_bytes<T>(steps[s].p1 - steps[s].p0, steps[s].nent);
+    boff[s + 1] = boff[s] + bytes;
+    capB = std::max(capB, bytes);
+  }
+  if (boff[ns] / 16 > INT32_MAX) return w;
+  std::vector<uint4> plan((size_t)(boff[ns] / 16), make_uint4(0, 0, 0, 0));
+  std::vector<int2> sdesc((size_t)ns);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int s = 0; s < ns; ++s) {
+    const Step &st = steps[s];
+    const int nr = st.p1 - st.p0;
+    unsigned char *base = reinterpret_cast<unsigned char *>(plan.data()) + boff[s];
+    int4 *hdr = reinterpret_cast<int4 *>(base);
+    *hdr = make_int4(nr, st.nent, 0, 0);
+    int4 *rows = reinterpret_cast<int4 *>(base + 16);
+    int *code = reinterpret_cast<int *>(base + 16 + 16 * nr);
+    T *val = reinterpret_cast<T *>(base + blk_off_val<T>(nr, st.nent));
+    int e = 0;
+    for (int q = st.p0; q < st.p1; ++q) {
+      const int ip = order[st.b][q];
+      const int o = orig(ip);
+      rows[q - st.p0] = make_int4(o, e, m.irp[o + 1] - m.irp[o], q);
+      for (int k = m.irp[o]; k < m.irp[o + 1]; ++k, ++e) {
+        const int jp = lowcol(m.ja[k]);
+        const bool ring = blk[jp] == st.b && lpos[jp] >= st.p1 - W;
+        code[e] = ring ? (lpos[jp] & (W - 1)) : -(orig(jp) + 1);
+        val[e] = (T)m.val[k];
+      }
+    }
+    sdesc[s] = make_int2((int)(boff[s] / 16), (int)((boff[s + 1] - boff[s]) / 16));
+  }
+  w.n = n;
+  w.nblocks = P;
+  w.nsteps = ns;
+  w.W = W;
+  w.stage_bytes = capB;
+  w.nnz = m.nnz();
+  w.plan_bytes = boff[ns];
+  w.smem = (size_t)W * sizeof(T) + (size_t)kBlkD * capB + 8 * kBlkD;
+  if (w.smem > 220 * 1024) return w;
+  w.bstep = ar.upload(bstep);
+  w.sdesc = ar.upload(sdesc);
+  w.plan = ar.upload(plan);
+  w.ticket = ar.alloc<int>(2);
+  MLDG_CUDA(cudaMemset(w.ticket, 0, 2 * sizeof(int)));
+  w.ok = true;
+  return w;
+}
+
+template <typename T>
+static void launch_blk(const DBlk<T> &w, const BlkArgs<T> &a, cudaStream_t st) {
+  k_trsv_blk<T><<<w.nblocks, kBlkThreads, w.smem, st>>>(a);
+}
+
 template <typename T>
 static DTri<T> build_tri_dev(Arena &ar, const HostCSR &m, bool upper, int nsm) {
   DTri<T> t;
@@ -2880,6 +3225,7 @@ static void set_trsv_smem_attr() {
   set_attr_t<T, 8>();
   set_attr_t<T, 16>();
   set_attr_t<T, 32>();
+  MLDG_CUDA(cudaFuncSetAttribute(k_trsv_blk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
   done = true;
 }
 
@@ -3115,6 +3461,30 @@ static Engine *make_engine(Handle *h) {
       }
     }
     tick("replicated-window plans");
+    // partitioned solves (k_trsv_blk) for the ILU(0) levels that keep their solves
+    {
+      int blk_min = 4096;
+      if (const char *ev = std::getenv("MLDG_BLK_MIN")) blk_min = std::atoi(ev);
+      if (H.kind == MLDG_SMOOTHER_BJAC && !L.minv && L.n >= blk_min && !std::getenv("MLDG_NO_BLK")) {
+        int P = std::min(h->nsm, std::max(1, L.n / 1024));
+        if (const char *ev = std::getenv("MLDG_BLK_P")) P = std::max(1, std::atoi(ev));
+        HostCSR Lt = transpose(H.L), Ut = transpose(H.U);
+        L.kL = build_blk_plan<T>(ar, H.L, false, P);
+        L.kU = build_blk_plan<T>(ar, H.U, true, P);
+        L.kUt = build_blk_plan<T>(ar, Ut, false, P);
+        L.kLt = build_blk_plan<T>(ar, Lt, true, P);
+        L.blk_ok = L.kL.ok && L.kU.ok && L.kUt.ok && L.kLt.ok;
+        if (std::getenv("MLDG_VERBOSE")) {
+          const DBlk<T> *ks[4] = {&L.kL, &L.kU, &L.kUt, &L.kLt};
+          const char *nm[4] = {"L", "U", "Ut", "Lt"};
+          for (int q = 0; q < 4; ++q)
+            std::fprintf(stderr, "mldg: level %d blk %-2s n=%d P=%d steps=%d W=%d stage=%d smem=%zu plan=%.1f MB ok=%d\n",
+                         l, nm[q], ks[q]->n, ks[q]->nblocks, ks[q]->nsteps, ks[q]->W, ks[q]->stage_bytes,
+                         ks[q]->smem, ks[q]->plan_bytes / 1e6, (int)ks[q]->ok);
+        }
+      }
+    }
+    tick("partitioned-solve plans");
     std::vector<T> dv(dh.begin(), dh.end());
     L.d = ar.upload(dv);
     const int n = std::max(L.n, 1);
@@ -3173,7 +3543,16 @@ static Engine *make_engine(Handle *h) {
       if (L.rep_ok && (std::atol(ev) <= 1 || L.n <= std::atol(ev))) {
         L.rep = true;
         L.ell1 = false;
+        L.blk = false;
         if (std::getenv("MLDG_VERBOSE")) std::fprintf(stderr, "mldg: level n=%d uses rep (forced)\n", L.n);
+      }
+  // MLDG_BLK_FORCE: every level with partitioned-solve plans uses them
+  if (std::getenv("MLDG_BLK_FORCE"))
+    for (auto &L : e->lv)
+      if (L.blk_ok) {
+        L.blk = true;
+        L.rep = false;
+        L.ell1 = false;
       }
   tick("autotune solves");
   if (!std::getenv("MLDG_NO_DENSE_INV"))
@@ -3220,6 +3599,13 @@ static void check_level(const HostLevel &H, int l, const HostLevel *prev) {
 
 static void tune_krylov_spmv(Handle *h);
 
+static void batch_evict(uint64_t serial);
+
+static uint64_t next_serial() {
+  static std::atomic<uint64_t> ctr{1};
+  return ctr.fetch_add(1);
+}
+
 static void finalize(Handle *h, int nlev, int precision) {
   if (nlev < 1 || nlev > (int)h->host.size()) fail(MLDG_ERR_ARG, "nlev %d: %zu levels uploaded", nlev, h->host.size());
   for (int l = 0; l < nlev; ++l)
@@ -3235,6 +3621,8 @@ static void finalize(Handle *h, int nlev, int precision) {
     }
   drop_multi_graphs(h);
   drop_krylov_graphs(h);
+  batch_evict(h->serial);
+  h->serial = 0;
   h->eng.reset();
   h->arena.release();
   h->karena.release();
@@ -3269,6 +3657,7 @@ static void finalize(Handle *h, int nlev, int precision) {
   else
     h->eng.reset(make_engine<float>(h));
   h->finalized = true;
+  h->serial = next_serial();
   if (h->opts.autotune) tune_krylov_spmv(h);
 }
 
@@ -3326,6 +3715,9 @@ static int check_device_error(Handle *h) {
   int e = 0;
   MLDG_CUDA(cudaMemcpy(&e, h->err, sizeof(int), cudaMemcpyDeviceToHost));
   if (e) {
+    // the solve that gave up may have left exchange buffers written and
+    // counters advanced: restore them before the handle is used again
+    if (h->eng) h->eng->reset_solve_state();
     MLDG_CUDA(cudaMemset(h->err, 0, sizeof(int)));
     fail(MLDG_ERR_TIMEOUT, "a triangular-solve dependency wait exceeded its limit (code %d)", e);
   }
@@ -3490,6 +3882,18 @@ static void krylov_prefix(Handle *h, const DCSR<double> &A, cudaGraphConditional
 // once when the device state says the solve is done.
 static void kry_spmv(Handle *h, const DCSR<double> &A) {
   double *r = h->xin, *z = h->yout;
+  if (A.sell) {
+    // grid: at most 16 blocks per SM (the partials hold 2 per block)
+    const int64_t thr = (int64_t)A.nslice() * 32;
+    const int g = (int)std::max<int64_t>(1, std::min<int64_t>((thr + 255) / 256, (int64_t)h->nsm * 16));
+    if (A.sjd)
+      k_kry_spmv_sell<short><<<g, 256, 0, h->st>>>(A.nr, A.soff, A.sjd, A.sval, z, h->kd, h->kd1, h->kq, r,
+                                                   h->kst, h->kpart);
+    else
+      k_kry_spmv_sell<int><<<g, 256, 0, h->st>>>(A.nr, A.soff, A.sja, A.sval, z, h->kd, h->kd1, h->kq, r,
+                                                 h->kst, h->kpart);
+    return;
+  }
   const int64_t thr = (int64_t)A.nr * A.tpr;
   const int g = (int)std::max<int64_t>(1, std::min<int64_t>((thr + 255) / 256, (int64_t)h->nsm * 16));
   switch (A.tpr) {
@@ -3535,9 +3939,12 @@ static void tune_krylov_spmv(Handle *h) {
   MLDG_CUDA(cudaEventCreate(&e1));
   float best = 1e30f;
   int best_t = A.tpr;
+  bool best_sell = false;
   for (double *v : {h->kd, h->kd1, h->kq}) MLDG_CUDA(cudaMemsetAsync(v, 0, sizeof(double) * (size_t)h->n0, h->st));
-  for (int t : {1, 2, 4, 8, 16, 32}) {
-    A.tpr = t;
+  for (int t : {1, 2, 4, 8, 16, 32, 0}) {
+    if (t == 0 && !A.soff) continue;
+    A.sell = t == 0;
+    if (t) A.tpr = t;
     *h->hkst = s0;
     MLDG_CUDA(cudaMemcpyAsync(h->kst, h->hkst, sizeof(KState), cudaMemcpyHostToDevice, h->st));
     kry_spmv(h, A);  // warm
@@ -3549,10 +3956,12 @@ static void tune_krylov_spmv(Handle *h) {
     MLDG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
     if (ms < best) {
       best = ms;
-      best_t = t;
+      best_t = t ? t : best_t;
+      best_sell = t == 0;
     }
   }
   A.tpr = best_t;
+  A.sell = best_sell;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   // leave clean vectors behind
@@ -3854,13 +4263,175 @@ static void krylov_multi(Handle *h, int method, const mldg_csr *Acsr, int nrhs, 
 }
 
 // ---------------------------------------------------------------------------
-// Independent systems solved together: every handle keeps its own hierarchy,
-// stream, FP64 Krylov state and whole-solve graph (capture_solve: initial
-// residual + a device-controlled WHILE loop of V-cycle and iteration).  The
-// batch launches every system's graph on its own stream once; the systems
-// then run concurrently to their own convergence with no host involvement
-// until all have finished.  Each system runs exactly the graph mldg_krylov
-// runs for it, so the results are the same bits.
+// Independent systems solved together in ONE graph launch: the prefixes of
+// all systems (initial residual and state) as parallel branches, then a
+// WHILE node whose body opens, per iteration, an IF branch for every
+// unfinished system -- its V-cycle and its CG/FCG iteration
+// (krylov_iteration) -- and closes with k_kry_any, which keeps the loop
+// going while any system is unfinished.  The branches of one iteration run
+// concurrently; nothing returns to the host until every system has
+// finished.  Each system runs exactly the kernels mldg_krylov runs for it,
+// so the results are the same bits.
+struct BatchGraph {
+  std::vector<uint64_t> key;  // method, then the handles' serials
+  cudaGraphExec_t exec = nullptr;
+  KState **dstates = nullptr;  // device array of the systems' states
+  cudaGraphConditionalHandle *dhc = nullptr;
+  int64_t launches_pre = 0, launches_loop = 0;  // per launch of the prefix / per loop iteration
+  std::vector<int64_t> launches_branch;         // per system, one branch
+  void release() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (dstates) cudaFree(dstates);
+    if (dhc) cudaFree(dhc);
+    exec = nullptr;
+    dstates = nullptr;
+    dhc = nullptr;
+  }
+};
+static std::mutex g_batch_mu;
+static std::vector<std::unique_ptr<BatchGraph>> g_batch_cache;  // most recent last, at most 4
+
+// drops the cached batch graphs that include a handle (at its finalize or destroy)
+static void batch_evict(uint64_t serial) {
+  if (serial == 0) return;
+  std::lock_guard<std::mutex> lk(g_batch_mu);
+  for (size_t k = 0; k < g_batch_cache.size();) {
+    const auto &key = g_batch_cache[k]->key;
+    if (std::find(key.begin() + 1, key.end(), serial) != key.end()) {
+      g_batch_cache[k]->release();
+      g_batch_cache.erase(g_batch_cache.begin() + k);
+    } else {
+      ++k;
+    }
+  }
+}
+
+static cudaGraphNode_t only_sink(cudaGraph_t g) {
+  size_t nn = 0;
+  MLDG_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+  std::vector<cudaGraphNode_t> nodes(nn);
+  MLDG_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+  cudaGraphNode_t sink = nullptr;
+  for (cudaGraphNode_t nd : nodes) {
+    size_t no = 0;
+    MLDG_CUDA(cudaGraphNodeGetDependentNodes(nd, nullptr, &no));
+    if (no == 0) {
+      if (sink) fail(MLDG_ERR_INTERNAL, "batch graph: more than one sink");
+      sink = nd;
+    }
+  }
+  if (!sink) fail(MLDG_ERR_INTERNAL, "batch graph: no sink");
+  return sink;
+}
+
+static void end_capture_quietly(cudaStream_t st) {
+  cudaGraph_t tmp = nullptr;
+  cudaStreamEndCapture(st, &tmp);
+  if (tmp) cudaGraphDestroy(tmp);
+}
+
+static std::unique_ptr<BatchGraph> capture_batch(int nsys, Handle **hs, int method, cudaStream_t ms) {
+  auto bg = std::make_unique<BatchGraph>();
+  bg->key.push_back((uint64_t)method);
+  for (int i = 0; i < nsys; ++i) bg->key.push_back(hs[i]->serial);
+  cudaGraph_t top = nullptr;
+  std::vector<cudaEvent_t> evs;
+  MLDG_CUDA(cudaGraphCreate(&top, 0));
+  try {
+    std::vector<KState *> states(nsys);
+    for (int i = 0; i < nsys; ++i) states[i] = hs[i]->kst;
+    MLDG_CUDA(cudaMalloc(&bg->dstates, sizeof(KState *) * nsys));
+    MLDG_CUDA(cudaMemcpy(bg->dstates, states.data(), sizeof(KState *) * nsys, cudaMemcpyHostToDevice));
+    cudaGraphConditionalHandle hw;
+    MLDG_CUDA(cudaGraphConditionalHandleCreate(&hw, top, 0, cudaGraphCondAssignDefault));
+    for (int i = 0; i <= nsys; ++i) {
+      cudaEvent_t e;
+      MLDG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      evs.push_back(e);
+    }
+    // prefixes: forked from the master stream, joined before k_kry_any
+    MLDG_CUDA(cudaStreamBeginCaptureToGraph(ms, top, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    try {
+      MLDG_CUDA(cudaEventRecord(evs[nsys], ms));
+      for (int i = 0; i < nsys; ++i) {
+        Handle *h = hs[i];
+        MLDG_CUDA(cudaStreamWaitEvent(h->st, evs[nsys], 0));
+        const int64_t l0 = h->last_launches;
+        krylov_prefix(h, h->A0, 0);
+        bg->launches_pre += h->last_launches - l0;
+        h->last_launches = l0;
+        MLDG_CUDA(cudaEventRecord(evs[i], h->st));
+        MLDG_CUDA(cudaStreamWaitEvent(ms, evs[i], 0));
+      }
+      k_kry_any<<<1, 256, 0, ms>>>(bg->dstates, nsys, hw);
+    } catch (...) {
+      end_capture_quietly(ms);
+      throw;
+    }
+    cudaGraph_t gout = nullptr;
+    MLDG_CUDA(cudaStreamEndCapture(ms, &gout));
+    bg->launches_pre += 1;
+    cudaGraphNode_t sink = only_sink(top);
+    cudaGraphNodeParams wp = {};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = hw;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t wn;
+    MLDG_CUDA(cudaGraphAddNode(&wn, top, &sink, 1, &wp));
+    cudaGraph_t body = wp.conditional.phGraph_out[0];
+    // the IF handles of the branches live in the loop body
+    std::vector<cudaGraphConditionalHandle> hc(nsys);
+    for (int i = 0; i < nsys; ++i) MLDG_CUDA(cudaGraphConditionalHandleCreate(&hc[i], body, 0, 0));
+    MLDG_CUDA(cudaMalloc(&bg->dhc, sizeof(cudaGraphConditionalHandle) * nsys));
+    MLDG_CUDA(cudaMemcpy(bg->dhc, hc.data(), sizeof(cudaGraphConditionalHandle) * nsys, cudaMemcpyHostToDevice));
+    MLDG_CUDA(cudaStreamBeginCaptureToGraph(ms, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    k_kry_gate<<<1, 256, 0, ms>>>(bg->dstates, bg->dhc, nsys);
+    MLDG_CUDA(cudaStreamEndCapture(ms, &gout));
+    cudaGraphNode_t gate = only_sink(body);
+    std::vector<cudaGraphNode_t> ifs(nsys);
+    bg->launches_branch.assign(nsys, 0);
+    for (int i = 0; i < nsys; ++i) {
+      Handle *h = hs[i];
+      cudaGraphNodeParams ip = {};
+      ip.type = cudaGraphNodeTypeConditional;
+      ip.conditional.handle = hc[i];
+      ip.conditional.type = cudaGraphCondTypeIf;
+      ip.conditional.size = 1;
+      MLDG_CUDA(cudaGraphAddNode(&ifs[i], body, &gate, 1, &ip));
+      cudaGraph_t br = ip.conditional.phGraph_out[0];
+      const int64_t l0 = h->last_launches;
+      MLDG_CUDA(cudaStreamBeginCaptureToGraph(h->st, br, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+      h->eng->capturing = true;
+      try {
+        h->eng->record('N');
+        krylov_iteration(h, h->A0, 0);
+      } catch (...) {
+        h->eng->capturing = false;
+        end_capture_quietly(h->st);
+        throw;
+      }
+      h->eng->capturing = false;
+      MLDG_CUDA(cudaStreamEndCapture(h->st, &gout));
+      bg->launches_branch[i] = h->eng->launches + (h->last_launches - l0);
+      h->last_launches = l0;
+    }
+    MLDG_CUDA(cudaStreamBeginCaptureToGraph(ms, body, ifs.data(), nullptr, nsys, cudaStreamCaptureModeThreadLocal));
+    k_kry_any<<<1, 256, 0, ms>>>(bg->dstates, nsys, hw);
+    MLDG_CUDA(cudaStreamEndCapture(ms, &gout));
+    bg->launches_loop = 2;  // gate and any
+    MLDG_CUDA(cudaGraphInstantiate(&bg->exec, top, 0));
+  } catch (...) {
+    for (cudaEvent_t e : evs) cudaEventDestroy(e);
+    cudaGraphDestroy(top);
+    bg->release();
+    throw;
+  }
+  for (cudaEvent_t e : evs) cudaEventDestroy(e);
+  cudaGraphDestroy(top);
+  return bg;
+}
+
 static void krylov_batch(int nsys, Handle **hs, int method, const double *const *b, double *const *x, double tol,
                          int itmax, int *iters, double *relres, int mem, double *ms_out) {
   if (nsys < 0) fail(MLDG_ERR_ARG, "nsys < 0");
@@ -3884,16 +4455,27 @@ static void krylov_batch(int nsys, Handle **hs, int method, const double *const 
   MLDG_CUDA(cudaSetDevice(dev));
   const cudaMemcpyKind h2d = mem == MLDG_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   const cudaMemcpyKind d2h = mem == MLDG_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  std::lock_guard<std::mutex> lk(g_batch_mu);
   cudaStream_t ms = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   MLDG_CUDA(cudaStreamCreateWithFlags(&ms, cudaStreamNonBlocking));
   MLDG_CUDA(cudaEventCreate(&e0));
   MLDG_CUDA(cudaEventCreate(&e1));
   try {
-    // graphs first (capture is not timed)
-    for (int i = 0; i < nsys; ++i) {
-      hs[i]->last_launches = 0;
-      capture_solve(hs[i], method, 'N', hs[i]->A0);
+    // the batch graph of exactly these finalized handles (captured on first use, not timed)
+    std::vector<uint64_t> key{(uint64_t)method};
+    for (int i = 0; i < nsys; ++i) key.push_back(hs[i]->serial);
+    BatchGraph *bg = nullptr;
+    for (auto &c : g_batch_cache)
+      if (c->key == key) bg = c.get();
+    if (!bg) {
+      for (int i = 0; i < nsys; ++i) MLDG_CUDA(cudaStreamSynchronize(hs[i]->st));
+      g_batch_cache.push_back(capture_batch(nsys, hs, method, ms));
+      bg = g_batch_cache.back().get();
+      if (g_batch_cache.size() > 4) {
+        g_batch_cache.front()->release();
+        g_batch_cache.erase(g_batch_cache.begin());
+      }
     }
     MLDG_CUDA(cudaEventRecord(e0, ms));
     for (int i = 0; i < nsys; ++i) {
@@ -3902,27 +4484,31 @@ static void krylov_batch(int nsys, Handle **hs, int method, const double *const 
       h->hkpar->tol = tol;
       h->hkpar->itmax = itmax;
       h->hkpar->method = method;
-      MLDG_CUDA(cudaStreamWaitEvent(h->st, e0, 0));
-      MLDG_CUDA(cudaMemcpyAsync(h->kb, b[i], sizeof(double) * n, h2d, h->st));
-      MLDG_CUDA(cudaMemcpyAsync(h->kx, x[i], sizeof(double) * n, h2d, h->st));
-      MLDG_CUDA(cudaMemcpyAsync(h->kpar, h->hkpar, sizeof(KParams), cudaMemcpyHostToDevice, h->st));
-      MLDG_CUDA(cudaGraphLaunch(h->sgraph[method][0], h->st));
-      MLDG_CUDA(cudaMemcpyAsync(h->hkst, h->kst, sizeof(KState), cudaMemcpyDeviceToHost, h->st));
-      MLDG_CUDA(cudaMemcpyAsync(x[i], h->kx, sizeof(double) * n, d2h, h->st));
-      MLDG_CUDA(cudaEventRecord(h->ev1, h->st));
-      MLDG_CUDA(cudaStreamWaitEvent(ms, h->ev1, 0));
+      MLDG_CUDA(cudaMemcpyAsync(h->kb, b[i], sizeof(double) * n, h2d, ms));
+      MLDG_CUDA(cudaMemcpyAsync(h->kx, x[i], sizeof(double) * n, h2d, ms));
+      MLDG_CUDA(cudaMemcpyAsync(h->kpar, h->hkpar, sizeof(KParams), cudaMemcpyHostToDevice, ms));
+    }
+    MLDG_CUDA(cudaGraphLaunch(bg->exec, ms));
+    for (int i = 0; i < nsys; ++i) {
+      Handle *h = hs[i];
+      MLDG_CUDA(cudaMemcpyAsync(h->hkst, h->kst, sizeof(KState), cudaMemcpyDeviceToHost, ms));
+      MLDG_CUDA(cudaMemcpyAsync(x[i], h->kx, sizeof(double) * h->n0, d2h, ms));
     }
     MLDG_CUDA(cudaEventRecord(e1, ms));
     MLDG_CUDA(cudaStreamSynchronize(ms));
     float t = 0;
     MLDG_CUDA(cudaEventElapsedTime(&t, e0, e1));
     if (ms_out) *ms_out = t;
+    int itmax_seen = 0;
+    for (int i = 0; i < nsys; ++i) itmax_seen = std::max(itmax_seen, hs[i]->hkst->it);
     for (int i = 0; i < nsys; ++i) {
       Handle *h = hs[i];
       iters[i] = h->hkst->it;
       relres[i] = h->hkst->err;
       h->last_ms = t;
-      h->last_launches = h->sglaunch_pre[method][0] + (int64_t)h->hkst->it * h->sglaunch_body[method][0];
+      // this system's own kernels; the batch's gate/any kernels are counted on the first system
+      h->last_launches = (int64_t)h->hkst->it * bg->launches_branch[i] +
+                         (i == 0 ? bg->launches_pre + (int64_t)itmax_seen * bg->launches_loop : 3);
       check_device_error(h);
     }
   } catch (...) {
@@ -4371,6 +4957,7 @@ extern "C" void mldg_destroy(mldg_handle *hp) {
     if (h.gexec[t]) cudaGraphExecDestroy(h.gexec[t]);
   mldg::drop_multi_graphs(&h);
   mldg::drop_krylov_graphs(&h);
+  mldg::batch_evict(h.serial);
   h.eng.reset();
   h.arena.release();
   h.karena.release();
@@ -4391,6 +4978,13 @@ extern "C" void mldg_destroy(mldg_handle *hp) {
 // host emulation of k_trsv_rep.  trans 'N': y = U^{-1} diag(d) L^{-1} x;
 // 'T': y = L^{-T} diag(d) U^{-T} x.  stats[4]: plan violations, steps of the
 // first solve, far entries, plans usable.
+extern "C" int mldg_test_set_spin_limit(int device, int polls) {
+  const int v = polls < 0 ? mldg::kSpinLimit : polls;
+  if (cudaSetDevice(device) != cudaSuccess) return MLDG_ERR_CUDA;
+  if (cudaMemcpyToSymbol(mldg::g_spin_limit, &v, sizeof(int)) != cudaSuccess) return MLDG_ERR_CUDA;
+  return cudaDeviceSynchronize() == cudaSuccess ? MLDG_SUCCESS : MLDG_ERR_CUDA;
+}
+
 extern "C" int mldg_rep_plan_check(const mldg_csr *Lc, const mldg_csr *Uc, const double *d, const double *x,
                                    double *y, int cluster, int fp32, char trans, long long *stats) {
   if (!Lc || !Uc || !d || !x || !y || !stats || (cluster != 8 && cluster != 16)) return MLDG_ERR_ARG;

@@ -74,6 +74,12 @@ template <> struct Bits<float> {
 constexpr int kSpinLimit = 1 << 22;
 constexpr int kSpinCheck = 64;
 constexpr int kErrTimeout = 4020;
+// The limit in force (kSpinLimit unless a test lowers it through
+// mldg_test_set_spin_limit to make waits run out on purpose).  Only these
+// sentinel polls of global memory read it; the mbarrier waits of the window
+// and cluster solves keep their fixed limit.
+static __device__ int g_spin_limit = kSpinLimit;
+__device__ __forceinline__ int spin_limit() { return *(volatile int *)&g_spin_limit; }
 
 template <typename T>
 __device__ __forceinline__ T wait_value(const T *p, int *err) {
@@ -81,7 +87,8 @@ __device__ __forceinline__ T wait_value(const T *p, int *err) {
   const U sent = (U)Sentinel<T>::bits;
   U v = Bits<T>::load(p);
   if (v != sent) return Bits<T>::from(v);
-  for (int it = 1; it < kSpinLimit; ++it) {
+  const int lim = spin_limit();
+  for (int it = 1; it < lim; ++it) {
     v = Bits<T>::load(p);
     if (v != sent) return Bits<T>::from(v);
     if ((it % kSpinCheck) == 0) {
@@ -130,6 +137,101 @@ __global__ void __launch_bounds__(256) k_spmv(int nr, const int *__restrict__ ir
       T r = a1 * s;
       if (b) r = fma(a0, b[row], r);
       if (a2 != T(0)) r = fma(a2, out[row], r);
+      out[row] = r;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The same operators on a sliced-ELL copy of the matrix (SELL-32): rows in
+// slices of 32, slice s holding its rows' k-th entries at
+// soff[s] + 32*k + lane (k < the slice's longest row; shorter rows padded
+// with zero values on an in-range column).  One thread per row: the 32
+// threads of a warp read 32 consecutive values and column indices per entry,
+// and every thread issues SELL_U entries' loads before using them, so many
+// more bytes are in flight per warp than with lanes sharing a short CSR row.
+// A row's entries are summed in stored order from zero.
+constexpr int kSellU = 8;
+
+__device__ __forceinline__ int sell_col(const int *__restrict__ sj, int k, int) { return sj[k]; }
+__device__ __forceinline__ int sell_col(const short *__restrict__ sj, int k, int row) { return row + (int)sj[k]; }
+
+// acc += sum over the row's slots of sv[k] * f(col(k)) for the thread's row
+template <typename T, typename CI, typename F>
+__device__ __forceinline__ T sell_row(const CI *__restrict__ sj, const T *__restrict__ sv, int e0, int e1,
+                                      int row, F f) {
+  T acc = T(0);
+  for (int e = e0; e < e1; e += 32 * kSellU) {
+    T vv[kSellU];
+    int jj[kSellU];
+#pragma unroll
+    for (int u = 0; u < kSellU; ++u) {
+      const int k = e + 32 * u;
+      const bool ok = k < e1;
+      vv[u] = ok ? sv[k] : T(0);
+      jj[u] = ok ? sell_col(sj, k, row) : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < kSellU; ++u)
+      if (e + 32 * u < e1) acc = fma(vv[u], f(jj[u]), acc);
+  }
+  return acc;
+}
+
+// out[i] = a0*b[i] + a1*(A v)[i] + a2*out[i]
+template <typename T, typename CI>
+__global__ void __launch_bounds__(256) k_spmv_sell(int nr, const int *__restrict__ soff,
+                                                   const CI *__restrict__ sj, const T *__restrict__ sv,
+                                                   const T *__restrict__ v, T a1, const T *__restrict__ b,
+                                                   T a0, T *out, T a2) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int ns = (nr + 31) >> 5;
+  for (int sl = warp; sl < ns; sl += nwarps) {
+    const int row = (sl << 5) + lane;
+    const T s = sell_row<T>(sj, sv, soff[sl] + lane, soff[sl + 1], row,
+                            [&](int j) { return __ldg(v + j); });
+    if (row < nr) {
+      T r = a1 * s;
+      if (b) r = fma(a0, b[row], r);
+      if (a2 != T(0)) r = fma(a2, out[row], r);
+      out[row] = r;
+    }
+  }
+}
+
+// the point-Jacobi sweep of k_jacobi on the SELL copy of ND
+template <typename T, typename CI>
+__global__ void __launch_bounds__(256) k_jacobi_sell(int nr, const int *__restrict__ soff,
+                                                     const CI *__restrict__ sj, const T *__restrict__ sv,
+                                                     const T *__restrict__ d, const T *__restrict__ x,
+                                                     const T *__restrict__ ty, int first, T omega, T alpha,
+                                                     T beta, T *out) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int ns = (nr + 31) >> 5;
+  for (int sl = warp; sl < ns; sl += nwarps) {
+    const int row = (sl << 5) + lane;
+    T s;
+    if (first)
+      s = sell_row<T>(sj, sv, soff[sl] + lane, soff[sl + 1], row,
+                      [&](int j) { return omega * (__ldg(d + j) * __ldg(x + j)); });
+    else
+      s = sell_row<T>(sj, sv, soff[sl] + lane, soff[sl + 1], row, [&](int j) { return __ldg(ty + j); });
+    if (row < nr) {
+      const T di = d[row], xi = x[row];
+      const T t = di * (xi - s);
+      T vv;
+      if (omega == T(1)) {
+        vv = t;
+      } else {
+        const T tyi = first ? omega * (di * xi) : ty[row];
+        vv = (T(1) - omega) * tyi + omega * t;
+      }
+      T r = alpha * vv;
+      if (beta != T(0)) r = fma(beta, out[row], r);
       out[row] = r;
     }
   }
@@ -603,12 +705,13 @@ __global__ void __launch_bounds__(256) k_trsv_sf(TriArgs<T> a) {
         src[e] = a.cur + (a.rev ? (a.n - 1 - r.j[e]) : r.j[e]);
         raw[e] = has ? Bits<T>::load(src[e]) : (U)0;
       }
+      const int lim = spin_limit();
       for (int it = 0;; ++it) {
         bool missing = false;
 #pragma unroll
         for (int e = 0; e < E; ++e) missing |= (raw[e] == sent);
         if (!missing) break;
-        if (it >= kSpinLimit) {
+        if (it >= lim) {
           atomicExch(a.err, kErrTimeout);
           break;
         }
@@ -880,6 +983,59 @@ __global__ void __launch_bounds__(256) k_kry_spmv(int nr, const int *__restrict_
   }
 }
 
+// k_kry_spmv on the SELL copy of A (one thread per row)
+template <typename CI>
+__global__ void __launch_bounds__(256) k_kry_spmv_sell(int nr, const int *__restrict__ soff,
+                                                       const CI *__restrict__ sj, const double *__restrict__ sv,
+                                                       const double *__restrict__ z, double *d0, double *d1,
+                                                       double *__restrict__ q, const double *__restrict__ r,
+                                                       KState *st, double *partial) {
+  __shared__ double sh[32];
+  if (st->done) return;
+  const int it = st->it;
+  const bool first = it == 0;
+  const double beta = st->beta;
+  const double *dold = (it & 1) ? d0 : d1;
+  double *dnew = (it & 1) ? d1 : d0;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int ns = (nr + 31) >> 5;
+  double sdq = 0, sdr = 0;
+  for (int sl = warp; sl < ns; sl += nwarps) {
+    const int row = (sl << 5) + lane;
+    double s;
+    if (first)
+      s = sell_row<double>(sj, sv, soff[sl] + lane, soff[sl + 1], row, [&](int j) { return __ldg(z + j); });
+    else
+      s = sell_row<double>(sj, sv, soff[sl] + lane, soff[sl + 1], row,
+                           [&](int j) { return fma(beta, dold[j], __ldg(z + j)); });
+    if (row < nr) {
+      const double di = first ? z[row] : fma(beta, dold[row], z[row]);
+      dnew[row] = di;
+      q[row] = s;
+      sdq = fma(di, s, sdq);
+      sdr = fma(di, r[row], sdr);
+    }
+  }
+  sdq = block_sum(sdq, sh);
+  sdr = block_sum(sdr, sh);
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = sdq;
+    partial[2 * blockIdx.x + 1] = sdr;
+  }
+  if (kry_last_block(&st->ticket[1])) {
+    const double dq = kry_sum_partials(partial, gridDim.x, 2, 0, sh);
+    const double dr = kry_sum_partials(partial, gridDim.x, 2, 1, sh);
+    if (threadIdx.x == 0) {
+      st->dq = dq;
+      st->dr = dr;
+      st->alpha = (st->method == 1) ? dr / dq : st->rho / dq;
+      st->ticket[1] = 0u;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kRedThreads) k_kry_update(int n, const double *d0, const double *d1,
                                                            const double *__restrict__ q, double *x,
                                                            double *r, KState *st, double *partial,
@@ -912,6 +1068,23 @@ __global__ void __launch_bounds__(kRedThreads) k_kry_update(int n, const double 
       if (hc) cudaGraphSetConditional(hc, done ? 0u : 1u);
     }
   }
+}
+
+// Independent systems solved in one graph: a WHILE loop whose body opens one
+// IF branch (V-cycle + iteration) per unfinished system.  k_kry_gate sets
+// every branch's conditional from its system's state at the top of the body;
+// k_kry_any keeps the loop going while any system is unfinished.
+__global__ void k_kry_gate(KState *const *st, const cudaGraphConditionalHandle *hc, int nsys) {
+  for (int i = threadIdx.x; i < nsys; i += blockDim.x) cudaGraphSetConditional(hc[i], st[i]->done ? 0u : 1u);
+}
+__global__ void k_kry_any(KState *const *st, int nsys, cudaGraphConditionalHandle hw) {
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < nsys; i += blockDim.x)
+    if (!st[i]->done) atomicOr(&any, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) cudaGraphSetConditional(hw, any ? 1u : 0u);
 }
 
 }  // namespace mldg

@@ -150,12 +150,13 @@ __global__ void __launch_bounds__(256) k_trsv_sf_m(TriArgs<T> a, int nblk_m, con
           src[e] = a.cur + (size_t)oj * K + c;
           raw[e] = has ? Bits<T>::load(src[e]) : (U)0;
         }
+        const int lim = spin_limit();
         for (int it = 0;; ++it) {
           bool missing = false;
 #pragma unroll
           for (int e = 0; e < 4; ++e) missing |= (raw[e] == sent);
           if (!missing) break;
-          if (it >= kSpinLimit) {
+          if (it >= lim) {
             atomicExch(a.err, kErrTimeout);
             break;
           }
@@ -273,12 +274,13 @@ __device__ __forceinline__ bool ell_wait(typename Bits<T>::U (&raw)[N], const in
                                          int *err, int backoff) {
   typedef typename Bits<T>::U U;
   const U sent = (U)Sentinel<T>::bits;
+  const int lim = spin_limit();
   for (int it = 0;; ++it) {
     bool missing = false;
 #pragma unroll
     for (int e = 0; e < N; ++e) missing |= (raw[e] == sent);
     if (!missing) return true;
-    if (it >= kSpinLimit) {
+    if (it >= lim) {
       atomicExch(err, kErrTimeout);
       return false;
     }
