@@ -184,10 +184,13 @@ int mldg_krylov_multi(mldg_handle *h, int method, const mldg_csr *A, int nrhs,
 
 /* nsys independent systems, each with its own finalized handle (hierarchy
  * and finest-level matrix A_i, all on one device), solved together by CG/FCG
- * in FP64: an iteration of system i (its V-cycle, in the handle's precision,
- * and its Krylov kernels) is one CUDA graph captured on first use, and every
- * iteration launches the graphs of all unconverged systems on their own
- * streams so that the small systems' latency-bound V-cycles overlap.  b[i],
+ * in FP64 in ONE graph launch: the systems' initial residuals, then a loop
+ * whose every iteration runs, as concurrent branches, the V-cycle (in the
+ * handle's precision) and the CG/FCG step of each unfinished system; the
+ * stopping tests run on the device and the loop ends when the last system
+ * has finished.  The graph is captured on the first call with these handles
+ * (kept for later calls until one of them is finalized again or destroyed);
+ * handles with a K-cycle, use_graphs = 0 or a probe set are rejected.  b[i],
  * x[i] are vectors of handle i's size (x[i] holds the initial guess); each
  * system stops on its own ||b_i - A_i x_i||_2 / ||b_i||_2 <= tol.  Results
  * equal mldg_krylov on each handle.  *ms (optional) receives the device time

@@ -28,6 +28,19 @@ extern "C" {
 int mldg_rep_plan_check(const mldg_csr *L, const mldg_csr *U, const double *d, const double *x,
                         double *y, int cluster, int fp32, char trans, long long *stats);
 
+/* Builds the partitioned-solve plan (k_trsv_blk) of the strictly triangular
+ * factor T (0-based CSR, n x n; upper != 0: an upper factor, walked in
+ * reverse) with nblocks blocks, exactly as mldg_finalize would, and replays
+ * it through a host emulation of the kernel: blocks in ticket order, steps
+ * in order, every plan access checked against its buffer, every ring read
+ * against the row that slot holds, every remote read against a written
+ * value, no slot overwritten while its step reads it.  t = scale o rhs -
+ * T_strict t (scale may be NULL).  stats[6]: violations, steps, ring size,
+ * plan usable (1) or not (0, t untouched), blocks, shared memory bytes.
+ * Returns MLDG_SUCCESS or an error code. */
+int mldg_blk_plan_check(const mldg_csr *T, int upper, const double *scale, const double *rhs, double *t,
+                        int nblocks, int fp32, long long *stats);
+
 /* Polls a sentinel wait of the sync-free and ELL triangular solves makes
  * before it gives up with MLDG_ERR_TIMEOUT, on `device`; polls < 0 restores
  * the default (2^22).  A test lowers it (0: give up at the first poll that

@@ -1298,7 +1298,7 @@ struct EngineT : Engine {
           }
         }
         op->tpr = best_t;
-        op->sell = best_sell;
+        op->sell = best_sell || (op->soff && std::getenv("MLDG_SELL_FORCE"));
       }
     }
     launches = 0;
@@ -2954,8 +2954,19 @@ constexpr int kBlkStageCap = 24 * 1024;
 constexpr int kBlkWMax = 8192;
 
 template <typename T>
-static DBlk<T> build_blk_plan(Arena &ar, const HostCSR &m, bool upper, int P) {
-  DBlk<T> w;
+struct HostBlk {
+  bool ok = false;
+  int n = 0, nblocks = 0, nsteps = 0, W = 0, stage_bytes = 0;
+  size_t smem = 0;
+  int64_t nnz = 0, plan_bytes = 0;
+  std::vector<int> bstep;
+  std::vector<int2> sdesc;
+  std::vector<uint4> plan;
+};
+
+template <typename T>
+static HostBlk<T> build_blk_host(const HostCSR &m, bool upper, int P) {
+  HostBlk<T> w;
   const int n = m.nr;
   if (n == 0 || P < 1) return w;
   P = std::min(P, n);
@@ -3084,13 +3095,126 @@ static DBlk<T> build_blk_plan(Arena &ar, const HostCSR &m, bool upper, int P) {
   w.plan_bytes = boff[ns];
   w.smem = (size_t)W * sizeof(T) + (size_t)kBlkD * capB + 8 * kBlkD;
   if (w.smem > 220 * 1024) return w;
-  w.bstep = ar.upload(bstep);
-  w.sdesc = ar.upload(sdesc);
-  w.plan = ar.upload(plan);
+  w.bstep = std::move(bstep);
+  w.sdesc = std::move(sdesc);
+  w.plan = std::move(plan);
+  w.ok = true;
+  return w;
+}
+
+template <typename T>
+static DBlk<T> build_blk_plan(Arena &ar, const HostCSR &m, bool upper, int P) {
+  DBlk<T> w;
+  HostBlk<T> hb = build_blk_host<T>(m, upper, P);
+  if (!hb.ok) return w;
+  w.n = hb.n;
+  w.nblocks = hb.nblocks;
+  w.nsteps = hb.nsteps;
+  w.W = hb.W;
+  w.stage_bytes = hb.stage_bytes;
+  w.nnz = hb.nnz;
+  w.plan_bytes = hb.plan_bytes;
+  w.smem = hb.smem;
+  w.bstep = ar.upload(hb.bstep);
+  w.sdesc = ar.upload(hb.sdesc);
+  w.plan = ar.upload(hb.plan);
   w.ticket = ar.alloc<int>(2);
   MLDG_CUDA(cudaMemset(w.ticket, 0, 2 * sizeof(int)));
   w.ok = true;
   return w;
+}
+
+// Host emulation of k_trsv_blk on a plan: blocks in ticket order, steps in
+// order, rows of a step in the kernel's thread order, with every access the
+// kernel makes checked against its buffer (plan block inside the plan and
+// within the stage, row and entry ranges, ring slots, exchange indices), every
+// ring read against the position that slot holds, and every remote read
+// against a written value.  Returns the number of violations; t receives the
+// solution (original numbering) of t = scale o rhs - T_strict t.
+template <typename T>
+static int64_t blk_emulate(const HostBlk<T> &w, const HostCSR &m, const std::vector<double> &rhs,
+                           const double *scale, std::vector<double> &t) {
+  int64_t bad = 0;
+  const int n = w.n, W = w.W;
+  if (W < 1 || (W & (W - 1)) || (int)w.bstep.size() != w.nblocks + 1 || w.bstep[0] != 0 ||
+      w.bstep[w.nblocks] != w.nsteps || w.stage_bytes % 16 || w.smem > 220 * 1024)
+    return 1;
+  std::vector<double> cur((size_t)n, std::nan(""));
+  std::vector<char> written((size_t)n, 0);
+  std::vector<double> ring((size_t)W, 0.0);
+  t.assign((size_t)n, 0.0);
+  const unsigned char *planb = reinterpret_cast<const unsigned char *>(w.plan.data());
+  const int64_t plan_size = (int64_t)w.plan.size() * 16;
+  for (int b = 0; b < w.nblocks; ++b) {
+    std::vector<int> ring_row((size_t)W, -1);  // original row whose value a slot holds
+    if (w.bstep[b + 1] < w.bstep[b]) return bad + 1;
+    for (int s = w.bstep[b]; s < w.bstep[b + 1]; ++s) {
+      const int2 dsc = w.sdesc[s];
+      const int64_t off = (int64_t)dsc.x * 16, bytes = (int64_t)dsc.y * 16;
+      if (off < 0 || bytes < 16 || off + bytes > plan_size || bytes > w.stage_bytes) {
+        ++bad;
+        continue;
+      }
+      const unsigned char *st = planb + off;
+      const int4 hdr = *reinterpret_cast<const int4 *>(st);
+      if (hdr.x < 0 || hdr.y < 0 || blk_bytes<T>(hdr.x, hdr.y) > bytes) {
+        ++bad;
+        continue;
+      }
+      const int4 *rows = reinterpret_cast<const int4 *>(st + 16);
+      const int *code = reinterpret_cast<const int *>(st + 16 + 16 * hdr.x);
+      const T *val = reinterpret_cast<const T *>(st + blk_off_val<T>(hdr.x, hdr.y));
+      std::vector<std::pair<int, double>> outv;
+      std::vector<char> read_slot((size_t)W, 0);
+      for (int r = 0; r < hdr.x; ++r) {
+        const int4 rw = rows[r];
+        if (rw.x < 0 || rw.x >= n || rw.y < 0 || rw.z < 0 || rw.y + rw.z > hdr.y ||
+            rw.z != m.irp[rw.x + 1] - m.irp[rw.x]) {
+          ++bad;
+          continue;
+        }
+        double acc = 0.0;
+        for (int e = rw.y; e < rw.y + rw.z; ++e) {
+          const int c = code[e];
+          const int k = m.irp[rw.x] + (e - rw.y);  // the CSR entry this slot stands for
+          const int dep = m.ja[k];
+          if ((double)val[e] != (double)(T)m.val[k]) ++bad;
+          double dv = 0.0;
+          if (c >= 0) {
+            if (c >= W || ring_row[c] != dep) {
+              ++bad;
+            } else {
+              dv = ring[c];
+              read_slot[c] = 1;
+            }
+          } else {
+            const int64_t j = -(int64_t)c - 1;
+            if (j != dep || !written[j])
+              ++bad;
+            else
+              dv = cur[j];
+          }
+          acc += (double)val[e] * dv;
+        }
+        const double sc = scale ? scale[rw.x] : 1.0;
+        outv.emplace_back(r, sc * rhs[rw.x] - acc);
+      }
+      // the step's values become visible after its barrier
+      for (auto &pr : outv) {
+        const int4 rw = rows[pr.first];
+        const int slot = rw.w & (W - 1);
+        if (read_slot[slot]) ++bad;  // a slot written while the step still reads it
+        ring[slot] = pr.second;
+        ring_row[slot] = rw.x;
+        if (written[rw.x]) ++bad;
+        cur[rw.x] = pr.second;
+        written[rw.x] = 1;
+        t[rw.x] = pr.second;
+      }
+    }
+  }
+  for (int i = 0; i < n; ++i) bad += !written[i];
+  return bad;
 }
 
 template <typename T>
@@ -3522,7 +3646,7 @@ static Engine *make_engine(Handle *h) {
     }
   }
   MLDG_CUDA(cudaStreamSynchronize(h->st));
-  if (h->opts.autotune) {
+  if (h->opts.autotune && !std::getenv("MLDG_NO_AUTOTUNE")) {
     int nmax = 1;
     for (auto &L : e->lv) nmax = std::max(nmax, L.n);
     e->tune_n = nmax;
@@ -3658,7 +3782,7 @@ static void finalize(Handle *h, int nlev, int precision) {
     h->eng.reset(make_engine<float>(h));
   h->finalized = true;
   h->serial = next_serial();
-  if (h->opts.autotune) tune_krylov_spmv(h);
+  if (h->opts.autotune && !std::getenv("MLDG_NO_AUTOTUNE")) tune_krylov_spmv(h);
 }
 
 static bool kcycle_handle(const Handle *h) { return h->cycle == MLDG_CYCLE_K || h->cycle == MLDG_CYCLE_KSYM; }
@@ -3961,7 +4085,7 @@ static void tune_krylov_spmv(Handle *h) {
     }
   }
   A.tpr = best_t;
-  A.sell = best_sell;
+  A.sell = best_sell || (A.soff && std::getenv("MLDG_SELL_FORCE"));
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   // leave clean vectors behind
@@ -4983,6 +5107,34 @@ extern "C" int mldg_test_set_spin_limit(int device, int polls) {
   if (cudaSetDevice(device) != cudaSuccess) return MLDG_ERR_CUDA;
   if (cudaMemcpyToSymbol(mldg::g_spin_limit, &v, sizeof(int)) != cudaSuccess) return MLDG_ERR_CUDA;
   return cudaDeviceSynchronize() == cudaSuccess ? MLDG_SUCCESS : MLDG_ERR_CUDA;
+}
+
+extern "C" int mldg_blk_plan_check(const mldg_csr *Tc, int upper, const double *scale, const double *rhs,
+                                   double *t, int nblocks, int fp32, long long *stats) {
+  if (!Tc || !rhs || !t || !stats || nblocks < 1) return MLDG_ERR_ARG;
+  try {
+    mldg::HostCSR m = mldg::copy_csr(*Tc, 0, "T", 0);
+    if (m.nr != m.nc) return MLDG_ERR_ARG;
+    std::vector<double> r(rhs, rhs + m.nr), out;
+    auto run = [&](auto tag) {
+      typedef decltype(tag) TT;
+      mldg::HostBlk<TT> hb = mldg::build_blk_host<TT>(m, upper != 0, nblocks);
+      stats[0] = hb.ok ? mldg::blk_emulate<TT>(hb, m, r, scale, out) : 0;
+      stats[1] = hb.nsteps;
+      stats[2] = hb.W;
+      stats[3] = hb.ok ? 1 : 0;
+      stats[4] = hb.nblocks;
+      stats[5] = (long long)hb.smem;
+    };
+    if (fp32)
+      run(float());
+    else
+      run(double());
+    if (stats[3]) std::copy(out.begin(), out.end(), t);
+  } catch (const mldg::Error &e) {
+    return e.code;
+  }
+  return MLDG_SUCCESS;
 }
 
 extern "C" int mldg_rep_plan_check(const mldg_csr *Lc, const mldg_csr *Uc, const double *d, const double *x,

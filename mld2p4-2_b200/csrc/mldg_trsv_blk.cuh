@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(kBlkThreads, 1) k_trsv_blk(BlkArgs<T> a) {
   // the next step's row of this thread: original row, right-hand side and
   // raw bits of its first kBlkRE remote dependencies (the sentinel if not yet written)
   int n_orig = -1;
-  T n_rhs = T(0);
+  T n_src = T(0), n_sc = T(1), n_out = T(0);
   U n_raw[kBlkRE];
   auto prefetch = [&](int k) {  // step s0 + k, whose stage is ready
     n_orig = -1;
@@ -136,7 +136,10 @@ __global__ void __launch_bounds__(kBlkThreads, 1) k_trsv_blk(BlkArgs<T> a) {
     const int4 rw = reinterpret_cast<const int4 *>(st + 16)[tid];
     const int *code = reinterpret_cast<const int *>(st + 16 + 16 * hdr.x);
     n_orig = rw.x;
-    n_rhs = a.scale ? a.scale[rw.x] * a.src[rw.x] : a.src[rw.x];
+    // loads only: nothing here waits for them (they are used in the next step)
+    n_src = a.src[rw.x];
+    if (a.scale) n_sc = a.scale[rw.x];
+    if (a.out && a.beta != T(0)) n_out = a.out[rw.x];
 #pragma unroll
     for (int e = 0; e < kBlkRE; ++e) {
       const int c = e < rw.z ? code[rw.y + e] : 0;
@@ -161,7 +164,8 @@ __global__ void __launch_bounds__(kBlkThreads, 1) k_trsv_blk(BlkArgs<T> a) {
       for (int r = tid; r < hdr.x; r += kBlkThreads) {
         const int4 rw = rows[r];
         const bool pre = r == tid && n_orig == rw.x;
-        const T rhs = pre ? n_rhs : (a.scale ? a.scale[rw.x] * a.src[rw.x] : a.src[rw.x]);
+        const T rhs = pre ? (a.scale ? n_sc * n_src : n_src)
+                          : (a.scale ? a.scale[rw.x] * a.src[rw.x] : a.src[rw.x]);
         T acc = T(0);
         for (int e = 0; e < rw.z; ++e) {
           const int c = code[rw.y + e];
@@ -178,7 +182,12 @@ __global__ void __launch_bounds__(kBlkThreads, 1) k_trsv_blk(BlkArgs<T> a) {
         ring[rw.w & a.wmask] = t;
         Bits<T>::store(a.cur + rw.x, Bits<T>::canon(t));
         if (a.other) Bits<T>::store(a.other + rw.x, Sentinel<T>::value());
-        if (a.out) a.out[rw.x] = (a.beta == T(0)) ? a.alpha * t : fma(a.beta, a.out[rw.x], a.alpha * t);
+        if (a.out) {
+          if (a.beta == T(0))
+            a.out[rw.x] = a.alpha * t;
+          else
+            a.out[rw.x] = fma(a.beta, pre ? n_out : a.out[rw.x], a.alpha * t);
+        }
       }
     }
     // the next step's stage, then this thread's row of it
