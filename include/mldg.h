@@ -293,6 +293,22 @@ int mldg_profile_multi(mldg_handle *h, char trans, int nrhs, int max, mldg_kerne
 int mldg_relres_noalloc(mldg_handle *h, const mldg_csr *A, const double *x, const double *b,
                         double *relres);
 
+/* ---- hierarchy set-up on the GPU --------------------------------------- */
+/* ILU(0) factorisation of A (0-based CSR, n x n, ascending columns) on the
+ * GPU, bit for bit the reference's row-by-row factorisation
+ * (mlprec/impl/mld_dilu0_fact.f90:284-477 with the row split of ilu_copyin
+ * :551-660): L unit lower (strict part stored), U unit upper (strict part,
+ * rows scaled by 1/pivot), d = 1/pivot -- the MLDG_SMOOTHER_BJAC data of
+ * mldg_level_desc.  Rows of one dependency level are factorised together,
+ * each in the host's operation order without fused multiply-adds.  Host
+ * arrays: Lirp, Uirp n + 1; Lja, Lval, Uja, Uval room for nnz(A) entries; d
+ * n.  Returns MLDG_SUCCESS, or 2 with *bad_row = the first row whose pivot
+ * is below 1.11e-16 (the reference's "pivot too small", :436-445), or an
+ * error code.  *ms (optional): device time.  Allocates its own device
+ * scratch (freed before return) and does not need a handle. */
+int mldg_ilu0_factor(int device, const mldg_csr *A, int32_t *Lirp, int32_t *Lja, double *Lval, int32_t *Uirp,
+                     int32_t *Uja, double *Uval, double *d, int *bad_row, double *ms);
+
 const char *mldg_last_error(const mldg_handle *h);
 
 /* replaces: prec%free (mlprec/mld_d_prec_type.f90:537-568) */

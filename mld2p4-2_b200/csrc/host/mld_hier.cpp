@@ -8,7 +8,12 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <string>
+
+#include "mldg.h"
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -302,6 +307,40 @@ void smoothed_aggr_asb(const CSR &a, const std::vector<int> &ilaggr, int naggr, 
 }
 
 // ILU(0), mlprec/impl/mld_dilu0_fact.f90:284-477 (ialg = ILU_N)
+// The same factorisation on a CUDA device (mldg_ilu0_factor): 0, 1 + the
+// row whose pivot is too small, or -1 with msg set on a CUDA error.
+int ilu0_factor_gpu(const CSR &a, CSR &L, CSR &U, std::vector<double> &d, int device, std::string &msg) {
+  const int m = a.nr;
+  const int64_t nz = (int64_t)a.irp[m];
+  L = CSR();
+  U = CSR();
+  L.nr = L.nc = U.nr = U.nc = m;
+  L.irp.assign((size_t)m + 1, 0);
+  U.irp.assign((size_t)m + 1, 0);
+  L.ja.resize((size_t)std::max<int64_t>(nz, 1));
+  L.val.resize((size_t)std::max<int64_t>(nz, 1));
+  U.ja.resize((size_t)std::max<int64_t>(nz, 1));
+  U.val.resize((size_t)std::max<int64_t>(nz, 1));
+  d.assign((size_t)m, 0.0);
+  mldg_csr c{m, m, a.irp.data(), a.ja.data(), a.val.data()};
+  int bad = -1;
+  double ms = 0;
+  const int rc = mldg_ilu0_factor(device, &c, L.irp.data(), L.ja.data(), L.val.data(), U.irp.data(), U.ja.data(),
+                                  U.val.data(), d.data(), &bad, &ms);
+  if (rc == 2) return 1 + bad;
+  if (rc != 0) {
+    msg = "ILU(0) on the GPU failed (code " + std::to_string(rc) + ")";
+    return -1;
+  }
+  L.ja.resize((size_t)L.irp[m]);
+  L.val.resize((size_t)L.irp[m]);
+  U.ja.resize((size_t)U.irp[m]);
+  U.val.resize((size_t)U.irp[m]);
+  if (std::getenv("MLDG_TIMING"))
+    std::fprintf(stderr, "mldg timing: ILU(0) on the GPU, n=%d: %.3f ms device\n", m, ms);
+  return 0;
+}
+
 int ilu0_factor(const CSR &a, CSR &L, CSR &U, std::vector<double> &d) {
   const int m = a.nr;
   L = CSR();
@@ -451,7 +490,9 @@ int smoothers_build(std::vector<Level> &lv, const Parms &p, std::string &msg) {
       for (double &v : L.d) v = (v == 0.0) ? 1.0 : 1.0 / v;
     } else if (L.kind == SM_BJAC) {
       // one rank: the off-block part (columns > nrow) is empty
-      const int rc = ilu0_factor(a, L.L, L.U, L.d);
+      const int rc = p.ilu_device >= 0 ? ilu0_factor_gpu(a, L.L, L.U, L.d, p.ilu_device, msg)
+                                       : ilu0_factor(a, L.L, L.U, L.d);
+      if (rc < 0) return 2;
       if (rc != 0) {
         msg = "ILU(0): pivot too small at level " + std::to_string(l) + " row " + std::to_string(rc - 1);
         return 2;

@@ -37,6 +37,9 @@ struct Parms {
   // coarsest level
   int coarse_solver = SM_BJAC;
   int coarse_sweeps = 1;
+  // extension: >= 0 runs the ILU(0) factorisations on this CUDA device
+  // (mldg_ilu0_factor, bit for bit the host's), < 0 on the host
+  int ilu_device = -1;
 };
 
 struct Level {
@@ -70,6 +73,7 @@ int dec_aggregate(const CSR &a, double theta, std::vector<int> &ilaggr, int &nag
 void smoothed_aggr_asb(const CSR &a, const std::vector<int> &ilaggr, int naggr, double &omega,
                        CSR &P, CSR &R, CSR &Ac);
 int ilu0_factor(const CSR &a, CSR &L, CSR &U, std::vector<double> &d);
+int ilu0_factor_gpu(const CSR &a, CSR &L, CSR &U, std::vector<double> &d, int device, std::string &msg);
 CSR transpose(const CSR &a);
 CSR spgemm(const CSR &a, const CSR &b);
 

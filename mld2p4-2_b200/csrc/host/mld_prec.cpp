@@ -211,6 +211,14 @@ static int set_common(mldp_prec *p, const std::string &w, const std::string *sv,
       p->precision = MLDG_PREC_FP32_P16;
     else
       return fail(p, MLDG_ERR_ARG, "set PRECISION: unknown value " + v);
+  } else if (w == "SETUP_DEVICE") {  // extension: HOST | GPU (ILU(0) factorisations on the GPU)
+    const std::string v = sv ? upper(sv->c_str()) : "";
+    if (v == "HOST")
+      p->parms.ilu_device = -1;
+    else if (v == "GPU")
+      p->parms.ilu_device = p->device;
+    else
+      return fail(p, MLDG_ERR_ARG, "set SETUP_DEVICE: unknown value " + v);
   } else {
     return fail(p, MLDG_ERR_ARG, "set: unknown keyword " + w);
   }

@@ -34,6 +34,7 @@
 #include "mldg_trsv_win.cuh"
 #include "mldg_trsv_rep.cuh"
 #include "mldg_trsv_blk.cuh"
+#include "mldg_ilu0.cuh"
 
 namespace mldg {
 
@@ -186,7 +187,7 @@ struct DCSR {
   short *sjd = nullptr;
   int *sja = nullptr;
   int64_t slots = 0;
-  bool sell = false;
+  int sell = 0;  // 0: CSR kernels; 1 or 2: SELL kernels with that many slices per warp iteration
   bool present() const { return irp != nullptr; }
   int64_t idx_bytes() const { return jd ? 2 : 4; }
   int nslice() const { return (nr + 31) / 32; }
@@ -649,11 +650,18 @@ struct EngineT : Engine {
     const int64_t vec = (int64_t)A.nc * sizeof(T) + (int64_t)A.nr * sizeof(T) * (1 + (b ? 1 : 0) + (a2 != T(0) ? 1 : 0));
     if (A.sell) {
       begin(MLDG_KERNEL_SPMV);
-      const int g = blocks_for((int64_t)A.nslice() * 32);
-      if (A.sjd)
-        k_spmv_sell<T, short><<<g, 256, 0, st>>>(A.nr, A.soff, A.sjd, A.sval, v, a1, b, a0, out, a2);
-      else
-        k_spmv_sell<T, int><<<g, 256, 0, st>>>(A.nr, A.soff, A.sja, A.sval, v, a1, b, a0, out, a2);
+      const int g = blocks_for((int64_t)A.nslice() * 32 / A.sell);
+      if (A.sell == 2) {
+        if (A.sjd)
+          k_spmv_sell<T, short, 2><<<g, 256, 0, st>>>(A.nr, A.soff, A.sjd, A.sval, v, a1, b, a0, out, a2);
+        else
+          k_spmv_sell<T, int, 2><<<g, 256, 0, st>>>(A.nr, A.soff, A.sja, A.sval, v, a1, b, a0, out, a2);
+      } else {
+        if (A.sjd)
+          k_spmv_sell<T, short, 1><<<g, 256, 0, st>>>(A.nr, A.soff, A.sjd, A.sval, v, a1, b, a0, out, a2);
+        else
+          k_spmv_sell<T, int, 1><<<g, 256, 0, st>>>(A.nr, A.soff, A.sja, A.sval, v, a1, b, a0, out, a2);
+      }
       end(A.mat_bytes() + vec, A.alg_bytes() + vec);
       return;
     }
@@ -679,13 +687,22 @@ struct EngineT : Engine {
     if (ND.sell) {
       const int64_t vec = (int64_t)ND.nr * sizeof(T) * (3 + (first ? 0 : 1) + (beta != T(0) ? 1 : 0));
       begin(MLDG_KERNEL_JACOBI);
-      const int g = blocks_for((int64_t)ND.nslice() * 32);
-      if (ND.sjd)
-        k_jacobi_sell<T, short><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sjd, ND.sval, d, x, ty, first, omega,
-                                                   alpha, beta, out);
-      else
-        k_jacobi_sell<T, int><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sja, ND.sval, d, x, ty, first, omega,
-                                                 alpha, beta, out);
+      const int g = blocks_for((int64_t)ND.nslice() * 32 / ND.sell);
+      if (ND.sell == 2) {
+        if (ND.sjd)
+          k_jacobi_sell<T, short, 2><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sjd, ND.sval, d, x, ty, first, omega,
+                                                        alpha, beta, out);
+        else
+          k_jacobi_sell<T, int, 2><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sja, ND.sval, d, x, ty, first, omega,
+                                                      alpha, beta, out);
+      } else {
+        if (ND.sjd)
+          k_jacobi_sell<T, short, 1><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sjd, ND.sval, d, x, ty, first, omega,
+                                                        alpha, beta, out);
+        else
+          k_jacobi_sell<T, int, 1><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sja, ND.sval, d, x, ty, first, omega,
+                                                      alpha, beta, out);
+      }
       end(ND.mat_bytes() + vec, ND.alg_bytes() + vec);
       return;
     }
@@ -1278,12 +1295,13 @@ struct EngineT : Engine {
         T *v = scratch_for(nmax, 0), *o = scratch_for(nmax, 1);
         float best = 1e30f;
         int best_t = op->tpr;
-        bool best_sell = false;
-        // candidates: CSR with 1..32 lanes per row, then the SELL copy (t = 0)
-        for (int t : {1, 2, 4, 8, 16, 32, 0}) {
-          if (t == 0 && !op->soff) continue;
-          op->sell = t == 0;
-          if (t) op->tpr = t;
+        int best_sell = 0;
+        // candidates: CSR with 1..32 lanes per row, then the SELL copy with 1
+        // and 2 slices per warp iteration (t = -1, -2)
+        for (int t : {1, 2, 4, 8, 16, 32, -1, -2}) {
+          if (t < 0 && !op->soff) continue;
+          op->sell = t < 0 ? -t : 0;
+          if (t > 0) op->tpr = t;
           spmv(*op, v, T(1), nullptr, T(0), o, T(0));  // warm
           MLDG_CUDA(cudaEventRecord(e0, st));
           for (int r = 0; r < reps; ++r) spmv(*op, v, T(1), nullptr, T(0), o, T(0));
@@ -1293,12 +1311,12 @@ struct EngineT : Engine {
           MLDG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
           if (ms < best) {
             best = ms;
-            best_t = t ? t : best_t;
-            best_sell = t == 0;
+            best_t = t > 0 ? t : best_t;
+            best_sell = t < 0 ? -t : 0;
           }
         }
         op->tpr = best_t;
-        op->sell = best_sell || (op->soff && std::getenv("MLDG_SELL_FORCE"));
+        op->sell = best_sell;
       }
     }
     launches = 0;
@@ -3678,6 +3696,11 @@ static Engine *make_engine(Handle *h) {
         L.rep = false;
         L.ell1 = false;
       }
+  // MLDG_SELL_FORCE: every operator with a SELL copy uses it (measurement aid)
+  if (std::getenv("MLDG_SELL_FORCE"))
+    for (auto &L : e->lv)
+      for (DCSR<T> *op : {&L.A, &L.AT, &L.P, &L.R, &L.ND, &L.NDT})
+        if (op->soff && !op->sell) op->sell = std::atoi(std::getenv("MLDG_SELL_FORCE")) == 2 ? 2 : 1;
   tick("autotune solves");
   if (!std::getenv("MLDG_NO_DENSE_INV"))
     for (int l = 1; l < h->nlev; ++l) {
@@ -3783,6 +3806,7 @@ static void finalize(Handle *h, int nlev, int precision) {
   h->finalized = true;
   h->serial = next_serial();
   if (h->opts.autotune && !std::getenv("MLDG_NO_AUTOTUNE")) tune_krylov_spmv(h);
+  if (std::getenv("MLDG_SELL_FORCE")) h->A0.sell = h->A0.soff != nullptr ? 1 : 0;
 }
 
 static bool kcycle_handle(const Handle *h) { return h->cycle == MLDG_CYCLE_K || h->cycle == MLDG_CYCLE_KSYM; }
@@ -4063,11 +4087,11 @@ static void tune_krylov_spmv(Handle *h) {
   MLDG_CUDA(cudaEventCreate(&e1));
   float best = 1e30f;
   int best_t = A.tpr;
-  bool best_sell = false;
+  int best_sell = 0;
   for (double *v : {h->kd, h->kd1, h->kq}) MLDG_CUDA(cudaMemsetAsync(v, 0, sizeof(double) * (size_t)h->n0, h->st));
   for (int t : {1, 2, 4, 8, 16, 32, 0}) {
     if (t == 0 && !A.soff) continue;
-    A.sell = t == 0;
+    A.sell = t == 0 ? 1 : 0;
     if (t) A.tpr = t;
     *h->hkst = s0;
     MLDG_CUDA(cudaMemcpyAsync(h->kst, h->hkst, sizeof(KState), cudaMemcpyHostToDevice, h->st));
@@ -4081,11 +4105,11 @@ static void tune_krylov_spmv(Handle *h) {
     if (ms < best) {
       best = ms;
       best_t = t ? t : best_t;
-      best_sell = t == 0;
+      best_sell = t == 0 ? 1 : 0;
     }
   }
   A.tpr = best_t;
-  A.sell = best_sell || (A.soff && std::getenv("MLDG_SELL_FORCE"));
+  A.sell = best_sell;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   // leave clean vectors behind
@@ -5102,6 +5126,123 @@ extern "C" void mldg_destroy(mldg_handle *hp) {
 // host emulation of k_trsv_rep.  trans 'N': y = U^{-1} diag(d) L^{-1} x;
 // 'T': y = L^{-T} diag(d) U^{-T} x.  stats[4]: plan violations, steps of the
 // first solve, far entries, plans usable.
+// ---------------------------------------------------------------------------
+// ILU(0) factorisation on the GPU (mldg_ilu0.cuh): rows grouped by the
+// dependency level of L's pattern (computed on the host, one pass), one
+// kernel per level.
+namespace mldg {
+static const double kIluEpsTol = 1.1102230246251565e-16;  // PSBLAS 3.5 d_epstol
+
+static void ilu0_factor_gpu(int device, const mldg_csr *Ac, int32_t *Lirp, int32_t *Lja, double *Lval,
+                            int32_t *Uirp, int32_t *Uja, double *Uval, double *d, int *bad_row, double *ms) {
+  if (!Ac || !Lirp || !Lja || !Lval || !Uirp || !Uja || !Uval || !d || !bad_row)
+    fail(MLDG_ERR_ARG, "null argument");
+  HostCSR a = copy_csr(*Ac, 0, "A", 0);
+  const int n = a.nr;
+  if (a.nc != n) fail(MLDG_ERR_ARG, "A must be square");
+  *bad_row = -1;
+  if (n == 0) {
+    Lirp[0] = Uirp[0] = 0;
+    return;
+  }
+  // dependency levels of L's pattern, rows in level order
+  std::vector<int> lev((size_t)n, 0);
+  int nl = 0;
+  for (int i = 0; i < n; ++i) {
+    int l = 0;
+    for (int k = a.irp[i]; k < a.irp[i + 1]; ++k)
+      if (a.ja[k] < i) l = std::max(l, lev[a.ja[k]] + 1);
+    lev[i] = l;
+    nl = std::max(nl, l + 1);
+  }
+  std::vector<int> lptr((size_t)nl + 1, 0), rows((size_t)n);
+  for (int i = 0; i < n; ++i) lptr[lev[i] + 1]++;
+  for (int l = 0; l < nl; ++l) lptr[l + 1] += lptr[l];
+  {
+    std::vector<int> fillp(lptr.begin(), lptr.end() - 1);
+    for (int i = 0; i < n; ++i) rows[fillp[lev[i]]++] = i;
+  }
+  MLDG_CUDA(cudaSetDevice(device));
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  cudaStream_t st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  MLDG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  Arena ar;
+  try {
+    MLDG_CUDA(cudaEventCreate(&e0));
+    MLDG_CUDA(cudaEventCreate(&e1));
+    MLDG_CUDA(cudaEventRecord(e0, st));
+    int *dirp = ar.upload(a.irp), *dja = ar.upload(a.ja), *drows = ar.upload(rows);
+    double *dval = ar.upload(a.val);
+    int *cl = ar.alloc<int>(n), *cu = ar.alloc<int>(n);
+    const int g = (int)std::min<int64_t>(((int64_t)n + 255) / 256, (int64_t)nsm * 16);
+    k_ilu0_count<<<g, 256, 0, st>>>(n, dirp, dja, cl, cu);
+    std::vector<int> hl((size_t)n), hu((size_t)n);
+    MLDG_CUDA(cudaMemcpyAsync(hl.data(), cl, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+    MLDG_CUDA(cudaMemcpyAsync(hu.data(), cu, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+    MLDG_CUDA(cudaStreamSynchronize(st));
+    Lirp[0] = Uirp[0] = 0;
+    for (int i = 0; i < n; ++i) {
+      Lirp[i + 1] = Lirp[i] + hl[i];
+      Uirp[i + 1] = Uirp[i] + hu[i];
+    }
+    std::vector<int> vl(Lirp, Lirp + n + 1), vu(Uirp, Uirp + n + 1);
+    int *dlirp = ar.upload(vl), *duirp = ar.upload(vu);
+    const size_t nzl = std::max(1, Lirp[n]), nzu = std::max(1, Uirp[n]);
+    int *dlja = ar.alloc<int>(nzl), *duja = ar.alloc<int>(nzu), *dbad = ar.alloc<int>(1);
+    double *dlval = ar.alloc<double>(nzl), *duval = ar.alloc<double>(nzu), *dd = ar.alloc<double>(n);
+    const int big = INT32_MAX;
+    MLDG_CUDA(cudaMemcpyAsync(dbad, &big, sizeof(int), cudaMemcpyHostToDevice, st));
+    k_ilu0_split<<<g, 256, 0, st>>>(n, dirp, dja, dval, dlirp, dlja, dlval, duirp, duja, duval, dd);
+    for (int l = 0; l < nl; ++l) {
+      const int cnt = lptr[l + 1] - lptr[l];
+      const int gl = (int)std::min<int64_t>(((int64_t)cnt + 127) / 128, (int64_t)nsm * 8);
+      k_ilu0_level<<<gl, 128, 0, st>>>(drows, lptr[l], lptr[l + 1], dlirp, dlja, dlval, duirp, duja, duval, dd,
+                                       kIluEpsTol, dbad);
+    }
+    int bad = big;
+    MLDG_CUDA(cudaMemcpyAsync(&bad, dbad, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (Lirp[n] > 0) {
+      MLDG_CUDA(cudaMemcpyAsync(Lja, dlja, sizeof(int) * Lirp[n], cudaMemcpyDeviceToHost, st));
+      MLDG_CUDA(cudaMemcpyAsync(Lval, dlval, sizeof(double) * Lirp[n], cudaMemcpyDeviceToHost, st));
+    }
+    if (Uirp[n] > 0) {
+      MLDG_CUDA(cudaMemcpyAsync(Uja, duja, sizeof(int) * Uirp[n], cudaMemcpyDeviceToHost, st));
+      MLDG_CUDA(cudaMemcpyAsync(Uval, duval, sizeof(double) * Uirp[n], cudaMemcpyDeviceToHost, st));
+    }
+    MLDG_CUDA(cudaMemcpyAsync(d, dd, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    MLDG_CUDA(cudaEventRecord(e1, st));
+    MLDG_CUDA(cudaStreamSynchronize(st));
+    float t = 0;
+    MLDG_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    if (ms) *ms = t;
+    *bad_row = bad == big ? -1 : bad;
+  } catch (...) {
+    cudaStreamSynchronize(st);
+    ar.release();
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaStreamDestroy(st);
+    throw;
+  }
+  ar.release();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamDestroy(st);
+}
+}  // namespace mldg
+
+extern "C" int mldg_ilu0_factor(int device, const mldg_csr *A, int32_t *Lirp, int32_t *Lja, double *Lval,
+                                int32_t *Uirp, int32_t *Uja, double *Uval, double *d, int *bad_row, double *ms) {
+  try {
+    mldg::ilu0_factor_gpu(device, A, Lirp, Lja, Lval, Uirp, Uja, Uval, d, bad_row, ms);
+  } catch (const mldg::Error &e) {
+    return e.code;
+  }
+  return (bad_row && *bad_row >= 0) ? 2 : MLDG_SUCCESS;
+}
+
 extern "C" int mldg_test_set_spin_limit(int device, int polls) {
   const int v = polls < 0 ? mldg::kSpinLimit : polls;
   if (cudaSetDevice(device) != cudaSuccess) return MLDG_ERR_CUDA;

@@ -156,30 +156,51 @@ constexpr int kSellU = 8;
 __device__ __forceinline__ int sell_col(const int *__restrict__ sj, int k, int) { return sj[k]; }
 __device__ __forceinline__ int sell_col(const short *__restrict__ sj, int k, int row) { return row + (int)sj[k]; }
 
-// acc += sum over the row's slots of sv[k] * f(col(k)) for the thread's row
-template <typename T, typename CI, typename F>
-__device__ __forceinline__ T sell_row(const CI *__restrict__ sj, const T *__restrict__ sv, int e0, int e1,
-                                      int row, F f) {
-  T acc = T(0);
-  for (int e = e0; e < e1; e += 32 * kSellU) {
-    T vv[kSellU];
-    int jj[kSellU];
+// acc[s] = sum over the slots of slice sl0 + s (s < S) for the thread's row
+// of that slice, the S slices' loads of each block of kSellU entries issued
+// together (S = 2 doubles the bytes in flight per warp, for short FP32 rows)
+template <typename T, typename CI, int S, typename F>
+__device__ __forceinline__ void sell_rows(const int *__restrict__ soff, const CI *__restrict__ sj,
+                                          const T *__restrict__ sv, int sl0, int ns, int lane, F f,
+                                          T (&acc)[S]) {
+  int e[S], e1[S], row[S];
 #pragma unroll
-    for (int u = 0; u < kSellU; ++u) {
-      const int k = e + 32 * u;
-      const bool ok = k < e1;
-      vv[u] = ok ? sv[k] : T(0);
-      jj[u] = ok ? sell_col(sj, k, row) : 0;
-    }
-#pragma unroll
-    for (int u = 0; u < kSellU; ++u)
-      if (e + 32 * u < e1) acc = fma(vv[u], f(jj[u]), acc);
+  for (int q = 0; q < S; ++q) {
+    const int sl = sl0 + q;
+    const bool ok = sl < ns;
+    e[q] = ok ? soff[sl] + lane : 0;
+    e1[q] = ok ? soff[sl + 1] : 0;
+    row[q] = (sl << 5) + lane;
+    acc[q] = T(0);
   }
-  return acc;
+  for (;;) {
+    bool more = false;
+#pragma unroll
+    for (int q = 0; q < S; ++q) more |= e[q] < e1[q];
+    if (!more) break;
+    T vv[S][kSellU];
+    int jj[S][kSellU];
+#pragma unroll
+    for (int q = 0; q < S; ++q)
+#pragma unroll
+      for (int u = 0; u < kSellU; ++u) {
+        const int k = e[q] + 32 * u;
+        const bool ok = k < e1[q];
+        vv[q][u] = ok ? sv[k] : T(0);
+        jj[q][u] = ok ? sell_col(sj, k, row[q]) : 0;
+      }
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+#pragma unroll
+      for (int u = 0; u < kSellU; ++u)
+        if (e[q] + 32 * u < e1[q]) acc[q] = fma(vv[q][u], f(jj[q][u]), acc[q]);
+      e[q] += 32 * kSellU;
+    }
+  }
 }
 
-// out[i] = a0*b[i] + a1*(A v)[i] + a2*out[i]
-template <typename T, typename CI>
+// out[i] = a0*b[i] + a1*(A v)[i] + a2*out[i]; S slices per warp iteration
+template <typename T, typename CI, int S>
 __global__ void __launch_bounds__(256) k_spmv_sell(int nr, const int *__restrict__ soff,
                                                    const CI *__restrict__ sj, const T *__restrict__ sv,
                                                    const T *__restrict__ v, T a1, const T *__restrict__ b,
@@ -188,21 +209,24 @@ __global__ void __launch_bounds__(256) k_spmv_sell(int nr, const int *__restrict
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   const int ns = (nr + 31) >> 5;
-  for (int sl = warp; sl < ns; sl += nwarps) {
-    const int row = (sl << 5) + lane;
-    const T s = sell_row<T>(sj, sv, soff[sl] + lane, soff[sl + 1], row,
-                            [&](int j) { return __ldg(v + j); });
-    if (row < nr) {
-      T r = a1 * s;
-      if (b) r = fma(a0, b[row], r);
-      if (a2 != T(0)) r = fma(a2, out[row], r);
-      out[row] = r;
+  for (int sl0 = warp * S; sl0 < ns; sl0 += nwarps * S) {
+    T acc[S];
+    sell_rows<T, CI, S>(soff, sj, sv, sl0, ns, lane, [&](int j) { return __ldg(v + j); }, acc);
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+      const int row = ((sl0 + q) << 5) + lane;
+      if (row < nr) {
+        T r = a1 * acc[q];
+        if (b) r = fma(a0, b[row], r);
+        if (a2 != T(0)) r = fma(a2, out[row], r);
+        out[row] = r;
+      }
     }
   }
 }
 
 // the point-Jacobi sweep of k_jacobi on the SELL copy of ND
-template <typename T, typename CI>
+template <typename T, typename CI, int S>
 __global__ void __launch_bounds__(256) k_jacobi_sell(int nr, const int *__restrict__ soff,
                                                      const CI *__restrict__ sj, const T *__restrict__ sv,
                                                      const T *__restrict__ d, const T *__restrict__ x,
@@ -212,27 +236,30 @@ __global__ void __launch_bounds__(256) k_jacobi_sell(int nr, const int *__restri
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   const int ns = (nr + 31) >> 5;
-  for (int sl = warp; sl < ns; sl += nwarps) {
-    const int row = (sl << 5) + lane;
-    T s;
+  for (int sl0 = warp * S; sl0 < ns; sl0 += nwarps * S) {
+    T acc[S];
     if (first)
-      s = sell_row<T>(sj, sv, soff[sl] + lane, soff[sl + 1], row,
-                      [&](int j) { return omega * (__ldg(d + j) * __ldg(x + j)); });
+      sell_rows<T, CI, S>(soff, sj, sv, sl0, ns, lane,
+                          [&](int j) { return omega * (__ldg(d + j) * __ldg(x + j)); }, acc);
     else
-      s = sell_row<T>(sj, sv, soff[sl] + lane, soff[sl + 1], row, [&](int j) { return __ldg(ty + j); });
-    if (row < nr) {
-      const T di = d[row], xi = x[row];
-      const T t = di * (xi - s);
-      T vv;
-      if (omega == T(1)) {
-        vv = t;
-      } else {
-        const T tyi = first ? omega * (di * xi) : ty[row];
-        vv = (T(1) - omega) * tyi + omega * t;
+      sell_rows<T, CI, S>(soff, sj, sv, sl0, ns, lane, [&](int j) { return __ldg(ty + j); }, acc);
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+      const int row = ((sl0 + q) << 5) + lane;
+      if (row < nr) {
+        const T di = d[row], xi = x[row];
+        const T t = di * (xi - acc[q]);
+        T vv;
+        if (omega == T(1)) {
+          vv = t;
+        } else {
+          const T tyi = first ? omega * (di * xi) : ty[row];
+          vv = (T(1) - omega) * tyi + omega * t;
+        }
+        T r = alpha * vv;
+        if (beta != T(0)) r = fma(beta, out[row], r);
+        out[row] = r;
       }
-      T r = alpha * vv;
-      if (beta != T(0)) r = fma(beta, out[row], r);
-      out[row] = r;
     }
   }
 }
@@ -1004,12 +1031,13 @@ __global__ void __launch_bounds__(256) k_kry_spmv_sell(int nr, const int *__rest
   double sdq = 0, sdr = 0;
   for (int sl = warp; sl < ns; sl += nwarps) {
     const int row = (sl << 5) + lane;
-    double s;
+    double acc[1];
     if (first)
-      s = sell_row<double>(sj, sv, soff[sl] + lane, soff[sl + 1], row, [&](int j) { return __ldg(z + j); });
+      sell_rows<double, CI, 1>(soff, sj, sv, sl, ns, lane, [&](int j) { return __ldg(z + j); }, acc);
     else
-      s = sell_row<double>(sj, sv, soff[sl] + lane, soff[sl + 1], row,
-                           [&](int j) { return fma(beta, dold[j], __ldg(z + j)); });
+      sell_rows<double, CI, 1>(soff, sj, sv, sl, ns, lane, [&](int j) { return fma(beta, dold[j], __ldg(z + j)); },
+                               acc);
+    const double s = acc[0];
     if (row < nr) {
       const double di = first ? z[row] : fma(beta, dold[row], z[row]);
       dnew[row] = di;
