@@ -309,6 +309,22 @@ int mldg_relres_noalloc(mldg_handle *h, const mldg_csr *A, const double *x, cons
 int mldg_ilu0_factor(int device, const mldg_csr *A, int32_t *Lirp, int32_t *Lja, double *Lval, int32_t *Uirp,
                      int32_t *Uja, double *Uval, double *d, int *bad_row, double *ms);
 
+/* C = A B (0-based CSR, ascending columns; A m x k, B k x n) on the GPU, bit
+ * for bit the host build's row-by-row (Gustavson) product that stands in for
+ * psb_spspmm in the smoothed prolongator and the Galerkin product
+ * (mlprec/impl/mld_daggrmat_smth_asb.f90:316,345,399): row i takes a_ik in
+ * stored order and, for each, row k of B in stored order; a column's first
+ * contribution is assigned, later ones added, every product and sum rounded
+ * on its own; columns ascending.  One warp per row, lanes across the
+ * distinct columns of a row of B; rows with more than 1,536 distinct
+ * columns are formed on the host in the same order.  *Cirp (m + 1), *Cja,
+ * *Cval (nnz) are allocated by the library (release each with mldg_free);
+ * *ms (optional): device time.  Allocates and frees its own device scratch;
+ * needs no handle. */
+int mldg_spgemm(int device, const mldg_csr *A, const mldg_csr *B, int32_t **Cirp, int32_t **Cja, double **Cval,
+                int *Cnrows, int *Cncols, double *ms);
+void mldg_free(void *p);
+
 const char *mldg_last_error(const mldg_handle *h);
 
 /* replaces: prec%free (mlprec/mld_d_prec_type.f90:537-568) */

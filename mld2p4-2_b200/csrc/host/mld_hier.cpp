@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <stdexcept>
 #include <string>
 
 #include "mldg.h"
@@ -274,7 +275,31 @@ int dec_aggregate(const CSR &a, double theta, std::vector<int> &ilaggr, int &nag
 
 // Smoothed prolongator P = (I - omega D^{-1} A) P_tent, omega = 4/(3 ||D^{-1}A||_inf),
 // R = P^T, Ac = R (A P)   (mlprec/impl/mld_daggrmat_smth_asb.f90:174-401)
-void smoothed_aggr_asb(const CSR &a, const std::vector<int> &ilaggr, int naggr, double &omega,
+// C = A B on a CUDA device (mldg_spgemm), the same arrays as spgemm(a, b)
+static CSR spgemm_dev(const CSR &a, const CSR &b, int device) {
+  mldg_csr ac{a.nr, a.nc, a.irp.data(), a.ja.data(), a.val.data()};
+  mldg_csr bc{b.nr, b.nc, b.irp.data(), b.ja.data(), b.val.data()};
+  int32_t *irp = nullptr, *ja = nullptr;
+  double *val = nullptr, ms = 0;
+  int nr = 0, nc = 0;
+  const int rc = mldg_spgemm(device, &ac, &bc, &irp, &ja, &val, &nr, &nc, &ms);
+  if (rc != 0) throw std::runtime_error("sparse product on the GPU failed (code " + std::to_string(rc) + ")");
+  CSR c;
+  c.nr = nr;
+  c.nc = nc;
+  c.irp.assign(irp, irp + nr + 1);
+  c.ja.assign(ja, ja + c.irp[nr]);
+  c.val.assign(val, val + c.irp[nr]);
+  mldg_free(irp);
+  mldg_free(ja);
+  mldg_free(val);
+  if (std::getenv("MLDG_TIMING"))
+    std::fprintf(stderr, "mldg timing: sparse product on the GPU %d x %d (%d entries): %.3f ms device\n", nr, nc,
+                 c.irp[nr], ms);
+  return c;
+}
+
+void smoothed_aggr_asb(const CSR &a, const std::vector<int> &ilaggr, int naggr, double &omega, int device,
                        CSR &P, CSR &R, CSR &Ac) {
   const int nr = a.nr;
   std::vector<double> dinv = diag_of(a);
@@ -300,6 +325,13 @@ void smoothed_aggr_asb(const CSR &a, const std::vector<int> &ilaggr, int naggr, 
   pt.ja.assign(ilaggr.begin(), ilaggr.end());
   pt.val.assign((size_t)nr, 1.0);
   for (int i = 0; i <= nr; ++i) pt.irp[i] = i;
+  if (device >= 0) {
+    P = spgemm_dev(s, pt, device);
+    CSR ap = spgemm_dev(a, P, device);
+    R = transpose(P);
+    Ac = spgemm_dev(R, ap, device);
+    return;
+  }
   P = spgemm(s, pt);
   CSR ap = spgemm(a, P);
   R = transpose(P);
@@ -449,7 +481,12 @@ int hierarchy_build(const CSR &a, const Parms &p, std::vector<Level> &lv, std::s
     Level &L = lv.back();
     L.ilaggr = std::move(il);
     L.naggr = na;
-    smoothed_aggr_asb(af, L.ilaggr, na, L.omega, L.P, L.R, L.A);
+    try {
+      smoothed_aggr_asb(af, L.ilaggr, na, L.omega, p.setup_device, L.P, L.R, L.A);
+    } catch (const std::exception &e) {
+      msg = e.what();
+      return 2;
+    }
     if (newsz > 0) break;
   }
   return 0;
@@ -490,7 +527,7 @@ int smoothers_build(std::vector<Level> &lv, const Parms &p, std::string &msg) {
       for (double &v : L.d) v = (v == 0.0) ? 1.0 : 1.0 / v;
     } else if (L.kind == SM_BJAC) {
       // one rank: the off-block part (columns > nrow) is empty
-      const int rc = p.ilu_device >= 0 ? ilu0_factor_gpu(a, L.L, L.U, L.d, p.ilu_device, msg)
+      const int rc = p.setup_device >= 0 ? ilu0_factor_gpu(a, L.L, L.U, L.d, p.setup_device, msg)
                                        : ilu0_factor(a, L.L, L.U, L.d);
       if (rc < 0) return 2;
       if (rc != 0) {

@@ -37,9 +37,10 @@ struct Parms {
   // coarsest level
   int coarse_solver = SM_BJAC;
   int coarse_sweeps = 1;
-  // extension: >= 0 runs the ILU(0) factorisations on this CUDA device
-  // (mldg_ilu0_factor, bit for bit the host's), < 0 on the host
-  int ilu_device = -1;
+  // extension: >= 0 runs the sparse products of the smoothed prolongator and
+  // the Galerkin product (mldg_spgemm) and the ILU(0) factorisations
+  // (mldg_ilu0_factor) on this CUDA device, bit for bit the host's; < 0 on the host
+  int setup_device = -1;
 };
 
 struct Level {
@@ -70,7 +71,8 @@ int smoothers_build(std::vector<Level> &lv, const Parms &p, std::string &msg);
 
 // building blocks (exposed for tests)
 int dec_aggregate(const CSR &a, double theta, std::vector<int> &ilaggr, int &naggr);
-void smoothed_aggr_asb(const CSR &a, const std::vector<int> &ilaggr, int naggr, double &omega,
+// device >= 0: the three sparse products on that CUDA device (mldg_spgemm)
+void smoothed_aggr_asb(const CSR &a, const std::vector<int> &ilaggr, int naggr, double &omega, int device,
                        CSR &P, CSR &R, CSR &Ac);
 int ilu0_factor(const CSR &a, CSR &L, CSR &U, std::vector<double> &d);
 int ilu0_factor_gpu(const CSR &a, CSR &L, CSR &U, std::vector<double> &d, int device, std::string &msg);

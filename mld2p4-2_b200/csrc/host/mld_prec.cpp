@@ -211,12 +211,12 @@ static int set_common(mldp_prec *p, const std::string &w, const std::string *sv,
       p->precision = MLDG_PREC_FP32_P16;
     else
       return fail(p, MLDG_ERR_ARG, "set PRECISION: unknown value " + v);
-  } else if (w == "SETUP_DEVICE") {  // extension: HOST | GPU (ILU(0) factorisations on the GPU)
+  } else if (w == "SETUP_DEVICE") {  // extension: HOST | GPU (sparse products and ILU(0) on the GPU)
     const std::string v = sv ? upper(sv->c_str()) : "";
     if (v == "HOST")
-      p->parms.ilu_device = -1;
+      p->parms.setup_device = -1;
     else if (v == "GPU")
-      p->parms.ilu_device = p->device;
+      p->parms.setup_device = p->device;
     else
       return fail(p, MLDG_ERR_ARG, "set SETUP_DEVICE: unknown value " + v);
   } else {

@@ -35,6 +35,7 @@
 #include "mldg_trsv_rep.cuh"
 #include "mldg_trsv_blk.cuh"
 #include "mldg_ilu0.cuh"
+#include "mldg_spgemm.cuh"
 
 namespace mldg {
 
@@ -1288,7 +1289,9 @@ struct EngineT : Engine {
     for (size_t l = 0; l < lv.size(); ++l) {
       Lev &L = lv[l];
       DCSR<T> *ops[6] = {&L.A, &L.AT, &L.P, &L.R, &L.ND, &L.NDT};
-      for (DCSR<T> *op : ops) {
+      const char *names[6] = {"A", "A^T", "P", "R", "ND", "ND^T"};
+      for (int oi = 0; oi < 6; ++oi) {
+        DCSR<T> *op = ops[oi];
         if (!op->present() || op->nr == 0) continue;
         // scratch vectors of this level/its neighbour large enough for nc / nr
         const int nmax = std::max(op->nr, op->nc);
@@ -1317,6 +1320,10 @@ struct EngineT : Engine {
         }
         op->tpr = best_t;
         op->sell = best_sell;
+        if (std::getenv("MLDG_VERBOSE"))
+          std::fprintf(stderr, "mldg: spmv autotune level %zu %-4s n=%d nnz=%lld -> %s%d %.4f ms\n", l,
+                       names[oi], op->nr, (long long)op->nnz, best_sell ? "sell" : "csr tpr ",
+                       best_sell ? best_sell : best_t, best / reps);
       }
     }
     launches = 0;
@@ -3603,11 +3610,15 @@ static Engine *make_engine(Handle *h) {
       }
     }
     tick("replicated-window plans");
-    // partitioned solves (k_trsv_blk) for the ILU(0) levels that keep their solves
+    // partitioned solves (k_trsv_blk) for the ILU(0) levels that keep their
+    // solves: built only on request (MLDG_BLK=1, or MLDG_BLK_FORCE), since on
+    // the pdegen hierarchies measured so far the other solves are faster
+    // (level 0 at idim=160: 2.2 ms per pair vs 1.3 ms; coarse levels far slower)
     {
       int blk_min = 4096;
       if (const char *ev = std::getenv("MLDG_BLK_MIN")) blk_min = std::atoi(ev);
-      if (H.kind == MLDG_SMOOTHER_BJAC && !L.minv && L.n >= blk_min && !std::getenv("MLDG_NO_BLK")) {
+      const bool want = std::getenv("MLDG_BLK") || std::getenv("MLDG_BLK_FORCE");
+      if (want && H.kind == MLDG_SMOOTHER_BJAC && !L.minv && L.n >= blk_min && !std::getenv("MLDG_NO_BLK")) {
         int P = std::min(h->nsm, std::max(1, L.n / 1024));
         if (const char *ev = std::getenv("MLDG_BLK_P")) P = std::max(1, std::atoi(ev));
         HostCSR Lt = transpose(H.L), Ut = transpose(H.U);
@@ -5232,6 +5243,150 @@ static void ilu0_factor_gpu(int device, const mldg_csr *Ac, int32_t *Lirp, int32
   cudaStreamDestroy(st);
 }
 }  // namespace mldg
+
+// ---------------------------------------------------------------------------
+// C = A B on the GPU (mldg_spgemm.cuh), bit for bit the host's Gustavson
+// product; rows with more distinct columns than a warp's table takes are
+// formed on the host with the same operation order.
+namespace mldg {
+static void spgemm_host_row(const HostCSR &a, const HostCSR &b, int i, std::vector<int> &cols,
+                            std::vector<double> &vals) {
+  std::map<int, double> acc;  // column -> value, first contribution assigned
+  for (int ka = a.irp[i]; ka < a.irp[i + 1]; ++ka) {
+    const int k = a.ja[ka];
+    const double av = a.val[ka];
+    for (int kb = b.irp[k]; kb < b.irp[k + 1]; ++kb) {
+      volatile double p = av * b.val[kb];  // one rounding, as the host build (no contraction)
+      auto it = acc.find(b.ja[kb]);
+      if (it == acc.end())
+        acc.emplace(b.ja[kb], (double)p);
+      else
+        it->second = it->second + (double)p;
+    }
+  }
+  cols.clear();
+  vals.clear();
+  for (auto &kv : acc) {
+    cols.push_back(kv.first);
+    vals.push_back(kv.second);
+  }
+}
+
+static void spgemm_gpu(int device, const mldg_csr *Ac, const mldg_csr *Bc, int32_t **cirp, int32_t **cja,
+                       double **cval, int *cnr, int *cnc, double *ms) {
+  HostCSR a = copy_csr(*Ac, 0, "A", 0), b = copy_csr(*Bc, 0, "B", 0);
+  if (a.nc != b.nr) fail(MLDG_ERR_SIZE, "spgemm: A is %d x %d, B is %d x %d", a.nr, a.nc, b.nr, b.nc);
+  const int m = a.nr;
+  MLDG_CUDA(cudaSetDevice(device));
+  static bool attr = false;
+  if (!attr) {
+    MLDG_CUDA(cudaFuncSetAttribute(k_spgemm_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSpgSmem));
+    MLDG_CUDA(cudaFuncSetAttribute(k_spgemm_fill, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSpgSmem));
+    attr = true;
+  }
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  cudaStream_t st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  MLDG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  Arena ar;
+  std::vector<int> irp((size_t)m + 1, 0);
+  std::vector<int> ja;
+  std::vector<double> val;
+  try {
+    MLDG_CUDA(cudaEventCreate(&e0));
+    MLDG_CUDA(cudaEventCreate(&e1));
+    MLDG_CUDA(cudaEventRecord(e0, st));
+    int *dairp = ar.upload(a.irp), *daja = ar.upload(a.ja), *dbirp = ar.upload(b.irp), *dbja = ar.upload(b.ja);
+    double *daval = ar.upload(a.val), *dbval = ar.upload(b.val);
+    int *dcnt = ar.alloc<int>((size_t)std::max(m, 1));
+    const int g = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)m + kSpgWarps - 1) / kSpgWarps, (int64_t)nsm * 8));
+    if (m > 0) k_spgemm_count<<<g, 32 * kSpgWarps, kSpgSmem, st>>>(m, dairp, daja, dbirp, dbja, dcnt);
+    std::vector<int> cnt((size_t)m);
+    if (m > 0) MLDG_CUDA(cudaMemcpyAsync(cnt.data(), dcnt, sizeof(int) * m, cudaMemcpyDeviceToHost, st));
+    MLDG_CUDA(cudaStreamSynchronize(st));
+    // rows left to the host
+    std::vector<int> big;
+    std::vector<std::vector<int>> bcols;
+    std::vector<std::vector<double>> bvals;
+    for (int i = 0; i < m; ++i)
+      if (cnt[i] < 0) big.push_back(i);
+    bcols.resize(big.size());
+    bvals.resize(big.size());
+#pragma omp parallel for schedule(dynamic, 16)
+    for (size_t q = 0; q < big.size(); ++q) spgemm_host_row(a, b, big[q], bcols[q], bvals[q]);
+    for (size_t q = 0; q < big.size(); ++q) cnt[big[q]] = (int)bcols[q].size();
+    for (int i = 0; i < m; ++i) irp[i + 1] = irp[i] + cnt[i];
+    const size_t nnz = (size_t)irp[m];
+    int *dcirp = ar.upload(irp);
+    int *dcja = ar.alloc<int>(std::max<size_t>(nnz, 1));
+    double *dcval = ar.alloc<double>(std::max<size_t>(nnz, 1));
+    // the host rows' counts go back as -1 so the fill pass skips them
+    for (int i : big) cnt[i] = -1;
+    std::vector<int> cflag(cnt);
+    int *dflag = ar.upload(cflag);
+    if (m > 0)
+      k_spgemm_fill<<<g, 32 * kSpgWarps, kSpgSmem, st>>>(m, dairp, daja, daval, dbirp, dbja, dbval, dflag, dcirp,
+                                                         dcja, dcval);
+    ja.resize(nnz);
+    val.resize(nnz);
+    if (nnz) {
+      MLDG_CUDA(cudaMemcpyAsync(ja.data(), dcja, sizeof(int) * nnz, cudaMemcpyDeviceToHost, st));
+      MLDG_CUDA(cudaMemcpyAsync(val.data(), dcval, sizeof(double) * nnz, cudaMemcpyDeviceToHost, st));
+    }
+    MLDG_CUDA(cudaEventRecord(e1, st));
+    MLDG_CUDA(cudaStreamSynchronize(st));
+    float t = 0;
+    MLDG_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    if (ms) *ms = t;
+    for (size_t q = 0; q < big.size(); ++q) {
+      std::copy(bcols[q].begin(), bcols[q].end(), ja.begin() + irp[big[q]]);
+      std::copy(bvals[q].begin(), bvals[q].end(), val.begin() + irp[big[q]]);
+    }
+  } catch (...) {
+    cudaStreamSynchronize(st);
+    ar.release();
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaStreamDestroy(st);
+    throw;
+  }
+  ar.release();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamDestroy(st);
+  // results in malloc'd arrays owned by the caller (mldg_free)
+  *cnr = m;
+  *cnc = b.nc;
+  *cirp = (int32_t *)std::malloc(sizeof(int32_t) * ((size_t)m + 1));
+  *cja = (int32_t *)std::malloc(sizeof(int32_t) * std::max<size_t>(ja.size(), 1));
+  *cval = (double *)std::malloc(sizeof(double) * std::max<size_t>(val.size(), 1));
+  if (!*cirp || !*cja || !*cval) fail(MLDG_ERR_ALLOC, "spgemm: host allocation failed");
+  std::copy(irp.begin(), irp.end(), *cirp);
+  std::copy(ja.begin(), ja.end(), *cja);
+  std::copy(val.begin(), val.end(), *cval);
+}
+}  // namespace mldg
+
+extern "C" int mldg_spgemm(int device, const mldg_csr *A, const mldg_csr *B, int32_t **Cirp, int32_t **Cja,
+                           double **Cval, int *Cnrows, int *Cncols, double *ms) {
+  if (!A || !B || !Cirp || !Cja || !Cval || !Cnrows || !Cncols) return MLDG_ERR_ARG;
+  *Cirp = *Cja = nullptr;
+  *Cval = nullptr;
+  try {
+    mldg::spgemm_gpu(device, A, B, Cirp, Cja, Cval, Cnrows, Cncols, ms);
+  } catch (const mldg::Error &e) {
+    std::free(*Cirp);
+    std::free(*Cja);
+    std::free(*Cval);
+    *Cirp = *Cja = nullptr;
+    *Cval = nullptr;
+    return e.code;
+  }
+  return MLDG_SUCCESS;
+}
+
+extern "C" void mldg_free(void *p) { std::free(p); }
 
 extern "C" int mldg_ilu0_factor(int device, const mldg_csr *A, int32_t *Lirp, int32_t *Lja, double *Lval,
                                 int32_t *Uirp, int32_t *Uja, double *Uval, double *d, int *bad_row, double *ms) {
