@@ -4209,7 +4209,10 @@ static void capture_solve(Handle *h, int method, char trans, const DCSR<double> 
 // (event nodes cannot sit in a conditional body), or the caller passed its
 // own matrix; those run the same kernels with one host check per iteration.
 static bool solve_graphable(const Handle *h, bool own_matrix) {
-  return own_matrix && h->opts.use_graphs && !kcycle_handle(h) && h->probe_kind == 0;
+  // MLDG_NO_SOLVE_GRAPH: host-stepped solves (a profiler cannot see the
+  // kernels of a graph with conditional nodes; the V-cycle graph stays)
+  return own_matrix && h->opts.use_graphs && !kcycle_handle(h) && h->probe_kind == 0 &&
+         !std::getenv("MLDG_NO_SOLVE_GRAPH");
 }
 
 static void krylov(Handle *h, int method, const mldg_csr *Acsr, const double *b, double *x,

@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(32 * kSpgWarps) k_spgemm_fill(int m, const int
         const double p = __dmul_rn(av, bval[kb]);
         bool fresh;
         const int h = spg_slot(mem.keys, bja[kb], &fresh);
-        mem.vals[h] = fresh ? p : __dadd_rn(mem.vals[h], p);
+        if (h >= 0) mem.vals[h] = fresh ? p : __dadd_rn(mem.vals[h], p);  // always: the count pass bounds the row
       }
       __syncwarp();
     }

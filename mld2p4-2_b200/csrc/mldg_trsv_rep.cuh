@@ -242,12 +242,14 @@ __global__ void __launch_bounds__(kRepThreads, 1) k_trsv_rep(RepArgs<T> a) {
     // ---- producer warp: lane 0 copies the plan and arms the value barriers ----
     // Descriptors and value bytes come 32 steps at a time, one step per lane,
     // loaded a chunk ahead; lane 0 takes each step's entries by shuffle.
+    int last_issued = -1;  // lane 0: the last step whose stage copy was issued
     auto issue = [&](int t, int4 d) {
       if (lane != 0 || !live || t >= a.nsteps) return;
       if (t >= D && !mbar_wait(&empty[t % D], (unsigned)(((t - D) / D) & 1))) {
         give_up();
         return;
       }
+      last_issued = t;
       unsigned char *dst = stg + (size_t)(t % D) * a.stage_bytes;
       const int r0a = d.z & ~(PER - 1);
       const int nrc = d.w > 0 ? (d.z + d.w - r0a + PER - 1) / PER : 0;
@@ -305,6 +307,12 @@ __global__ void __launch_bounds__(kRepThreads, 1) k_trsv_rep(RepArgs<T> a) {
       issue(t + D - 1, di);
       prefetch(t + kRepPF, dp);
     }
+    // no bulk copy may still be writing this CTA's shared memory when it
+    // exits: wait (bounded) for the last copy issued into every stage (on the
+    // normal path the compute groups have already seen them all complete)
+    if (lane == 0)
+      for (int t = last_issued - D + 1; t <= last_issued; ++t)
+        if (t >= 0) mbar_wait(&full[t % D], (unsigned)((t / D) & 1));
     cluster_sync();
     return;
   }
@@ -499,8 +507,13 @@ __global__ void __launch_bounds__(kRepThreads, 1) k_trsv_rep(RepArgs<T> a) {
       c_a += t7 - t6;
     }
   }
-  // every value sent to this CTA has landed before it exits
+  // every value sent to this CTA has landed before it exits: one thread waits
+  // (bounded, also after a give-up) on the last phase of every value barrier,
+  // so that no peer's st.async is still in flight into this CTA's memory
   values_ready(a.nsteps - 1);
+  if (tid == 0)
+    for (int t = a.nsteps - MV; t < a.nsteps; ++t)
+      if (t >= 0) rep_wait_cluster(&vbar[t % MV], (unsigned)((t / MV) & 1));
   cluster_sync();
   // far copies read in the last step: every reader is done
   if (a.tail_ptr)

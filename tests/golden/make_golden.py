@@ -7,7 +7,7 @@ Reads the reference's own recorded test data (read-only, this container only):
 and stores them as a compressed CSR npz, so that the tests do not need the
 reference tree at run time.
 
-Usage:  python tests/golden/make_golden.py [/path/to/reference]
+Usage:  python tests/golden/make_golden.py /path/to/reference
 """
 import os
 import sys
@@ -34,4 +34,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py /path/to/reference")
+    main(sys.argv[1])
