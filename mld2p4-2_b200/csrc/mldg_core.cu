@@ -188,7 +188,10 @@ struct DCSR {
   short *sjd = nullptr;
   int *sja = nullptr;
   int64_t slots = 0;
-  int sell = 0;  // 0: CSR kernels; 1 or 2: SELL kernels with that many slices per warp iteration
+  // 0: CSR kernels; 1 or 2: SELL kernels with that many slices per warp
+  // iteration; 3: the software-pipelined SELL SpMV (k_spmv_sellp; the Jacobi
+  // sweep then uses the one-slice form)
+  int sell = 0;
   bool present() const { return irp != nullptr; }
   int64_t idx_bytes() const { return jd ? 2 : 4; }
   int nslice() const { return (nr + 31) / 32; }
@@ -651,8 +654,13 @@ struct EngineT : Engine {
     const int64_t vec = (int64_t)A.nc * sizeof(T) + (int64_t)A.nr * sizeof(T) * (1 + (b ? 1 : 0) + (a2 != T(0) ? 1 : 0));
     if (A.sell) {
       begin(MLDG_KERNEL_SPMV);
-      const int g = blocks_for((int64_t)A.nslice() * 32 / A.sell);
-      if (A.sell == 2) {
+      const int g = blocks_for((int64_t)A.nslice() * 32 / (A.sell == 2 ? 2 : 1));
+      if (A.sell == 3) {
+        if (A.sjd)
+          k_spmv_sellp<T, short><<<g, 256, 0, st>>>(A.nr, A.soff, A.sjd, A.sval, v, a1, b, a0, out, a2);
+        else
+          k_spmv_sellp<T, int><<<g, 256, 0, st>>>(A.nr, A.soff, A.sja, A.sval, v, a1, b, a0, out, a2);
+      } else if (A.sell == 2) {
         if (A.sjd)
           k_spmv_sell<T, short, 2><<<g, 256, 0, st>>>(A.nr, A.soff, A.sjd, A.sval, v, a1, b, a0, out, a2);
         else
@@ -688,7 +696,7 @@ struct EngineT : Engine {
     if (ND.sell) {
       const int64_t vec = (int64_t)ND.nr * sizeof(T) * (3 + (first ? 0 : 1) + (beta != T(0) ? 1 : 0));
       begin(MLDG_KERNEL_JACOBI);
-      const int g = blocks_for((int64_t)ND.nslice() * 32 / ND.sell);
+      const int g = blocks_for((int64_t)ND.nslice() * 32 / (ND.sell == 2 ? 2 : 1));
       if (ND.sell == 2) {
         if (ND.sjd)
           k_jacobi_sell<T, short, 2><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sjd, ND.sval, d, x, ty, first, omega,
@@ -1301,7 +1309,7 @@ struct EngineT : Engine {
         int best_sell = 0;
         // candidates: CSR with 1..32 lanes per row, then the SELL copy with 1
         // and 2 slices per warp iteration (t = -1, -2)
-        for (int t : {1, 2, 4, 8, 16, 32, -1, -2}) {
+        for (int t : {1, 2, 4, 8, 16, 32, -1, -2, -3}) {
           if (t < 0 && !op->soff) continue;
           op->sell = t < 0 ? -t : 0;
           if (t > 0) op->tpr = t;
@@ -3711,7 +3719,10 @@ static Engine *make_engine(Handle *h) {
   if (std::getenv("MLDG_SELL_FORCE"))
     for (auto &L : e->lv)
       for (DCSR<T> *op : {&L.A, &L.AT, &L.P, &L.R, &L.ND, &L.NDT})
-        if (op->soff && !op->sell) op->sell = std::atoi(std::getenv("MLDG_SELL_FORCE")) == 2 ? 2 : 1;
+        if (op->soff) {
+          const int f = std::atoi(std::getenv("MLDG_SELL_FORCE"));
+          op->sell = (f >= 1 && f <= 3) ? f : 1;
+        }
   tick("autotune solves");
   if (!std::getenv("MLDG_NO_DENSE_INV"))
     for (int l = 1; l < h->nlev; ++l) {
@@ -4074,9 +4085,12 @@ static void kry_spmv(Handle *h, const DCSR<double> &A) {
 static void krylov_iteration(Handle *h, const DCSR<double> &A, cudaGraphConditionalHandle hc) {
   const int n = h->n0;
   double *r = h->xin, *z = h->yout;
-  k_kry_beta<<<kRedBlocks, kRedThreads, 0, h->st>>>(n, z, h->kq, r, h->kst, h->kpart);
+  // vector kernels: 8 blocks of 256 threads per SM (64 warps), so that enough
+  // loads are in flight to stream the vectors at HBM bandwidth
+  const int gv = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)n + 255) / 256, (int64_t)h->nsm * 8));
+  k_kry_beta<<<gv, kRedThreads, 0, h->st>>>(n, z, h->kq, r, h->kst, h->kpart);
   kry_spmv(h, A);
-  k_kry_update<<<kRedBlocks, kRedThreads, 0, h->st>>>(n, h->kd, h->kd1, h->kq, h->kx, r, h->kst, h->kpart,
+  k_kry_update<<<gv, kRedThreads, 0, h->st>>>(n, h->kd, h->kd1, h->kq, h->kx, r, h->kst, h->kpart,
                                                       hc);
   h->last_launches += 3;
 }

@@ -225,6 +225,79 @@ __global__ void __launch_bounds__(256) k_spmv_sell(int nr, const int *__restrict
   }
 }
 
+// k_spmv_sell with the slices of a warp software-pipelined: the values and
+// column indices of the warp's next slice (first kSellU entries) and the
+// offsets of the one after are loaded before the current slice's vector
+// gathers and sums, so a warp keeps two slices' loads in flight instead of
+// waiting for each slice's offsets, then its entries, then its gathers.
+template <typename T, typename CI>
+__global__ void __launch_bounds__(256) k_spmv_sellp(int nr, const int *__restrict__ soff,
+                                                    const CI *__restrict__ sj, const T *__restrict__ sv,
+                                                    const T *__restrict__ v, T a1, const T *__restrict__ b,
+                                                    T a0, T *out, T a2) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int ns = (nr + 31) >> 5;
+  int sl = warp;
+  if (sl >= ns) return;
+  auto load = [&](int e, int e1, int row, T (&vv)[kSellU], int (&jj)[kSellU]) {
+#pragma unroll
+    for (int u = 0; u < kSellU; ++u) {
+      const int k = e + 32 * u;
+      const bool ok = k < e1;
+      vv[u] = ok ? sv[k] : T(0);
+      jj[u] = ok ? sell_col(sj, k, row) : 0;
+    }
+  };
+  int ec = soff[sl] + lane, e1c = soff[sl + 1];
+  T vc[kSellU];
+  int jc[kSellU];
+  load(ec, e1c, (sl << 5) + lane, vc, jc);
+  int sn = sl + nwarps;
+  int en = sn < ns ? soff[sn] + lane : 0, e1n = sn < ns ? soff[sn + 1] : 0;
+  for (;;) {
+    // next slice's first block and the offsets of the one after, issued now
+    T vn[kSellU];
+    int jn[kSellU];
+    load(en, e1n, (sn << 5) + lane, vn, jn);
+    const int snn = sn + nwarps;
+    const int enn = snn < ns ? soff[snn] + lane : 0, e1nn = snn < ns ? soff[snn + 1] : 0;
+    // the current slice
+    const int row = (sl << 5) + lane;
+    T acc = T(0);
+#pragma unroll
+    for (int u = 0; u < kSellU; ++u)
+      if (ec + 32 * u < e1c) acc = fma(vc[u], __ldg(v + jc[u]), acc);
+    for (int e = ec + 32 * kSellU; e < e1c; e += 32 * kSellU) {  // slices wider than kSellU
+      T vv[kSellU];
+      int jj[kSellU];
+      load(e, e1c, row, vv, jj);
+#pragma unroll
+      for (int u = 0; u < kSellU; ++u)
+        if (e + 32 * u < e1c) acc = fma(vv[u], __ldg(v + jj[u]), acc);
+    }
+    if (row < nr) {
+      T r = a1 * acc;
+      if (b) r = fma(a0, b[row], r);
+      if (a2 != T(0)) r = fma(a2, out[row], r);
+      out[row] = r;
+    }
+    if (sn >= ns) break;
+    sl = sn;
+    ec = en;
+    e1c = e1n;
+#pragma unroll
+    for (int u = 0; u < kSellU; ++u) {
+      vc[u] = vn[u];
+      jc[u] = jn[u];
+    }
+    sn = snn;
+    en = enn;
+    e1n = e1nn;
+  }
+}
+
 // the point-Jacobi sweep of k_jacobi on the SELL copy of ND
 template <typename T, typename CI, int S>
 __global__ void __launch_bounds__(256) k_jacobi_sell(int nr, const int *__restrict__ soff,

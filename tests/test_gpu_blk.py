@@ -57,8 +57,10 @@ def test_blk_krylov_iterations(mld, orc, monkeypatch):
 
 @pytest.mark.parametrize("smoother,sweeps,damp", [("JACOBI", 2, 0.8), ("BJAC", 1, 1.0)])
 @pytest.mark.parametrize("coef", [ISO, ANISO])
-def test_sell_kernels_match_oracle(mld, orc, monkeypatch, smoother, sweeps, damp, coef):
-    monkeypatch.setenv("MLDG_SELL_FORCE", "1")
+@pytest.mark.parametrize("form", ["1", "2", "3"])
+def test_sell_kernels_match_oracle(mld, orc, monkeypatch, smoother, sweeps, damp, coef, form):
+    """SELL forms: 1 and 2 slices per warp iteration, and the software-pipelined SpMV."""
+    monkeypatch.setenv("MLDG_SELL_FORCE", form)
     a = orc.gen_pde3d(30, 1, coef)
     op = orc.Prec(oracle_params(orc, smoother, sweeps, damp, mcs=300))
     op.build(a)
