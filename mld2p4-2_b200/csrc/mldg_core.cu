@@ -189,8 +189,8 @@ struct DCSR {
   int *sja = nullptr;
   int64_t slots = 0;
   // 0: CSR kernels; 1 or 2: SELL kernels with that many slices per warp
-  // iteration; 3: the software-pipelined SELL SpMV (k_spmv_sellp; the Jacobi
-  // sweep then uses the one-slice form)
+  // iteration; 3: the software-pipelined SELL kernels (k_spmv_sellp,
+  // k_jacobi_sellp)
   int sell = 0;
   bool present() const { return irp != nullptr; }
   int64_t idx_bytes() const { return jd ? 2 : 4; }
@@ -697,7 +697,14 @@ struct EngineT : Engine {
       const int64_t vec = (int64_t)ND.nr * sizeof(T) * (3 + (first ? 0 : 1) + (beta != T(0) ? 1 : 0));
       begin(MLDG_KERNEL_JACOBI);
       const int g = blocks_for((int64_t)ND.nslice() * 32 / (ND.sell == 2 ? 2 : 1));
-      if (ND.sell == 2) {
+      if (ND.sell == 3) {
+        if (ND.sjd)
+          k_jacobi_sellp<T, short><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sjd, ND.sval, d, x, ty, first, omega,
+                                                      alpha, beta, out);
+        else
+          k_jacobi_sellp<T, int><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sja, ND.sval, d, x, ty, first, omega,
+                                                    alpha, beta, out);
+      } else if (ND.sell == 2) {
         if (ND.sjd)
           k_jacobi_sell<T, short, 2><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sjd, ND.sval, d, x, ty, first, omega,
                                                         alpha, beta, out);

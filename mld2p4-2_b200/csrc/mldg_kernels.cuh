@@ -225,16 +225,16 @@ __global__ void __launch_bounds__(256) k_spmv_sell(int nr, const int *__restrict
   }
 }
 
-// k_spmv_sell with the slices of a warp software-pipelined: the values and
+// SELL loop with the slices of a warp software-pipelined: the values and
 // column indices of the warp's next slice (first kSellU entries) and the
 // offsets of the one after are loaded before the current slice's vector
 // gathers and sums, so a warp keeps two slices' loads in flight instead of
 // waiting for each slice's offsets, then its entries, then its gathers.
-template <typename T, typename CI>
-__global__ void __launch_bounds__(256) k_spmv_sellp(int nr, const int *__restrict__ soff,
-                                                    const CI *__restrict__ sj, const T *__restrict__ sv,
-                                                    const T *__restrict__ v, T a1, const T *__restrict__ b,
-                                                    T a0, T *out, T a2) {
+// f(j): the vector entry an entry of column j multiplies; done(row, acc): the
+// epilogue of a row (row < nr).
+template <typename T, typename CI, typename F, typename D>
+__device__ __forceinline__ void sellp_loop(int nr, const int *__restrict__ soff, const CI *__restrict__ sj,
+                                           const T *__restrict__ sv, F f, D done) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -268,21 +268,16 @@ __global__ void __launch_bounds__(256) k_spmv_sellp(int nr, const int *__restric
     T acc = T(0);
 #pragma unroll
     for (int u = 0; u < kSellU; ++u)
-      if (ec + 32 * u < e1c) acc = fma(vc[u], __ldg(v + jc[u]), acc);
+      if (ec + 32 * u < e1c) acc = fma(vc[u], f(jc[u]), acc);
     for (int e = ec + 32 * kSellU; e < e1c; e += 32 * kSellU) {  // slices wider than kSellU
       T vv[kSellU];
       int jj[kSellU];
       load(e, e1c, row, vv, jj);
 #pragma unroll
       for (int u = 0; u < kSellU; ++u)
-        if (e + 32 * u < e1c) acc = fma(vv[u], __ldg(v + jj[u]), acc);
+        if (e + 32 * u < e1c) acc = fma(vv[u], f(jj[u]), acc);
     }
-    if (row < nr) {
-      T r = a1 * acc;
-      if (b) r = fma(a0, b[row], r);
-      if (a2 != T(0)) r = fma(a2, out[row], r);
-      out[row] = r;
-    }
+    if (row < nr) done(row, acc);
     if (sn >= ns) break;
     sl = sn;
     ec = en;
@@ -296,6 +291,49 @@ __global__ void __launch_bounds__(256) k_spmv_sellp(int nr, const int *__restric
     en = enn;
     e1n = e1nn;
   }
+}
+
+template <typename T, typename CI>
+__global__ void __launch_bounds__(256) k_spmv_sellp(int nr, const int *__restrict__ soff,
+                                                    const CI *__restrict__ sj, const T *__restrict__ sv,
+                                                    const T *__restrict__ v, T a1, const T *__restrict__ b,
+                                                    T a0, T *out, T a2) {
+  sellp_loop<T, CI>(
+      nr, soff, sj, sv, [&](int j) { return __ldg(v + j); },
+      [&](int row, T acc) {
+        T r = a1 * acc;
+        if (b) r = fma(a0, b[row], r);
+        if (a2 != T(0)) r = fma(a2, out[row], r);
+        out[row] = r;
+      });
+}
+
+// the Jacobi sweep of k_jacobi_sell, software-pipelined like k_spmv_sellp
+template <typename T, typename CI>
+__global__ void __launch_bounds__(256) k_jacobi_sellp(int nr, const int *__restrict__ soff,
+                                                      const CI *__restrict__ sj, const T *__restrict__ sv,
+                                                      const T *__restrict__ d, const T *__restrict__ x,
+                                                      const T *__restrict__ ty, int first, T omega, T alpha,
+                                                      T beta, T *out) {
+  auto done = [&](int row, T acc) {
+    const T di = d[row], xi = x[row];
+    const T t = di * (xi - acc);
+    T vv;
+    if (omega == T(1)) {
+      vv = t;
+    } else {
+      const T tyi = first ? omega * (di * xi) : ty[row];
+      vv = (T(1) - omega) * tyi + omega * t;
+    }
+    T r = alpha * vv;
+    if (beta != T(0)) r = fma(beta, out[row], r);
+    out[row] = r;
+  };
+  if (first)
+    sellp_loop<T, CI>(
+        nr, soff, sj, sv, [&](int j) { return omega * (__ldg(d + j) * __ldg(x + j)); }, done);
+  else
+    sellp_loop<T, CI>(nr, soff, sj, sv, [&](int j) { return __ldg(ty + j); }, done);
 }
 
 // the point-Jacobi sweep of k_jacobi on the SELL copy of ND

@@ -39,6 +39,7 @@ module mld_d_gpu_prec_mod
     procedure, pass(prec) :: gpu_build => mld_d_gpu_build
     procedure, pass(prec) :: gpu_free  => mld_d_gpu_free
     procedure, pass(prec) :: psb_d_apply2_vect => mld_d_gpu_apply2_vect
+    procedure, pass(prec) :: apply_device => mld_d_gpu_apply_device
   end type mld_d_gpu_prec_type
 
 contains
@@ -241,6 +242,34 @@ contains
       call psb_errpush(info, name, a_err=mldg_error_string(prec%h))
     end if
   end subroutine mld_d_gpu_apply2_vect
+
+  ! The same apply on vectors that already live on the GPU (the device
+  ! addresses of a CUDA-resident PSBLAS vector, e.g. one built with a device
+  ! vmold, mld_dprecbld.f90:72-74): nothing is copied between host and device.
+  ! xdev, ydev: device addresses of n doubles.
+  subroutine mld_d_gpu_apply_device(prec, xdev, ydev, n, info, trans)
+    class(mld_d_gpu_prec_type), intent(inout) :: prec
+    type(c_ptr), intent(in) :: xdev, ydev
+    integer(psb_ipk_), intent(in) :: n
+    integer(psb_ipk_), intent(out) :: info
+    character(len=1), optional :: trans
+    character(kind=c_char) :: trans_
+    character(len=20) :: name = 'mld_d_gpu_apply_dev'
+    integer(c_int) :: rc
+    info = psb_success_
+    if (.not. c_associated(prec%h)) then
+      info = MLDG_ERR_NOT_BUILT
+      call psb_errpush(info, name)
+      return
+    end if
+    trans_ = 'N'
+    if (present(trans)) trans_ = psb_toupper(trans)
+    rc = mldg_apply(prec%h, xdev, ydev, trans_, 1_c_int, int(n, c_int), MLDG_MEM_DEVICE)
+    if (rc /= 0) then
+      info = rc
+      call psb_errpush(info, name, a_err=mldg_error_string(prec%h))
+    end if
+  end subroutine mld_d_gpu_apply_device
 
   subroutine mld_d_gpu_free(prec)
     class(mld_d_gpu_prec_type), intent(inout) :: prec
