@@ -48,29 +48,6 @@ __device__ __forceinline__ void st_relaxed_u32(void *p, unsigned int v) {
   asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Fire-and-forget bulk prefetch of [p, p + bytes) into L2 (sm_90+), issued
-// by one lane for a whole warp.  The streaming kernels below prefetch the
-// data a warp takes in its NEXT grid-stride iteration: DRAM latency then
-// overlaps the current iteration without registers held for the loads (a
-// thread of these kernels has only a few dependent loads in flight, which
-// leaves HBM at ~55 % of its peak).  Start rounded down and end rounded up to
-// 16 bytes; callers pass ranges inside one allocation with 16-byte aligned
-// ends (array bases are 256-byte aligned).
-__device__ __forceinline__ void l2_prefetch(const void *p, unsigned bytes) {
-  if (bytes == 0) return;
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "r"(bytes)
-               : "memory");
-}
-// elements [a, b) of an array of S-byte elements, widened to 16-byte bounds
-// that stay inside [0, n) elements rounded down to 16 bytes
-template <int S>
-__device__ __forceinline__ void l2_prefetch_range(const void *base, long long a, long long b, long long n) {
-  long long lo = (a * S) & ~15ll, hi = ((b * S) + 15) & ~15ll;
-  const long long cap = (n * S) & ~15ll;
-  if (hi > cap) hi = cap;
-  if (hi > lo) l2_prefetch(static_cast<const char *>(base) + lo, (unsigned)(hi - lo));
-}
-
 template <typename T> struct Bits;
 template <> struct Bits<double> {
   typedef unsigned long long U;
@@ -149,12 +126,6 @@ __global__ void __launch_bounds__(256) k_spmv(int nr, const int *__restrict__ ir
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int r0 = warp * RPW; r0 < nr; r0 += nwarps * RPW) {
     const int row = r0 + grp;
-    const int rn = r0 + nwarps * RPW;  // this warp's next row block
-    if (lane == 0 && rn < nr) {
-      const int pa = irp[rn], pb = irp[min(rn + RPW, nr)], nz = irp[nr];
-      l2_prefetch_range<sizeof(T)>(val, pa, pb, nz);
-      l2_prefetch_range<sizeof(CI)>(ja, pa, pb, nz);
-    }
     T s = T(0);
     if (row < nr) {
       const int e = irp[row + 1];
@@ -191,12 +162,7 @@ __device__ __forceinline__ int sell_col(const short *__restrict__ sj, int k, int
 template <typename T, typename CI, int S, typename F>
 __device__ __forceinline__ void sell_rows(const int *__restrict__ soff, const CI *__restrict__ sj,
                                           const T *__restrict__ sv, int sl0, int ns, int lane, F f,
-                                          T (&acc)[S], int snext = -1) {
-  if (lane == 0 && snext >= 0 && snext < ns) {  // the slices this warp takes next
-    const int pa = soff[snext], pb = soff[min(snext + S, ns)], nz = soff[ns];
-    l2_prefetch_range<sizeof(T)>(sv, pa, pb, nz);
-    l2_prefetch_range<sizeof(CI)>(sj, pa, pb, nz);
-  }
+                                          T (&acc)[S]) {
   int e[S], e1[S], row[S];
 #pragma unroll
   for (int q = 0; q < S; ++q) {
@@ -245,7 +211,7 @@ __global__ void __launch_bounds__(256) k_spmv_sell(int nr, const int *__restrict
   const int ns = (nr + 31) >> 5;
   for (int sl0 = warp * S; sl0 < ns; sl0 += nwarps * S) {
     T acc[S];
-    sell_rows<T, CI, S>(soff, sj, sv, sl0, ns, lane, [&](int j) { return __ldg(v + j); }, acc, sl0 + nwarps * S);
+    sell_rows<T, CI, S>(soff, sj, sv, sl0, ns, lane, [&](int j) { return __ldg(v + j); }, acc);
 #pragma unroll
     for (int q = 0; q < S; ++q) {
       const int row = ((sl0 + q) << 5) + lane;
@@ -385,10 +351,9 @@ __global__ void __launch_bounds__(256) k_jacobi_sell(int nr, const int *__restri
     T acc[S];
     if (first)
       sell_rows<T, CI, S>(soff, sj, sv, sl0, ns, lane,
-                          [&](int j) { return omega * (__ldg(d + j) * __ldg(x + j)); }, acc, sl0 + nwarps * S);
+                          [&](int j) { return omega * (__ldg(d + j) * __ldg(x + j)); }, acc);
     else
-      sell_rows<T, CI, S>(soff, sj, sv, sl0, ns, lane, [&](int j) { return __ldg(ty + j); }, acc,
-                          sl0 + nwarps * S);
+      sell_rows<T, CI, S>(soff, sj, sv, sl0, ns, lane, [&](int j) { return __ldg(ty + j); }, acc);
 #pragma unroll
     for (int q = 0; q < S; ++q) {
       const int row = ((sl0 + q) << 5) + lane;
@@ -462,12 +427,6 @@ __global__ void __launch_bounds__(256) k_jacobi(int nr, const int *__restrict__ 
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int r0 = warp * RPW; r0 < nr; r0 += nwarps * RPW) {
     const int row = r0 + grp;
-    const int rn = r0 + nwarps * RPW;  // this warp's next row block
-    if (lane == 0 && rn < nr) {
-      const int pa = irp[rn], pb = irp[min(rn + RPW, nr)], nz = irp[nr];
-      l2_prefetch_range<sizeof(T)>(val, pa, pb, nz);
-      l2_prefetch_range<sizeof(CI)>(ja, pa, pb, nz);
-    }
     T s = T(0);
     if (row < nr) {
       const int e = irp[row + 1];
@@ -1071,17 +1030,14 @@ __global__ void __launch_bounds__(kRedThreads) k_kry_beta(int n, const double *_
   if (st->done) return;
   const int it = st->it, method = st->method;
   double s = 0;
-  const int stride = gridDim.x * blockDim.x;
-  const double *u = method == 1 ? z : r, *w = method == 1 ? q : z;
-  if (method != 1 || it > 0)
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-      if ((threadIdx.x & 31) == 0 && i + stride < n) {  // this warp's next chunk
-        const long long a = i + stride, b = min(i + stride + 32, n);
-        l2_prefetch_range<8>(u, a, b, n);
-        l2_prefetch_range<8>(w, a, b, n);
-      }
-      s = fma(u[i], w[i], s);
-    }
+  if (method == 1) {
+    if (it > 0)
+      for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        s = fma(z[i], q[i], s);
+  } else {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+      s = fma(r[i], z[i], s);
+  }
   s = block_sum(s, sh);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
   if (kry_last_block(&st->ticket[0])) {
@@ -1125,12 +1081,6 @@ __global__ void __launch_bounds__(256) k_kry_spmv(int nr, const int *__restrict_
   double sdq = 0, sdr = 0;
   for (int r0 = warp * RPW; r0 < nr; r0 += nwarps * RPW) {
     const int row = r0 + grp;
-    const int rn = r0 + nwarps * RPW;  // this warp's next row block
-    if (lane == 0 && rn < nr) {
-      const int pa = irp[rn], pb = irp[min(rn + RPW, nr)], nz = irp[nr];
-      l2_prefetch_range<8>(val, pa, pb, nz);
-      l2_prefetch_range<sizeof(CI)>(ja, pa, pb, nz);
-    }
     double s = 0;
     if (row < nr) {
       const int e = irp[row + 1];
@@ -1194,10 +1144,10 @@ __global__ void __launch_bounds__(256) k_kry_spmv_sell(int nr, const int *__rest
     const int row = (sl << 5) + lane;
     double acc[1];
     if (first)
-      sell_rows<double, CI, 1>(soff, sj, sv, sl, ns, lane, [&](int j) { return __ldg(z + j); }, acc, sl + nwarps);
+      sell_rows<double, CI, 1>(soff, sj, sv, sl, ns, lane, [&](int j) { return __ldg(z + j); }, acc);
     else
       sell_rows<double, CI, 1>(soff, sj, sv, sl, ns, lane, [&](int j) { return fma(beta, dold[j], __ldg(z + j)); },
-                               acc, sl + nwarps);
+                               acc);
     const double s = acc[0];
     if (row < nr) {
       const double di = first ? z[row] : fma(beta, dold[row], z[row]);
@@ -1235,15 +1185,7 @@ __global__ void __launch_bounds__(kRedThreads) k_kry_update(int n, const double 
   const double *__restrict__ d = (it & 1) ? d1 : d0;
   const double alpha = st->alpha;
   double s = 0;
-  const int stride = gridDim.x * blockDim.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    if ((threadIdx.x & 31) == 0 && i + stride < n) {  // this warp's next chunk of the four inputs
-      const long long a = i + stride, b = min(i + stride + 32, n);
-      l2_prefetch_range<8>(d, a, b, n);
-      l2_prefetch_range<8>(q, a, b, n);
-      l2_prefetch_range<8>(x, a, b, n);
-      l2_prefetch_range<8>(r, a, b, n);
-    }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     x[i] = fma(alpha, d[i], x[i]);
     const double ri = fma(-alpha, q[i], r[i]);
     r[i] = ri;
