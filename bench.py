@@ -482,7 +482,7 @@ def run_ours(args, rank, world, local_rank):
     forms = {}
     with Clocks(dev) as clk:
         # the headline form, then the FP64 V-cycle it is compared with
-        order = [args.precision] + [f for f in ("FP64", "FP32", "FP32_P16")
+        order = [args.precision] + [f for f in ("FP64", "FP32", "FP32_P16", "FP32_H16")
                                     if f != args.precision and not (args.no_variants and f != "FP64")]
         sols = {}
         for pr in order:
@@ -587,7 +587,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--idim", type=int, default=160)
-    ap.add_argument("--precision", default="FP32", choices=["FP64", "FP32", "FP32_P16"])
+    ap.add_argument("--precision", default="FP32", choices=["FP64", "FP32", "FP32_P16", "FP32_H16"])
     ap.add_argument("--eps", type=float, default=1e-10)
     ap.add_argument("--sample-its", type=int, default=8,
                     help="reference arm: FCG iterations timed per step (scaled to the full solve)")

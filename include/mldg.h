@@ -55,6 +55,11 @@ extern "C" {
 #define MLDG_PREC_FP32 1         /* FP32 hierarchy and V-cycle                */
 #define MLDG_PREC_FP32_P16 2     /* FP32 V-cycle, FP16 prolongator values with
                                     an FP32 per-row scale                     */
+#define MLDG_PREC_FP32_H16 3     /* FP32 V-cycle, FP16 values with an FP32
+                                    per-row scale for every level's A, P, R
+                                    and Jacobi off-diagonal part (the
+                                    single-vector V-cycle; multi-RHS and the
+                                    triangular factors read FP32 values)     */
 
 /* ---- memory kinds for vector arguments ---------------------------------- */
 #define MLDG_MEM_HOST 0

@@ -30,7 +30,7 @@ SMOOTHER_JACOBI = 1
 SMOOTHER_BJAC = 2
 SMOOTHER_FBGS = 3
 CYCLE_V, CYCLE_W, CYCLE_K, CYCLE_KSYM, CYCLE_ADD = 0, 1, 2, 3, 4
-PREC_FP64, PREC_FP32, PREC_FP32_P16 = 0, 1, 2
+PREC_FP64, PREC_FP32, PREC_FP32_P16, PREC_FP32_H16 = 0, 1, 2, 3
 MEM_HOST, MEM_DEVICE = 0, 1
 
 ERR_NOT_BUILT = 3112

@@ -201,7 +201,7 @@ static int set_common(mldp_prec *p, const std::string &w, const std::string *sv,
     need("EIG_EST");
   } else if (w == "AGGR_EIG") {
     need("MAX_NORM");
-  } else if (w == "PRECISION") {  // extension: FP64 | FP32 | FP32_P16
+  } else if (w == "PRECISION") {  // extension: FP64 | FP32 | FP32_P16 | FP32_H16
     const std::string v = sv ? upper(sv->c_str()) : "";
     if (v == "FP64")
       p->precision = MLDG_PREC_FP64;
@@ -209,6 +209,8 @@ static int set_common(mldp_prec *p, const std::string &w, const std::string *sv,
       p->precision = MLDG_PREC_FP32;
     else if (v == "FP32_P16")
       p->precision = MLDG_PREC_FP32_P16;
+    else if (v == "FP32_H16")
+      p->precision = MLDG_PREC_FP32_H16;
     else
       return fail(p, MLDG_ERR_ARG, "set PRECISION: unknown value " + v);
   } else if (w == "SETUP_DEVICE") {  // extension: HOST | GPU (sparse products and ILU(0) on the GPU)
@@ -451,7 +453,9 @@ extern "C" int mldp_descr(const mldp_prec *p, char *buf, int len) {
   std::string s = "Multilevel preconditioner (GPU V-cycle apply)\n";
   char line[256];
   const char *prec = p->precision == MLDG_PREC_FP64 ? "FP64"
-                     : p->precision == MLDG_PREC_FP32 ? "FP32" : "FP32 (FP16 prolongator)";
+                     : p->precision == MLDG_PREC_FP32     ? "FP32"
+                     : p->precision == MLDG_PREC_FP32_P16 ? "FP32 (FP16 prolongator)"
+                                                          : "FP32 (FP16 operator values)";
   std::snprintf(line, sizeof line, "  levels: %zu   V-cycle precision: %s\n", p->lv.size(), prec);
   s += line;
   double opc = 0, nnz0 = p->lv.empty() ? 1 : (double)p->lv[0].A.nnz();

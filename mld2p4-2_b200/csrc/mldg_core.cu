@@ -36,6 +36,7 @@
 #include "mldg_trsv_blk.cuh"
 #include "mldg_ilu0.cuh"
 #include "mldg_spgemm.cuh"
+#include "mldg_spmv_stg.cuh"
 
 namespace mldg {
 
@@ -152,7 +153,9 @@ struct Arena {
   T *alloc(size_t n) {
     void *p = nullptr;
     if (n == 0) n = 1;
-    cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+    // 64 bytes of slack past the end: the staged kernels' bulk copies widen
+    // each slice to 16-byte boundaries (mldg_spmv_stg.cuh)
+    cudaError_t e = cudaMalloc(&p, n * sizeof(T) + 64);
     if (e != cudaSuccess)
       fail(MLDG_ERR_ALLOC, "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
     ptrs.push_back(p);
@@ -172,6 +175,39 @@ struct Arena {
   }
 };
 
+// Staged kernels (mldg_spmv_stg.cuh): dynamic shared memory opted in once
+// per (kernel, size) and the resident CTAs per SM cached.  The engine fills
+// the cache for every (kernel, size) its operators can launch before any
+// stream capture (stg_prepare); a launch that misses it while its stream is
+// being captured fails instead of configuring a kernel under capture.
+template <typename K>
+static int stg_occ(K kern, size_t smem, cudaStream_t st = nullptr) {
+  static std::mutex mu;
+  static std::map<std::pair<const void *, size_t>, int> occ;
+  std::lock_guard<std::mutex> lk(mu);
+  auto key = std::make_pair((const void *)kern, smem);
+  auto it = occ.find(key);
+  if (it != occ.end()) return it->second;
+  if (st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    MLDG_CUDA(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) fail(MLDG_ERR_INTERNAL, "staged kernel not prepared before capture");
+  }
+  int per_sm = 0;
+  MLDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  MLDG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStgThreads, smem));
+  occ[key] = per_sm;
+  return per_sm;
+}
+// a persistent grid of (resident CTAs per SM) x SMs, at most one CTA per tile
+template <typename K, typename... Args>
+static void stg_launch(K kern, size_t smem, int ntiles, int nsm, cudaStream_t st, Args... args) {
+  const int per_sm = stg_occ(kern, smem, st);
+  if (per_sm < 1) fail(MLDG_ERR_INTERNAL, "staged kernel does not fit (%zu bytes of shared memory)", smem);
+  const int grid = std::max(1, std::min(ntiles, per_sm * nsm));
+  kern<<<grid, kStgThreads, smem, st>>>(args...);
+}
+
 template <typename T>
 struct DCSR {
   int nr = 0, nc = 0;
@@ -190,18 +226,32 @@ struct DCSR {
   int64_t slots = 0;
   // 0: CSR kernels; 1 or 2: SELL kernels with that many slices per warp
   // iteration; 3: the software-pipelined SELL kernels (k_spmv_sellp,
-  // k_jacobi_sellp)
+  // k_jacobi_sellp); 4: the staged CSR kernels (k_spmv_stg, k_jacobi_stg)
   int sell = 0;
+  // staged CSR plan (k_spmv_stg, k_jacobi_stg): tiles of consecutive rows
+  // {first row, end row, first entry, end entry}, at most trmax rows and
+  // temax entries each, computed with stpr lanes per row; used when sell == 4
+  int4 *tiles = nullptr;
+  int ntiles = 0, trmax = 0, temax = 0, stpr = 1, stpr0 = 1;
+  // FP16 operator form (float engines only): FP16 copies of val and sval
+  // scaled by rows, a_ij = rs_i * h_ij with rs_i = max_j |a_ij| in FP32;
+  // the single-vector SpMV and Jacobi kernels read these instead of val/sval
+  __half *hval = nullptr, *shval = nullptr;
+  float *rs = nullptr;
   bool present() const { return irp != nullptr; }
+  bool h16() const { return rs != nullptr; }
   int64_t idx_bytes() const { return jd ? 2 : 4; }
+  int64_t val_bytes() const { return h16() ? 2 : (int64_t)sizeof(T); }
+  int64_t scale_bytes() const { return h16() ? 4 * (int64_t)nr : 0; }
   int nslice() const { return (nr + 31) / 32; }
   // bytes of the matrix as the chosen kernel reads it
   int64_t mat_bytes() const {
-    return sell ? slots * (int64_t)(sizeof(T) + idx_bytes()) + 4 * ((int64_t)nslice() + 1)
-                : nnz * (int64_t)(sizeof(T) + idx_bytes()) + 4 * ((int64_t)nr + 1);
+    return ((sell >= 1 && sell <= 3) ? slots * (val_bytes() + idx_bytes()) + 4 * ((int64_t)nslice() + 1)
+                 : nnz * (val_bytes() + idx_bytes()) + 4 * ((int64_t)nr + 1)) +
+           scale_bytes();
   }
-  // algorithmic CSR bytes nnz*(value + index) + 4*(rows + 1)
-  int64_t alg_bytes() const { return nnz * (int64_t)(sizeof(T) + idx_bytes()) + 4 * ((int64_t)nr + 1); }
+  // algorithmic CSR bytes nnz*(value + index) + 4*(rows + 1) (+ the row scales)
+  int64_t alg_bytes() const { return nnz * (val_bytes() + idx_bytes()) + 4 * ((int64_t)nr + 1) + scale_bytes(); }
 };
 
 template <typename T>
@@ -358,8 +408,76 @@ static void build_sell(Arena &ar, const HostCSR &h, DCSR<T> &d) {
   d.slots = slots;
 }
 
+// Staged CSR plan (mldg_spmv_stg.cuh): consecutive rows cut into tiles of
+// at most trmax rows and temax entries (a row longer than temax gets a tile
+// of its own, temax raised to it).  temax: 3072 entries (2048 for FP64
+// values), MLDG_STG_E overrides; trmax: the power of two (32..1024) of rows
+// that holds about temax entries at the mean row length.
 template <typename T>
-static DCSR<T> to_dev(Arena &ar, const HostCSR &h) {
+static void build_stg_plan(Arena &ar, const HostCSR &h, DCSR<T> &d) {
+  if (std::getenv("MLDG_NO_STG") || h.nr == 0 || h.nnz() == 0) return;
+  int emax = sizeof(T) == 8 ? 2048 : 3072;
+  if (const char *e = std::getenv("MLDG_STG_E")) emax = std::max(256, std::min(16384, std::atoi(e)));
+  const double avg = (double)h.nnz() / h.nr;
+  int rmax = 32;
+  while (rmax < 1024 && rmax * avg < emax) rmax *= 2;
+  int maxrow = 0;
+  for (int i = 0; i < h.nr; ++i) maxrow = std::max(maxrow, h.irp[i + 1] - h.irp[i]);
+  if (maxrow > emax) emax = (maxrow + 63) & ~63;
+  // two stages of the widest form (8-byte values and vectors, int32 columns,
+  // four staged vectors) must fit one CTA's shared memory
+  if (2 * stg_smem(stg_layout<double, double, int>(rmax, emax, 1, kStgVecs)) > kStgSmemMax) return;
+  std::vector<int4> tiles;
+  tiles.reserve((size_t)h.nr / rmax + 1);
+  for (int r = 0; r < h.nr;) {
+    int r1 = r + 1;  // a tile holds at least one row (maxrow <= emax)
+    while (r1 < h.nr && r1 - r < rmax && h.irp[r1 + 1] - h.irp[r] <= emax) ++r1;
+    tiles.push_back(make_int4(r, r1, h.irp[r], h.irp[r1]));
+    r = r1;
+  }
+  d.tiles = ar.upload(tiles);
+  d.ntiles = (int)tiles.size();
+  d.trmax = rmax;
+  d.temax = emax;
+  d.stpr = d.stpr0 = pick_tpr(h.nnz(), h.nr);
+}
+
+// FP16 row-scaled copies of a level operator's values (CSR and, when built,
+// SELL order): rs_i = max_j |a_ij| rounded to FP32, h_ij = a_ij / rs_i
+// rounded to FP32 and then to FP16 (round to nearest even), so |h_ij| <= 1.
+template <typename T>
+static void make_h16(Arena &ar, const HostCSR &h, DCSR<T> &d) {
+  std::vector<float> sc((size_t)h.nr, 1.f);
+  std::vector<__half> hv(h.val.size());
+#pragma omp parallel for schedule(static, 4096)
+  for (int i = 0; i < h.nr; ++i) {
+    double mx = 0;
+    for (int k = h.irp[i]; k < h.irp[i + 1]; ++k) mx = std::max(mx, std::fabs(h.val[k]));
+    const float s = mx > 0 ? (float)mx : 1.f;
+    sc[i] = s;
+    for (int k = h.irp[i]; k < h.irp[i + 1]; ++k) hv[k] = __float2half_rn((float)(h.val[k] / (double)s));
+  }
+  d.rs = ar.upload(sc);
+  d.hval = ar.upload(hv);
+  if (d.soff) {
+    // the SELL slots in the order build_sell wrote them (padding: zero)
+    const int ns = d.nslice();
+    std::vector<int> soff((size_t)ns + 1);
+    MLDG_CUDA(cudaMemcpy(soff.data(), d.soff, sizeof(int) * soff.size(), cudaMemcpyDeviceToHost));
+    std::vector<__half> sh((size_t)d.slots, __float2half_rn(0.f));
+#pragma omp parallel for schedule(static, 256)
+    for (int s = 0; s < ns; ++s)
+      for (int lane = 0; lane < 32; ++lane) {
+        const int i = s * 32 + lane;
+        if (i >= h.nr) continue;
+        for (int k = 0; k < h.irp[i + 1] - h.irp[i]; ++k) sh[(size_t)soff[s] + 32 * (size_t)k + lane] = hv[h.irp[i] + k];
+      }
+    d.shval = ar.upload(sh);
+  }
+}
+
+template <typename T>
+static DCSR<T> to_dev(Arena &ar, const HostCSR &h, bool h16 = false) {
   DCSR<T> d;
   if (!h.present()) return d;
   d.nr = h.nr;
@@ -384,6 +502,8 @@ static DCSR<T> to_dev(Arena &ar, const HostCSR &h) {
   d.val = ar.upload(v);
   d.tpr = pick_tpr(d.nnz, d.nr);
   build_sell(ar, h, d);
+  build_stg_plan(ar, h, d);
+  if (h16) make_h16(ar, h, d);
   return d;
 }
 
@@ -651,25 +771,161 @@ struct EngineT : Engine {
     return (int)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)nsm * 16));
   }
   void spmv(const DCSR<T> &A, const T *v, T a1, const T *b, T a0, T *out, T a2) {
+    if constexpr (std::is_same<T, float>::value) {
+      if (A.h16()) {
+        spmv_v<__half>(A, A.hval, A.shval, A.rs, v, a1, b, a0, out, a2);
+        return;
+      }
+    }
+    spmv_v<T>(A, A.val, A.sval, nullptr, v, a1, b, a0, out, a2);
+  }
+  // values of type V (T, or FP16 with the row scales rs)
+  int stg_stages = 4;
+  template <int K, typename F>
+  static void tpr_case(int tpr, F &&f) {
+    if (tpr == K) f(std::integral_constant<int, K>());
+  }
+  template <typename F>
+  void tpr_dispatch(int tpr, F &&f) {
+    if (tpr != 1 && tpr != 2 && tpr != 4 && tpr != 8 && tpr != 16 && tpr != 32) fail(MLDG_ERR_INTERNAL, "bad tpr %d", tpr);
+    tpr_case<1>(tpr, f);
+    tpr_case<2>(tpr, f);
+    tpr_case<4>(tpr, f);
+    tpr_case<8>(tpr, f);
+    tpr_case<16>(tpr, f);
+    tpr_case<32>(tpr, f);
+  }
+  // the staged kernels' bulk copies read every array from a 16-byte boundary
+  static bool al16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+  // ring depth of a launch: the configured stages, fewer if they would not fit
+  template <typename V, typename CI>
+  int stg_fit(const DCSR<T> &A, int nvec) const {
+    int sgs = stg_stages;
+    while (sgs > 2 && stg_smem(stg_layout<T, V, CI>(A.trmax, A.temax, sgs, nvec)) > kStgSmemMax) --sgs;
+    return sgs;
+  }
+  template <typename V, typename CI>
+  StgArgs<T, V, CI> stg_args(const DCSR<T> &A, const CI *cj, const V *val, const float *rs, int nvec) {
+    StgArgs<T, V, CI> a{};
+    a.ntiles = A.ntiles;
+    a.tiles = A.tiles;
+    a.irp = A.irp;
+    a.cj = cj;
+    a.val = val;
+    a.rs = rs;
+    a.L = stg_layout<T, V, CI>(A.trmax, A.temax, stg_fit<V, CI>(A, nvec), nvec);
+    a.err = err;
+    return a;
+  }
+  // fill the staged kernels' launch cache for every (kernel, shared memory)
+  // pair an operator can launch: both kinds, the autotuner's three lanes-per-
+  // row choices, every count of staged vectors
+  template <typename V, typename CI>
+  void stg_prepare_op(const DCSR<T> &A) {
+    for (int sp : {A.stpr0 / 2, A.stpr0, A.stpr0 * 2}) {
+      if (sp < 1 || sp > 32) continue;
+      for (int nv = 0; nv <= kStgVecs; ++nv) {
+        const size_t sm = stg_smem(stg_layout<T, V, CI>(A.trmax, A.temax, stg_fit<V, CI>(A, nv), nv));
+        tpr_dispatch(sp, [&](auto kc) {
+          constexpr int K = decltype(kc)::value;
+          if (nv <= 2) stg_occ(k_spmv_stg<T, V, CI, K>, sm);
+          if (nv >= 2) stg_occ(k_jacobi_stg<T, V, CI, K>, sm);
+        });
+      }
+    }
+  }
+  void stg_prepare() {
+    for (auto &L : lv)
+      for (DCSR<T> *op : {&L.A, &L.AT, &L.P, &L.R, &L.ND, &L.NDT}) {
+        if (!op->tiles) continue;
+        auto go = [&](auto vtag) {
+          using V = typename decltype(vtag)::type;
+          if (op->jd)
+            stg_prepare_op<V, short>(*op);
+          else
+            stg_prepare_op<V, int>(*op);
+        };
+        if constexpr (std::is_same<T, float>::value) {
+          if (op->h16()) {
+            go(std::common_type<__half>());
+            continue;
+          }
+        }
+        go(std::common_type<T>());
+      }
+  }
+  template <typename V>
+  void spmv_stg(const DCSR<T> &A, const V *val, const float *rs, const T *v, T a1, const T *b, T a0, T *out,
+                T a2) {
+    const int nvec = (b ? 1 : 0) + (a2 != T(0) ? 1 : 0);
+    auto go = [&](auto *cj) {
+      using CI = std::remove_const_t<std::remove_pointer_t<decltype(cj)>>;
+      StgArgs<T, V, CI> a = stg_args<V, CI>(A, cj, val, rs, nvec);
+      int q = 0;
+      if (b) a.vec[q++] = b;
+      if (a2 != T(0)) a.vec[q++] = out;
+      tpr_dispatch(A.stpr, [&](auto kc) {
+        stg_launch(k_spmv_stg<T, V, CI, decltype(kc)::value>, stg_smem(a.L), A.ntiles, nsm, st, a, v, a1,
+                   b ? 1 : 0, a0, out, a2);
+      });
+    };
+    if (A.jd)
+      go((const short *)A.jd);
+    else
+      go((const int *)A.ja);
+  }
+  template <typename V>
+  void jacobi_stg(const DCSR<T> &ND, const V *val, const float *rs, const T *d, const T *x, const T *ty, int first,
+                  T omega, T alpha, T beta, T *out) {
+    const bool use_ty = !first && omega != T(1);
+    const int nvec = 2 + (use_ty ? 1 : 0) + (beta != T(0) ? 1 : 0);
+    auto go = [&](auto *cj) {
+      using CI = std::remove_const_t<std::remove_pointer_t<decltype(cj)>>;
+      StgArgs<T, V, CI> a = stg_args<V, CI>(ND, cj, val, rs, nvec);
+      int q = 0;
+      a.vec[q++] = d;
+      a.vec[q++] = x;
+      if (use_ty) a.vec[q++] = ty;
+      if (beta != T(0)) a.vec[q++] = out;
+      tpr_dispatch(ND.stpr, [&](auto kc) {
+        stg_launch(k_jacobi_stg<T, V, CI, decltype(kc)::value>, stg_smem(a.L), ND.ntiles, nsm, st, a, d, x, ty,
+                   first, omega, alpha, beta, out);
+      });
+    };
+    if (ND.jd)
+      go((const short *)ND.jd);
+    else
+      go((const int *)ND.ja);
+  }
+  template <typename V>
+  void spmv_v(const DCSR<T> &A, const V *val, const V *sval, const float *rs, const T *v, T a1, const T *b,
+              T a0, T *out, T a2) {
     const int64_t vec = (int64_t)A.nc * sizeof(T) + (int64_t)A.nr * sizeof(T) * (1 + (b ? 1 : 0) + (a2 != T(0) ? 1 : 0));
-    if (A.sell) {
+    if (A.sell == 4 && al16(A.irp) && al16(A.jd ? (const void *)A.jd : (const void *)A.ja) && al16(val) &&
+        al16(b) && (a2 == T(0) || al16(out))) {
+      begin(MLDG_KERNEL_SPMV);
+      spmv_stg<V>(A, val, rs, v, a1, b, a0, out, a2);
+      end(A.alg_bytes() + vec);
+      return;
+    }
+    if (A.sell >= 1 && A.sell <= 3 && A.soff) {
       begin(MLDG_KERNEL_SPMV);
       const int g = blocks_for((int64_t)A.nslice() * 32 / (A.sell == 2 ? 2 : 1));
       if (A.sell == 3) {
         if (A.sjd)
-          k_spmv_sellp<T, short><<<g, 256, 0, st>>>(A.nr, A.soff, A.sjd, A.sval, v, a1, b, a0, out, a2);
+          k_spmv_sellp<T, short, V><<<g, 256, 0, st>>>(A.nr, A.soff, A.sjd, sval, v, a1, b, a0, out, a2, rs);
         else
-          k_spmv_sellp<T, int><<<g, 256, 0, st>>>(A.nr, A.soff, A.sja, A.sval, v, a1, b, a0, out, a2);
+          k_spmv_sellp<T, int, V><<<g, 256, 0, st>>>(A.nr, A.soff, A.sja, sval, v, a1, b, a0, out, a2, rs);
       } else if (A.sell == 2) {
         if (A.sjd)
-          k_spmv_sell<T, short, 2><<<g, 256, 0, st>>>(A.nr, A.soff, A.sjd, A.sval, v, a1, b, a0, out, a2);
+          k_spmv_sell<T, short, 2, V><<<g, 256, 0, st>>>(A.nr, A.soff, A.sjd, sval, v, a1, b, a0, out, a2, rs);
         else
-          k_spmv_sell<T, int, 2><<<g, 256, 0, st>>>(A.nr, A.soff, A.sja, A.sval, v, a1, b, a0, out, a2);
+          k_spmv_sell<T, int, 2, V><<<g, 256, 0, st>>>(A.nr, A.soff, A.sja, sval, v, a1, b, a0, out, a2, rs);
       } else {
         if (A.sjd)
-          k_spmv_sell<T, short, 1><<<g, 256, 0, st>>>(A.nr, A.soff, A.sjd, A.sval, v, a1, b, a0, out, a2);
+          k_spmv_sell<T, short, 1, V><<<g, 256, 0, st>>>(A.nr, A.soff, A.sjd, sval, v, a1, b, a0, out, a2, rs);
         else
-          k_spmv_sell<T, int, 1><<<g, 256, 0, st>>>(A.nr, A.soff, A.sja, A.sval, v, a1, b, a0, out, a2);
+          k_spmv_sell<T, int, 1, V><<<g, 256, 0, st>>>(A.nr, A.soff, A.sja, sval, v, a1, b, a0, out, a2, rs);
       }
       end(A.mat_bytes() + vec, A.alg_bytes() + vec);
       return;
@@ -677,47 +933,64 @@ struct EngineT : Engine {
     const int g = blocks_for((int64_t)A.nr * A.tpr);
     begin(MLDG_KERNEL_SPMV);
     switch (A.tpr) {
-#define CASE(K)                                                                                  \
-  case K:                                                                                        \
-    if (A.jd)                                                                                    \
-      k_spmv<T, K, short><<<g, 256, 0, st>>>(A.nr, A.irp, A.jd, A.val, v, a1, b, a0, out, a2);  \
-    else                                                                                         \
-      k_spmv<T, K, int><<<g, 256, 0, st>>>(A.nr, A.irp, A.ja, A.val, v, a1, b, a0, out, a2);    \
+#define CASE(K)                                                                                         \
+  case K:                                                                                               \
+    if (A.jd)                                                                                           \
+      k_spmv<T, K, short, V><<<g, 256, 0, st>>>(A.nr, A.irp, A.jd, val, v, a1, b, a0, out, a2, rs);    \
+    else                                                                                                \
+      k_spmv<T, K, int, V><<<g, 256, 0, st>>>(A.nr, A.irp, A.ja, val, v, a1, b, a0, out, a2, rs);      \
     break;
       CASE(1) CASE(2) CASE(4) CASE(8) CASE(16) CASE(32)
 #undef CASE
       default: fail(MLDG_ERR_INTERNAL, "bad tpr %d", A.tpr);
     }
-    end(A.nnz * (int64_t)(sizeof(T) + A.idx_bytes()) + 4 * ((int64_t)A.nr + 1) + (int64_t)A.nc * sizeof(T) +
-        (int64_t)A.nr * sizeof(T) * (1 + (b ? 1 : 0) + (a2 != T(0) ? 1 : 0)));
+    end(A.alg_bytes() + vec);
   }
   void jacobi(const DCSR<T> &ND, const T *d, const T *x, const T *ty, int first, T omega,
               T alpha, T beta, T *out) {
-    if (ND.sell) {
-      const int64_t vec = (int64_t)ND.nr * sizeof(T) * (3 + (first ? 0 : 1) + (beta != T(0) ? 1 : 0));
+    if constexpr (std::is_same<T, float>::value) {
+      if (ND.h16()) {
+        jacobi_v<__half>(ND, ND.hval, ND.shval, ND.rs, d, x, ty, first, omega, alpha, beta, out);
+        return;
+      }
+    }
+    jacobi_v<T>(ND, ND.val, ND.sval, nullptr, d, x, ty, first, omega, alpha, beta, out);
+  }
+  template <typename V>
+  void jacobi_v(const DCSR<T> &ND, const V *val, const V *sval, const float *rs, const T *d, const T *x,
+                const T *ty, int first, T omega, T alpha, T beta, T *out) {
+    const int64_t vec = (int64_t)ND.nr * sizeof(T) * (3 + (first ? 0 : 1) + (beta != T(0) ? 1 : 0));
+    if (ND.sell == 4 && al16(ND.irp) && al16(ND.jd ? (const void *)ND.jd : (const void *)ND.ja) && al16(val) &&
+        al16(d) && al16(x) && al16(ty) && (beta == T(0) || al16(out))) {
+      begin(MLDG_KERNEL_JACOBI);
+      jacobi_stg<V>(ND, val, rs, d, x, ty, first, omega, alpha, beta, out);
+      end(ND.alg_bytes() + vec);
+      return;
+    }
+    if (ND.sell >= 1 && ND.sell <= 3 && ND.soff) {
       begin(MLDG_KERNEL_JACOBI);
       const int g = blocks_for((int64_t)ND.nslice() * 32 / (ND.sell == 2 ? 2 : 1));
       if (ND.sell == 3) {
         if (ND.sjd)
-          k_jacobi_sellp<T, short><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sjd, ND.sval, d, x, ty, first, omega,
-                                                      alpha, beta, out);
+          k_jacobi_sellp<T, short, V><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sjd, sval, d, x, ty, first, omega,
+                                                         alpha, beta, out, rs);
         else
-          k_jacobi_sellp<T, int><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sja, ND.sval, d, x, ty, first, omega,
-                                                    alpha, beta, out);
+          k_jacobi_sellp<T, int, V><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sja, sval, d, x, ty, first, omega,
+                                                       alpha, beta, out, rs);
       } else if (ND.sell == 2) {
         if (ND.sjd)
-          k_jacobi_sell<T, short, 2><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sjd, ND.sval, d, x, ty, first, omega,
-                                                        alpha, beta, out);
+          k_jacobi_sell<T, short, 2, V><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sjd, sval, d, x, ty, first, omega,
+                                                           alpha, beta, out, rs);
         else
-          k_jacobi_sell<T, int, 2><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sja, ND.sval, d, x, ty, first, omega,
-                                                      alpha, beta, out);
+          k_jacobi_sell<T, int, 2, V><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sja, sval, d, x, ty, first, omega,
+                                                         alpha, beta, out, rs);
       } else {
         if (ND.sjd)
-          k_jacobi_sell<T, short, 1><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sjd, ND.sval, d, x, ty, first, omega,
-                                                        alpha, beta, out);
+          k_jacobi_sell<T, short, 1, V><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sjd, sval, d, x, ty, first, omega,
+                                                           alpha, beta, out, rs);
         else
-          k_jacobi_sell<T, int, 1><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sja, ND.sval, d, x, ty, first, omega,
-                                                      alpha, beta, out);
+          k_jacobi_sell<T, int, 1, V><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sja, sval, d, x, ty, first, omega,
+                                                         alpha, beta, out, rs);
       }
       end(ND.mat_bytes() + vec, ND.alg_bytes() + vec);
       return;
@@ -725,21 +998,20 @@ struct EngineT : Engine {
     const int g = blocks_for((int64_t)ND.nr * ND.tpr);
     begin(MLDG_KERNEL_JACOBI);
     switch (ND.tpr) {
-#define CASE(K)                                                                                       \
-  case K:                                                                                             \
-    if (ND.jd)                                                                                        \
-      k_jacobi<T, K, short><<<g, 256, 0, st>>>(ND.nr, ND.irp, ND.jd, ND.val, d, x, ty, first, omega, \
-                                               alpha, beta, out);                                     \
-    else                                                                                              \
-      k_jacobi<T, K, int><<<g, 256, 0, st>>>(ND.nr, ND.irp, ND.ja, ND.val, d, x, ty, first, omega,   \
-                                             alpha, beta, out);                                       \
+#define CASE(K)                                                                                          \
+  case K:                                                                                                \
+    if (ND.jd)                                                                                           \
+      k_jacobi<T, K, short, V><<<g, 256, 0, st>>>(ND.nr, ND.irp, ND.jd, val, d, x, ty, first, omega,    \
+                                                  alpha, beta, out, rs);                                 \
+    else                                                                                                 \
+      k_jacobi<T, K, int, V><<<g, 256, 0, st>>>(ND.nr, ND.irp, ND.ja, val, d, x, ty, first, omega,      \
+                                                alpha, beta, out, rs);                                   \
     break;
       CASE(1) CASE(2) CASE(4) CASE(8) CASE(16) CASE(32)
 #undef CASE
       default: fail(MLDG_ERR_INTERNAL, "bad tpr %d", ND.tpr);
     }
-    end(ND.nnz * (int64_t)(sizeof(T) + ND.idx_bytes()) + 4 * ((int64_t)ND.nr + 1) +
-        (int64_t)ND.nr * sizeof(T) * (3 + (first ? 0 : 1) + (beta != T(0) ? 1 : 0)));
+    end(ND.alg_bytes() + vec);
   }
   void diag(int n, const T *d, const T *x, T alpha, T beta, T *out) {
     begin(MLDG_KERNEL_VEC);
@@ -1296,7 +1568,9 @@ struct EngineT : Engine {
     copy(n, k.xk, L.y);
   }
   // Lanes-per-row autotuner: times k_spmv with every TPR on each level's
-  // operators (A, A^T, P, R, ND, ND^T) and keeps the fastest.
+  // operators (A, A^T, P, R, ND, ND^T) and keeps the fastest.  The
+  // off-diagonal parts of point-Jacobi levels are timed in the sweep that
+  // reads them (k_jacobi, first sweep: two vector gathers per entry).
   void autotune_spmv(int reps) {
     cudaEvent_t e0, e1;
     MLDG_CUDA(cudaEventCreate(&e0));
@@ -1316,13 +1590,29 @@ struct EngineT : Engine {
         int best_sell = 0;
         // candidates: CSR with 1..32 lanes per row, then the SELL copy with 1
         // and 2 slices per warp iteration (t = -1, -2)
-        for (int t : {1, 2, 4, 8, 16, 32, -1, -2, -3}) {
-          if (t < 0 && !op->soff) continue;
-          op->sell = t < 0 ? -t : 0;
+        const bool sweep = oi >= 4 && L.kind == MLDG_SMOOTHER_JACOBI && L.d && op->nr == op->nc;
+        auto run = [&]() {
+          if (sweep)
+            jacobi(*op, L.d, v, nullptr, 1, (T)L.damp, T(1), T(0), o);
+          else
+            spmv(*op, v, T(1), nullptr, T(0), o, T(0));
+        };
+        int best_stpr = op->stpr0;
+        // t = -4, -5, -6: the staged kernels with the mean-length lanes per
+        // row, twice and half that
+        for (int t : {1, 2, 4, 8, 16, 32, -1, -2, -3, -4, -5, -6}) {
+          if (t < 0 && t >= -3 && !op->soff) continue;
+          if (t <= -4) {
+            if (!op->tiles) continue;
+            const int sp = t == -4 ? op->stpr0 : (t == -5 ? op->stpr0 * 2 : op->stpr0 / 2);
+            if (sp < 1 || sp > 32 || (t != -4 && sp == op->stpr0)) continue;
+            op->stpr = sp;
+          }
+          op->sell = t < 0 ? std::min(-t, 4) : 0;
           if (t > 0) op->tpr = t;
-          spmv(*op, v, T(1), nullptr, T(0), o, T(0));  // warm
+          run();  // warm
           MLDG_CUDA(cudaEventRecord(e0, st));
-          for (int r = 0; r < reps; ++r) spmv(*op, v, T(1), nullptr, T(0), o, T(0));
+          for (int r = 0; r < reps; ++r) run();
           MLDG_CUDA(cudaEventRecord(e1, st));
           MLDG_CUDA(cudaEventSynchronize(e1));
           float ms = 0;
@@ -1330,15 +1620,18 @@ struct EngineT : Engine {
           if (ms < best) {
             best = ms;
             best_t = t > 0 ? t : best_t;
-            best_sell = t < 0 ? -t : 0;
+            best_sell = t < 0 ? std::min(-t, 4) : 0;
+            if (t <= -4) best_stpr = op->stpr;
           }
         }
         op->tpr = best_t;
         op->sell = best_sell;
+        op->stpr = best_stpr;
         if (std::getenv("MLDG_VERBOSE"))
           std::fprintf(stderr, "mldg: spmv autotune level %zu %-4s n=%d nnz=%lld -> %s%d %.4f ms\n", l,
-                       names[oi], op->nr, (long long)op->nnz, best_sell ? "sell" : "csr tpr ",
-                       best_sell ? best_sell : best_t, best / reps);
+                       names[oi], op->nr, (long long)op->nnz,
+                       best_sell == 4 ? "staged tpr " : (best_sell ? "sell" : "csr tpr "),
+                       best_sell == 4 ? best_stpr : (best_sell ? best_sell : best_t), best / reps);
       }
     }
     launches = 0;
@@ -3456,6 +3749,7 @@ static Engine *make_engine(Handle *h) {
   e->xin = h->xin;
   e->yout = h->yout;
   e->nsm = h->nsm;
+  if (const char *ev = std::getenv("MLDG_STG_S")) e->stg_stages = std::max(2, std::min(kStgMaxStages, std::atoi(ev)));
   Arena &ar = h->arena;
   e->lv.resize(h->nlev);
   for (int l = 0; l < h->nlev; ++l) {
@@ -3466,13 +3760,14 @@ static Engine *make_engine(Handle *h) {
     L.spre = H.sweeps_pre;
     L.spost = H.sweeps_post;
     L.damp = H.damp;
-    L.A = to_dev<T>(ar, H.A);
+    const bool h16 = std::is_same<T, float>::value && h->precision == MLDG_PREC_FP32_H16;
+    L.A = to_dev<T>(ar, H.A, h16);
     tick("A upload");
-    L.AT = to_dev<T>(ar, transpose(H.A));
+    L.AT = to_dev<T>(ar, transpose(H.A), h16);
     tick("A^T transpose + upload");
     if (l > 0) {
-      L.P = to_dev<T>(ar, H.P);
-      L.R = to_dev<T>(ar, H.R);
+      L.P = to_dev<T>(ar, H.P, h16);
+      L.R = to_dev<T>(ar, H.R, h16);
       if (std::is_same<T, float>::value && h->precision == MLDG_PREC_FP32_P16) {
         // FP16 values with an FP32 per-row scale = max |p_ij| of the row
         std::vector<__half> hv(H.P.val.size());
@@ -3571,8 +3866,8 @@ static Engine *make_engine(Handle *h) {
       }
     }
     if (H.ND.present() && L.nnz_nd > 0) {
-      L.ND = to_dev<T>(ar, H.ND);
-      L.NDT = to_dev<T>(ar, transpose(H.ND));
+      L.ND = to_dev<T>(ar, H.ND, h16);
+      L.NDT = to_dev<T>(ar, transpose(H.ND), h16);
     }
     tick("FBGS factors, ND");
     if (H.kind == MLDG_SMOOTHER_BJAC && l == h->nlev - 1 && h->nlev > 1 && L.n <= kDenseCoarseRows &&
@@ -3690,6 +3985,7 @@ static Engine *make_engine(Handle *h) {
     }
   }
   MLDG_CUDA(cudaStreamSynchronize(h->st));
+  e->stg_prepare();
   if (h->opts.autotune && !std::getenv("MLDG_NO_AUTOTUNE")) {
     int nmax = 1;
     for (auto &L : e->lv) nmax = std::max(nmax, L.n);
@@ -3730,6 +4026,12 @@ static Engine *make_engine(Handle *h) {
           const int f = std::atoi(std::getenv("MLDG_SELL_FORCE"));
           op->sell = (f >= 1 && f <= 3) ? f : 1;
         }
+  // MLDG_STG_FORCE: every operator with a staged plan uses it (lanes per row
+  // from the mean row length unless the autotuner chose)
+  if (std::getenv("MLDG_STG_FORCE"))
+    for (auto &L : e->lv)
+      for (DCSR<T> *op : {&L.A, &L.AT, &L.P, &L.R, &L.ND, &L.NDT})
+        if (op->tiles) op->sell = 4;
   tick("autotune solves");
   if (!std::getenv("MLDG_NO_DENSE_INV"))
     for (int l = 1; l < h->nlev; ++l) {
@@ -3787,7 +4089,8 @@ static void finalize(Handle *h, int nlev, int precision) {
   for (int l = 0; l < nlev; ++l)
     if (!h->host[l].uploaded) fail(MLDG_ERR_ARG, "level %d not uploaded", l);
   for (int l = 0; l < nlev; ++l) check_level(h->host[l], l, l ? &h->host[l - 1] : nullptr);
-  if (precision != MLDG_PREC_FP64 && precision != MLDG_PREC_FP32 && precision != MLDG_PREC_FP32_P16)
+  if (precision != MLDG_PREC_FP64 && precision != MLDG_PREC_FP32 && precision != MLDG_PREC_FP32_P16 &&
+      precision != MLDG_PREC_FP32_H16)
     fail(MLDG_ERR_ARG, "unknown precision %d", precision);
   // drop any previous device state
   for (int t = 0; t < 2; ++t)

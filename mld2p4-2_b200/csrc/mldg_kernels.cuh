@@ -8,6 +8,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace mldg {
 
 // ---------------------------------------------------------------------------
@@ -111,13 +113,58 @@ __device__ __forceinline__ T wait_value(const T *p, int *err) {
 // diagonal: 2 bytes per entry instead of 4 on a bandwidth-bound sweep).
 __device__ __forceinline__ int colof(const int *__restrict__ cj, int k, int) { return cj[k]; }
 __device__ __forceinline__ int colof(const short *__restrict__ cj, int k, int row) { return row + (int)cj[k]; }
+// Stored value of entry k widened to the vector type T: values of the
+// matrix's own type, or FP16 values of a row-scaled copy (the FP16 operator
+// form: a_ij = rs_i * h_ij, rs_i = max_j |a_ij| in FP32), whose row sum the
+// epilogue multiplies by rs_i (row_scaled).
+template <typename T, typename V>
+__device__ __forceinline__ T ldval(const V *__restrict__ p, int64_t k) {
+  if constexpr (std::is_same<V, __half>::value)
+    return (T)__half2float(p[k]);
+  else
+    return p[k];
+}
+template <typename T, typename V>
+__device__ __forceinline__ T row_scaled(T acc, const float *__restrict__ rs, int row) {
+  if constexpr (std::is_same<V, __half>::value)
+    return acc * (T)rs[row];
+  else
+    return acc;
+}
 
-template <typename T, int TPR, typename CI = int>
+// One lane's part of a CSR row sum: entries k = k0, k0 + TPR, ... < e,
+// s = fma(val[k], g(col k), s) in that order from zero.  The loads are
+// issued kCsrU entries at a time (column indices and values, then the
+// gathers g, then the sums), so a long row costs two memory latencies per
+// kCsrU entries instead of two per entry; the sums are the plain loop's.
+constexpr int kCsrU = 4;
+template <typename T, int TPR, typename CI, typename V, typename G>
+__device__ __forceinline__ T csr_lane_sum(int k0, int e, int row, const CI *__restrict__ ja,
+                                          const V *__restrict__ val, G g) {
+  T s = T(0);
+  for (int k = k0; k < e; k += TPR * kCsrU) {
+    T vv[kCsrU], xv[kCsrU];
+#pragma unroll
+    for (int u = 0; u < kCsrU; ++u) {
+      const int kk = k + u * TPR;
+      const bool ok = kk < e;
+      vv[u] = ok ? ldval<T>(val, kk) : T(0);
+      xv[u] = ok ? g(colof(ja, kk, row)) : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kCsrU; ++u)
+      if (k + u * TPR < e) s = fma(vv[u], xv[u], s);
+  }
+  return s;
+}
+
+template <typename T, int TPR, typename CI = int, typename V = T>
 __global__ void __launch_bounds__(256) k_spmv(int nr, const int *__restrict__ irp,
                                               const CI *__restrict__ ja,
-                                              const T *__restrict__ val,
+                                              const V *__restrict__ val,
                                               const T *__restrict__ v, T a1,
-                                              const T *__restrict__ b, T a0, T *out, T a2) {
+                                              const T *__restrict__ b, T a0, T *out, T a2,
+                                              const float *__restrict__ rs = nullptr) {
   constexpr int RPW = 32 / TPR;
   const int lane = threadIdx.x & 31;
   const int sub = lane % TPR;
@@ -127,14 +174,12 @@ __global__ void __launch_bounds__(256) k_spmv(int nr, const int *__restrict__ ir
   for (int r0 = warp * RPW; r0 < nr; r0 += nwarps * RPW) {
     const int row = r0 + grp;
     T s = T(0);
-    if (row < nr) {
-      const int e = irp[row + 1];
-      for (int k = irp[row] + sub; k < e; k += TPR) s = fma(val[k], __ldg(v + colof(ja, k, row)), s);
-    }
+    if (row < nr)
+      s = csr_lane_sum<T, TPR>(irp[row] + sub, irp[row + 1], row, ja, val, [&](int j) { return __ldg(v + j); });
 #pragma unroll
     for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, TPR);
     if (row < nr && sub == 0) {
-      T r = a1 * s;
+      T r = a1 * row_scaled<T, V>(s, rs, row);
       if (b) r = fma(a0, b[row], r);
       if (a2 != T(0)) r = fma(a2, out[row], r);
       out[row] = r;
@@ -159,9 +204,9 @@ __device__ __forceinline__ int sell_col(const short *__restrict__ sj, int k, int
 // acc[s] = sum over the slots of slice sl0 + s (s < S) for the thread's row
 // of that slice, the S slices' loads of each block of kSellU entries issued
 // together (S = 2 doubles the bytes in flight per warp, for short FP32 rows)
-template <typename T, typename CI, int S, typename F>
+template <typename T, typename CI, int S, typename F, typename V>
 __device__ __forceinline__ void sell_rows(const int *__restrict__ soff, const CI *__restrict__ sj,
-                                          const T *__restrict__ sv, int sl0, int ns, int lane, F f,
+                                          const V *__restrict__ sv, int sl0, int ns, int lane, F f,
                                           T (&acc)[S]) {
   int e[S], e1[S], row[S];
 #pragma unroll
@@ -186,7 +231,7 @@ __device__ __forceinline__ void sell_rows(const int *__restrict__ soff, const CI
       for (int u = 0; u < kSellU; ++u) {
         const int k = e[q] + 32 * u;
         const bool ok = k < e1[q];
-        vv[q][u] = ok ? sv[k] : T(0);
+        vv[q][u] = ok ? ldval<T>(sv, k) : T(0);
         jj[q][u] = ok ? sell_col(sj, k, row[q]) : 0;
       }
 #pragma unroll
@@ -200,11 +245,12 @@ __device__ __forceinline__ void sell_rows(const int *__restrict__ soff, const CI
 }
 
 // out[i] = a0*b[i] + a1*(A v)[i] + a2*out[i]; S slices per warp iteration
-template <typename T, typename CI, int S>
+template <typename T, typename CI, int S, typename V = T>
 __global__ void __launch_bounds__(256) k_spmv_sell(int nr, const int *__restrict__ soff,
-                                                   const CI *__restrict__ sj, const T *__restrict__ sv,
+                                                   const CI *__restrict__ sj, const V *__restrict__ sv,
                                                    const T *__restrict__ v, T a1, const T *__restrict__ b,
-                                                   T a0, T *out, T a2) {
+                                                   T a0, T *out, T a2,
+                                                   const float *__restrict__ rs = nullptr) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -216,7 +262,7 @@ __global__ void __launch_bounds__(256) k_spmv_sell(int nr, const int *__restrict
     for (int q = 0; q < S; ++q) {
       const int row = ((sl0 + q) << 5) + lane;
       if (row < nr) {
-        T r = a1 * acc[q];
+        T r = a1 * row_scaled<T, V>(acc[q], rs, row);
         if (b) r = fma(a0, b[row], r);
         if (a2 != T(0)) r = fma(a2, out[row], r);
         out[row] = r;
@@ -232,9 +278,9 @@ __global__ void __launch_bounds__(256) k_spmv_sell(int nr, const int *__restrict
 // waiting for each slice's offsets, then its entries, then its gathers.
 // f(j): the vector entry an entry of column j multiplies; done(row, acc): the
 // epilogue of a row (row < nr).
-template <typename T, typename CI, typename F, typename D>
+template <typename T, typename CI, typename F, typename D, typename V>
 __device__ __forceinline__ void sellp_loop(int nr, const int *__restrict__ soff, const CI *__restrict__ sj,
-                                           const T *__restrict__ sv, F f, D done) {
+                                           const V *__restrict__ sv, F f, D done) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -246,7 +292,7 @@ __device__ __forceinline__ void sellp_loop(int nr, const int *__restrict__ soff,
     for (int u = 0; u < kSellU; ++u) {
       const int k = e + 32 * u;
       const bool ok = k < e1;
-      vv[u] = ok ? sv[k] : T(0);
+      vv[u] = ok ? ldval<T>(sv, k) : T(0);
       jj[u] = ok ? sell_col(sj, k, row) : 0;
     }
   };
@@ -293,15 +339,16 @@ __device__ __forceinline__ void sellp_loop(int nr, const int *__restrict__ soff,
   }
 }
 
-template <typename T, typename CI>
+template <typename T, typename CI, typename V = T>
 __global__ void __launch_bounds__(256) k_spmv_sellp(int nr, const int *__restrict__ soff,
-                                                    const CI *__restrict__ sj, const T *__restrict__ sv,
+                                                    const CI *__restrict__ sj, const V *__restrict__ sv,
                                                     const T *__restrict__ v, T a1, const T *__restrict__ b,
-                                                    T a0, T *out, T a2) {
+                                                    T a0, T *out, T a2,
+                                                    const float *__restrict__ rs = nullptr) {
   sellp_loop<T, CI>(
       nr, soff, sj, sv, [&](int j) { return __ldg(v + j); },
       [&](int row, T acc) {
-        T r = a1 * acc;
+        T r = a1 * row_scaled<T, V>(acc, rs, row);
         if (b) r = fma(a0, b[row], r);
         if (a2 != T(0)) r = fma(a2, out[row], r);
         out[row] = r;
@@ -309,13 +356,14 @@ __global__ void __launch_bounds__(256) k_spmv_sellp(int nr, const int *__restric
 }
 
 // the Jacobi sweep of k_jacobi_sell, software-pipelined like k_spmv_sellp
-template <typename T, typename CI>
+template <typename T, typename CI, typename V = T>
 __global__ void __launch_bounds__(256) k_jacobi_sellp(int nr, const int *__restrict__ soff,
-                                                      const CI *__restrict__ sj, const T *__restrict__ sv,
+                                                      const CI *__restrict__ sj, const V *__restrict__ sv,
                                                       const T *__restrict__ d, const T *__restrict__ x,
                                                       const T *__restrict__ ty, int first, T omega, T alpha,
-                                                      T beta, T *out) {
+                                                      T beta, T *out, const float *__restrict__ rs = nullptr) {
   auto done = [&](int row, T acc) {
+    acc = row_scaled<T, V>(acc, rs, row);
     const T di = d[row], xi = x[row];
     const T t = di * (xi - acc);
     T vv;
@@ -337,12 +385,12 @@ __global__ void __launch_bounds__(256) k_jacobi_sellp(int nr, const int *__restr
 }
 
 // the point-Jacobi sweep of k_jacobi on the SELL copy of ND
-template <typename T, typename CI, int S>
+template <typename T, typename CI, int S, typename V = T>
 __global__ void __launch_bounds__(256) k_jacobi_sell(int nr, const int *__restrict__ soff,
-                                                     const CI *__restrict__ sj, const T *__restrict__ sv,
+                                                     const CI *__restrict__ sj, const V *__restrict__ sv,
                                                      const T *__restrict__ d, const T *__restrict__ x,
                                                      const T *__restrict__ ty, int first, T omega, T alpha,
-                                                     T beta, T *out) {
+                                                     T beta, T *out, const float *__restrict__ rs = nullptr) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -359,7 +407,7 @@ __global__ void __launch_bounds__(256) k_jacobi_sell(int nr, const int *__restri
       const int row = ((sl0 + q) << 5) + lane;
       if (row < nr) {
         const T di = d[row], xi = x[row];
-        const T t = di * (xi - acc[q]);
+        const T t = di * (xi - row_scaled<T, V>(acc[q], rs, row));
         T vv;
         if (omega == T(1)) {
           vv = t;
@@ -411,14 +459,15 @@ __global__ void __launch_bounds__(256) k_spmv_h(int nr, const int *__restrict__ 
 //   out_i = alpha*v_i + beta*out_i
 // When first != 0 the incoming iterate is ty = omega*d o x (the unrolled first
 // sweep, :136), computed on the fly from x and d instead of being stored.
-template <typename T, int TPR, typename CI = int>
+template <typename T, int TPR, typename CI = int, typename V = T>
 __global__ void __launch_bounds__(256) k_jacobi(int nr, const int *__restrict__ irp,
                                                 const CI *__restrict__ ja,
-                                                const T *__restrict__ val,
+                                                const V *__restrict__ val,
                                                 const T *__restrict__ d,
                                                 const T *__restrict__ x,
                                                 const T *__restrict__ ty, int first,
-                                                T omega, T alpha, T beta, T *out) {
+                                                T omega, T alpha, T beta, T *out,
+                                                const float *__restrict__ rs = nullptr) {
   constexpr int RPW = 32 / TPR;
   const int lane = threadIdx.x & 31;
   const int sub = lane % TPR;
@@ -429,19 +478,16 @@ __global__ void __launch_bounds__(256) k_jacobi(int nr, const int *__restrict__ 
     const int row = r0 + grp;
     T s = T(0);
     if (row < nr) {
-      const int e = irp[row + 1];
-      if (first) {
-        for (int k = irp[row] + sub; k < e; k += TPR) {
-          const int j = colof(ja, k, row);
-          s = fma(val[k], omega * (__ldg(d + j) * __ldg(x + j)), s);
-        }
-      } else {
-        for (int k = irp[row] + sub; k < e; k += TPR) s = fma(val[k], __ldg(ty + colof(ja, k, row)), s);
-      }
+      const int k0 = irp[row] + sub, e = irp[row + 1];
+      if (first)
+        s = csr_lane_sum<T, TPR>(k0, e, row, ja, val, [&](int j) { return omega * (__ldg(d + j) * __ldg(x + j)); });
+      else
+        s = csr_lane_sum<T, TPR>(k0, e, row, ja, val, [&](int j) { return __ldg(ty + j); });
     }
 #pragma unroll
     for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, TPR);
     if (row < nr && sub == 0) {
+      s = row_scaled<T, V>(s, rs, row);
       const T di = d[row], xi = x[row];
       T t = di * (xi - s);
       T v;
@@ -1083,15 +1129,11 @@ __global__ void __launch_bounds__(256) k_kry_spmv(int nr, const int *__restrict_
     const int row = r0 + grp;
     double s = 0;
     if (row < nr) {
-      const int e = irp[row + 1];
-      if (first) {
-        for (int k = irp[row] + sub; k < e; k += TPR) s = fma(val[k], __ldg(z + colof(ja, k, row)), s);
-      } else {
-        for (int k = irp[row] + sub; k < e; k += TPR) {
-          const int j = colof(ja, k, row);
-          s = fma(val[k], fma(beta, dold[j], __ldg(z + j)), s);
-        }
-      }
+      const int k0 = irp[row] + sub, e = irp[row + 1];
+      if (first)
+        s = csr_lane_sum<double, TPR>(k0, e, row, ja, val, [&](int j) { return __ldg(z + j); });
+      else
+        s = csr_lane_sum<double, TPR>(k0, e, row, ja, val, [&](int j) { return fma(beta, dold[j], __ldg(z + j)); });
     }
 #pragma unroll
     for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, TPR);

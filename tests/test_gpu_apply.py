@@ -63,10 +63,10 @@ def test_fp32_apply(mld, orc):
     op.build(a)
     x = np.random.default_rng(5).uniform(-1, 1, a.nrows)
     y_ref = op.apply(x)
-    for prec in (mld.PREC_FP32, mld.PREC_FP32_P16):
+    for prec in (mld.PREC_FP32, mld.PREC_FP32_P16, mld.PREC_FP32_H16):
         h = upload_oracle_hierarchy(mld, orc, op, precision=prec)
         y = h.apply(x)
-        tol = TOL_FP32 if prec == mld.PREC_FP32 else 5e-3
+        tol = {mld.PREC_FP32: TOL_FP32, mld.PREC_FP32_P16: 5e-3}.get(prec, 2e-2)
         assert _rel(y, y_ref) <= tol, (prec, _rel(y, y_ref))
 
 

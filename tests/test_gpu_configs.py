@@ -9,14 +9,15 @@ Krylov iteration counts are compared with the oracle's:
       <= 2000 rows, coarsest 4 sweeps of BJAC-ILU(0); CG to 1e-9
   C2  isotropic, idim=160 (4,096,000 rows): BJAC-ILU(0) 1 sweep, and point
       Jacobi 2 sweeps with damping 0.8; FCG to 1e-10
-  C3  anisotropic (0.01 u_zz), idim=160, b uniform[-1,1] (seed 0): the FP32
-      and FP32+FP16-prolongator V-cycles inside FP64 FCG to 1e-10
+  C3  anisotropic (0.01 u_zz), idim=160, b uniform[-1,1] (seed 0): the FP32,
+      FP32+FP16-prolongator and FP16-operator V-cycles inside FP64 FCG to 1e-10
 
 Bars: an FP64 apply within 1e-12 relative of the oracle's apply
 (mld_dmlprec_aply.f90:590-809); iteration counts within +-1; the reduced
-precision applies within 2e-5 (FP32) and 5e-3 (FP16 prolongators) of the
-FP64 oracle apply; the reduced precision solves reach 1e-10 with at most 2
-extra iterations, and their solutions agree with the oracle's FP64 solution.
+precision applies within 2e-5 (FP32), 5e-3 (FP16 prolongators) and 2e-2 (FP16
+operator values) of the FP64 oracle apply; the reduced precision solves reach
+1e-10 with at most 2 extra iterations, and their solutions agree with the
+oracle's FP64 solution.
 """
 import numpy as np
 import pytest
@@ -28,6 +29,7 @@ pytestmark = pytest.mark.gpu
 TOL_FP64 = 1e-12
 TOL_FP32 = 2e-5
 TOL_P16 = 5e-3
+TOL_H16 = 2e-2
 
 
 def _rel(a, b):
@@ -83,7 +85,7 @@ def test_c3_idim160_reduced_precision(mld, orc):
     op.build(a)
     b = np.random.default_rng(0).uniform(-1.0, 1.0, a.nrows)
     x_ref, it_ref, _, _ = orc.krylov("FCG", a, op, b, eps=1e-10)
-    for prec, tol in ((mld.PREC_FP32, TOL_FP32), (mld.PREC_FP32_P16, TOL_P16)):
+    for prec, tol in ((mld.PREC_FP32, TOL_FP32), (mld.PREC_FP32_P16, TOL_P16), (mld.PREC_FP32_H16, TOL_H16)):
         h = upload_oracle_hierarchy(mld, orc, op, precision=prec)
         _check_applies(h, op, a.nrows, 3, tol)
         x, it, rr = h.krylov("FCG", b.copy(), eps=1e-10)
