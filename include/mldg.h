@@ -61,6 +61,10 @@ extern "C" {
                                     single-vector V-cycle; multi-RHS and the
                                     triangular factors read FP32 values)     */
 
+/* ---- Krylov methods of mldg_krylov, mldg_krylov_multi, mldg_krylov_batch */
+#define MLDG_METHOD_CG 0         /* psb_krylov('CG', ...)                     */
+#define MLDG_METHOD_FCG 1        /* psb_krylov('FCG', ...)                    */
+
 /* ---- memory kinds for vector arguments ---------------------------------- */
 #define MLDG_MEM_HOST 0
 #define MLDG_MEM_DEVICE 1

@@ -15,6 +15,7 @@
 #include <chrono>
 #include <cmath>
 #include <map>
+#include <set>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -176,7 +177,8 @@ struct Arena {
 };
 
 // Staged kernels (mldg_spmv_stg.cuh): dynamic shared memory opted in once
-// per (kernel, size) and the resident CTAs per SM cached.  The engine fills
+// per kernel (to the most a CTA may have) and the resident CTAs per SM
+// cached per (kernel, size).  The engine fills
 // the cache for every (kernel, size) its operators can launch before any
 // stream capture (stg_prepare); a launch that misses it while its stream is
 // being captured fails instead of configuring a kernel under capture.
@@ -193,18 +195,21 @@ static int stg_occ(K kern, size_t smem, cudaStream_t st = nullptr) {
     MLDG_CUDA(cudaStreamIsCapturing(st, &cs));
     if (cs != cudaStreamCaptureStatusNone) fail(MLDG_ERR_INTERNAL, "staged kernel not prepared before capture");
   }
+  // the opt-in is one value per kernel: the largest any launch may ask for
+  static std::set<const void *> opted;
+  if (opted.insert((const void *)kern).second)
+    MLDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStgSmemMax));
   int per_sm = 0;
-  MLDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   MLDG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStgThreads, smem));
   occ[key] = per_sm;
   return per_sm;
 }
-// a persistent grid of (resident CTAs per SM) x SMs, at most one CTA per tile
+// a persistent grid of (resident CTAs per SM) x SMs, at most one warp per tile
 template <typename K, typename... Args>
 static void stg_launch(K kern, size_t smem, int ntiles, int nsm, cudaStream_t st, Args... args) {
   const int per_sm = stg_occ(kern, smem, st);
   if (per_sm < 1) fail(MLDG_ERR_INTERNAL, "staged kernel does not fit (%zu bytes of shared memory)", smem);
-  const int grid = std::max(1, std::min(ntiles, per_sm * nsm));
+  const int grid = std::max(1, std::min((ntiles + kStgWarps - 1) / kStgWarps, per_sm * nsm));
   kern<<<grid, kStgThreads, smem, st>>>(args...);
 }
 
@@ -232,7 +237,7 @@ struct DCSR {
   // {first row, end row, first entry, end entry}, at most trmax rows and
   // temax entries each, computed with stpr lanes per row; used when sell == 4
   int4 *tiles = nullptr;
-  int ntiles = 0, trmax = 0, temax = 0, stpr = 1, stpr0 = 1;
+  int ntiles = 0, trmax = 0, temax = 0, tvecs = 0, stpr = 1, stpr0 = 1;
   // FP16 operator form (float engines only): FP16 copies of val and sval
   // scaled by rows, a_ij = rs_i * h_ij with rs_i = max_j |a_ij| in FP32;
   // the single-vector SpMV and Jacobi kernels read these instead of val/sval
@@ -409,24 +414,33 @@ static void build_sell(Arena &ar, const HostCSR &h, DCSR<T> &d) {
 }
 
 // Staged CSR plan (mldg_spmv_stg.cuh): consecutive rows cut into tiles of
-// at most trmax rows and temax entries (a row longer than temax gets a tile
-// of its own, temax raised to it).  temax: 3072 entries (2048 for FP64
-// values), MLDG_STG_E overrides; trmax: the power of two (32..1024) of rows
-// that holds about temax entries at the mean row length.
+// at most trmax rows and temax entries, sized so that kStgStages stages of
+// the widest launch (T values and vectors, tvecs staged vectors: 2 for an
+// operator the SpMV reads, 4 for a Jacobi off-diagonal part) for each of a
+// CTA's kStgWarps warps fit the shared memory a CTA may have: trmax is the
+// largest power of two (32..256) whose rows at the mean length fit the entry
+// budget left beside them.  No plan when a row is longer than the budget
+// (the long-row levels keep the CSR kernels) or with MLDG_NO_STG.
 template <typename T>
-static void build_stg_plan(Arena &ar, const HostCSR &h, DCSR<T> &d) {
+static void build_stg_plan(Arena &ar, const HostCSR &h, DCSR<T> &d, int tvecs) {
   if (std::getenv("MLDG_NO_STG") || h.nr == 0 || h.nnz() == 0) return;
-  int emax = sizeof(T) == 8 ? 2048 : 3072;
-  if (const char *e = std::getenv("MLDG_STG_E")) emax = std::max(256, std::min(16384, std::atoi(e)));
+  const int ci = d.jd ? 2 : 4, es = (int)sizeof(T) + ci;
+  const int budget = (int)((kStgSmemMax - 1024) / ((size_t)kStgWarps * kStgStages)) & ~15;
   const double avg = (double)h.nnz() / h.nr;
-  int rmax = 32;
-  while (rmax < 1024 && rmax * avg < emax) rmax *= 2;
+  auto emax_for = [&](int rmax) {
+    const int fixed = stg_al16(4 * (rmax + 8)) + tvecs * stg_al16((int)sizeof(T) * (rmax + 8));
+    return ((budget - fixed) / es - 16 - 16) & ~15;  // the col/val slices round up to 16 bytes each
+  };
+  int rmax = 32, emax = emax_for(32);
+  for (int r = 256; r >= 32; r /= 2)
+    if (emax_for(r) > 0 && r * avg <= emax_for(r)) {
+      rmax = r;
+      emax = emax_for(r);
+      break;
+    }
   int maxrow = 0;
   for (int i = 0; i < h.nr; ++i) maxrow = std::max(maxrow, h.irp[i + 1] - h.irp[i]);
-  if (maxrow > emax) emax = (maxrow + 63) & ~63;
-  // two stages of the widest form (8-byte values and vectors, int32 columns,
-  // four staged vectors) must fit one CTA's shared memory
-  if (2 * stg_smem(stg_layout<double, double, int>(rmax, emax, 1, kStgVecs)) > kStgSmemMax) return;
+  if (emax <= 0 || maxrow > emax) return;
   std::vector<int4> tiles;
   tiles.reserve((size_t)h.nr / rmax + 1);
   for (int r = 0; r < h.nr;) {
@@ -439,6 +453,7 @@ static void build_stg_plan(Arena &ar, const HostCSR &h, DCSR<T> &d) {
   d.ntiles = (int)tiles.size();
   d.trmax = rmax;
   d.temax = emax;
+  d.tvecs = tvecs;
   d.stpr = d.stpr0 = pick_tpr(h.nnz(), h.nr);
 }
 
@@ -477,7 +492,7 @@ static void make_h16(Arena &ar, const HostCSR &h, DCSR<T> &d) {
 }
 
 template <typename T>
-static DCSR<T> to_dev(Arena &ar, const HostCSR &h, bool h16 = false) {
+static DCSR<T> to_dev(Arena &ar, const HostCSR &h, bool h16 = false, int stg_vecs = 2) {
   DCSR<T> d;
   if (!h.present()) return d;
   d.nr = h.nr;
@@ -502,7 +517,7 @@ static DCSR<T> to_dev(Arena &ar, const HostCSR &h, bool h16 = false) {
   d.val = ar.upload(v);
   d.tpr = pick_tpr(d.nnz, d.nr);
   build_sell(ar, h, d);
-  build_stg_plan(ar, h, d);
+  build_stg_plan(ar, h, d, stg_vecs);
   if (h16) make_h16(ar, h, d);
   return d;
 }
@@ -780,7 +795,7 @@ struct EngineT : Engine {
     spmv_v<T>(A, A.val, A.sval, nullptr, v, a1, b, a0, out, a2);
   }
   // values of type V (T, or FP16 with the row scales rs)
-  int stg_stages = 4;
+  int stg_stages = kStgStages;
   template <int K, typename F>
   static void tpr_case(int tpr, F &&f) {
     if (tpr == K) f(std::integral_constant<int, K>());
@@ -824,7 +839,7 @@ struct EngineT : Engine {
   void stg_prepare_op(const DCSR<T> &A) {
     for (int sp : {A.stpr0 / 2, A.stpr0, A.stpr0 * 2}) {
       if (sp < 1 || sp > 32) continue;
-      for (int nv = 0; nv <= kStgVecs; ++nv) {
+      for (int nv = 0; nv <= A.tvecs; ++nv) {
         const size_t sm = stg_smem(stg_layout<T, V, CI>(A.trmax, A.temax, stg_fit<V, CI>(A, nv), nv));
         tpr_dispatch(sp, [&](auto kc) {
           constexpr int K = decltype(kc)::value;
@@ -901,7 +916,7 @@ struct EngineT : Engine {
   void spmv_v(const DCSR<T> &A, const V *val, const V *sval, const float *rs, const T *v, T a1, const T *b,
               T a0, T *out, T a2) {
     const int64_t vec = (int64_t)A.nc * sizeof(T) + (int64_t)A.nr * sizeof(T) * (1 + (b ? 1 : 0) + (a2 != T(0) ? 1 : 0));
-    if (A.sell == 4 && al16(A.irp) && al16(A.jd ? (const void *)A.jd : (const void *)A.ja) && al16(val) &&
+    if (A.sell == 4 && (b ? 1 : 0) + (a2 != T(0) ? 1 : 0) <= A.tvecs && al16(A.irp) && al16(A.jd ? (const void *)A.jd : (const void *)A.ja) && al16(val) &&
         al16(b) && (a2 == T(0) || al16(out))) {
       begin(MLDG_KERNEL_SPMV);
       spmv_stg<V>(A, val, rs, v, a1, b, a0, out, a2);
@@ -960,7 +975,8 @@ struct EngineT : Engine {
   void jacobi_v(const DCSR<T> &ND, const V *val, const V *sval, const float *rs, const T *d, const T *x,
                 const T *ty, int first, T omega, T alpha, T beta, T *out) {
     const int64_t vec = (int64_t)ND.nr * sizeof(T) * (3 + (first ? 0 : 1) + (beta != T(0) ? 1 : 0));
-    if (ND.sell == 4 && al16(ND.irp) && al16(ND.jd ? (const void *)ND.jd : (const void *)ND.ja) && al16(val) &&
+    if (ND.sell == 4 && 2 + (!first && omega != T(1) ? 1 : 0) + (beta != T(0) ? 1 : 0) <= ND.tvecs &&
+        al16(ND.irp) && al16(ND.jd ? (const void *)ND.jd : (const void *)ND.ja) && al16(val) &&
         al16(d) && al16(x) && al16(ty) && (beta == T(0) || al16(out))) {
       begin(MLDG_KERNEL_JACOBI);
       jacobi_stg<V>(ND, val, rs, d, x, ty, first, omega, alpha, beta, out);
@@ -1017,6 +1033,14 @@ struct EngineT : Engine {
     begin(MLDG_KERNEL_VEC);
     k_diag<T><<<blocks_for(n), 256, 0, st>>>(n, d, x, alpha, beta, out);
     end((int64_t)n * sizeof(T) * (3 + (beta != T(0) ? 1 : 0)));
+  }
+  // precision cast of a boundary vector (k_cast4 when both are 16-byte aligned)
+  template <typename A, typename B>
+  void cast(int n, const A *x, B *y) {
+    if ((((uintptr_t)x | (uintptr_t)y) & 15u) == 0)
+      k_cast4<A, B><<<blocks_for(((int64_t)n + 3) / 4), 256, 0, st>>>(n, x, y);
+    else
+      k_cast<A, B><<<blocks_for(n), 256, 0, st>>>(n, x, y);
   }
   void fill(int n, T v, T *y) {
     begin(MLDG_KERNEL_VEC);
@@ -2377,7 +2401,7 @@ struct EngineT : Engine {
     Lev &F = lv[0];
     if (!std::is_same<T, double>::value) {
       begin(MLDG_KERNEL_VEC);
-      k_cast<double, T><<<blocks_for(F.n), 256, 0, st>>>(F.n, xin, F.x);
+      cast(F.n, xin, F.x);
       end((int64_t)F.n * (8 + sizeof(T)));
     }
     if (lv.size() == 1 && F.kind == MLDG_SMOOTHER_FBGS) {
@@ -2404,7 +2428,7 @@ struct EngineT : Engine {
     if (!std::is_same<T, double>::value) {
       cur_lev = 0;
       begin(MLDG_KERNEL_VEC);
-      k_cast<T, double><<<blocks_for(F.n), 256, 0, st>>>(F.n, F.y, yout);
+      cast(F.n, F.y, yout);
       end((int64_t)F.n * (8 + sizeof(T)));
     }
   }
@@ -3866,8 +3890,8 @@ static Engine *make_engine(Handle *h) {
       }
     }
     if (H.ND.present() && L.nnz_nd > 0) {
-      L.ND = to_dev<T>(ar, H.ND, h16);
-      L.NDT = to_dev<T>(ar, transpose(H.ND), h16);
+      L.ND = to_dev<T>(ar, H.ND, h16, kStgVecs);
+      L.NDT = to_dev<T>(ar, transpose(H.ND), h16, kStgVecs);
     }
     tick("FBGS factors, ND");
     if (H.kind == MLDG_SMOOTHER_BJAC && l == h->nlev - 1 && h->nlev > 1 && L.n <= kDenseCoarseRows &&

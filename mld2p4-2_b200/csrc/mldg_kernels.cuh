@@ -132,6 +132,23 @@ __device__ __forceinline__ T row_scaled(T acc, const float *__restrict__ rs, int
     return acc;
 }
 
+// The point-Jacobi update of one row from its off-diagonal sum s, every
+// operation explicit (no multiply-add left to contraction), so that all the
+// Jacobi kernels round alike: t = d_i (x_i - s); v = t when omega = 1, else
+// (1 - omega) ty_i + omega t with ty_i = omega d_i x_i on the unrolled first
+// sweep; result alpha v + beta out_i.
+template <typename T>
+__device__ __forceinline__ T jac_row(T di, T xi, T s, T tyi, bool first, T omega, T alpha, T beta, T outi) {
+  const T t = di * (xi - s);
+  T v = t;
+  if (omega != T(1)) {
+    const T ty0 = first ? omega * (di * xi) : tyi;
+    v = fma(omega, t, (T(1) - omega) * ty0);
+  }
+  const T r = alpha * v;
+  return beta != T(0) ? fma(beta, outi, r) : r;
+}
+
 // One lane's part of a CSR row sum: entries k = k0, k0 + TPR, ... < e,
 // s = fma(val[k], g(col k), s) in that order from zero.  The loads are
 // issued kCsrU entries at a time (column indices and values, then the
@@ -363,19 +380,8 @@ __global__ void __launch_bounds__(256) k_jacobi_sellp(int nr, const int *__restr
                                                       const T *__restrict__ ty, int first, T omega, T alpha,
                                                       T beta, T *out, const float *__restrict__ rs = nullptr) {
   auto done = [&](int row, T acc) {
-    acc = row_scaled<T, V>(acc, rs, row);
-    const T di = d[row], xi = x[row];
-    const T t = di * (xi - acc);
-    T vv;
-    if (omega == T(1)) {
-      vv = t;
-    } else {
-      const T tyi = first ? omega * (di * xi) : ty[row];
-      vv = (T(1) - omega) * tyi + omega * t;
-    }
-    T r = alpha * vv;
-    if (beta != T(0)) r = fma(beta, out[row], r);
-    out[row] = r;
+    out[row] = jac_row(d[row], x[row], row_scaled<T, V>(acc, rs, row), (!first && omega != T(1)) ? ty[row] : T(0),
+                       first != 0, omega, alpha, beta, beta != T(0) ? out[row] : T(0));
   };
   if (first)
     sellp_loop<T, CI>(
@@ -405,20 +411,10 @@ __global__ void __launch_bounds__(256) k_jacobi_sell(int nr, const int *__restri
 #pragma unroll
     for (int q = 0; q < S; ++q) {
       const int row = ((sl0 + q) << 5) + lane;
-      if (row < nr) {
-        const T di = d[row], xi = x[row];
-        const T t = di * (xi - row_scaled<T, V>(acc[q], rs, row));
-        T vv;
-        if (omega == T(1)) {
-          vv = t;
-        } else {
-          const T tyi = first ? omega * (di * xi) : ty[row];
-          vv = (T(1) - omega) * tyi + omega * t;
-        }
-        T r = alpha * vv;
-        if (beta != T(0)) r = fma(beta, out[row], r);
-        out[row] = r;
-      }
+      if (row < nr)
+        out[row] = jac_row(d[row], x[row], row_scaled<T, V>(acc[q], rs, row),
+                           (!first && omega != T(1)) ? ty[row] : T(0), first != 0, omega, alpha, beta,
+                           beta != T(0) ? out[row] : T(0));
     }
   }
 }
@@ -486,21 +482,9 @@ __global__ void __launch_bounds__(256) k_jacobi(int nr, const int *__restrict__ 
     }
 #pragma unroll
     for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, TPR);
-    if (row < nr && sub == 0) {
-      s = row_scaled<T, V>(s, rs, row);
-      const T di = d[row], xi = x[row];
-      T t = di * (xi - s);
-      T v;
-      if (omega == T(1)) {
-        v = t;
-      } else {
-        const T tyi = first ? omega * (di * xi) : ty[row];
-        v = (T(1) - omega) * tyi + omega * t;
-      }
-      T r = alpha * v;
-      if (beta != T(0)) r = fma(beta, out[row], r);
-      out[row] = r;
-    }
+    if (row < nr && sub == 0)
+      out[row] = jac_row(d[row], x[row], row_scaled<T, V>(s, rs, row), (!first && omega != T(1)) ? ty[row] : T(0),
+                         first != 0, omega, alpha, beta, beta != T(0) ? out[row] : T(0));
   }
 }
 
@@ -566,6 +550,38 @@ template <typename A, typename B>
 __global__ void k_cast(int n, const A *__restrict__ x, B *__restrict__ y) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     y[i] = (B)x[i];
+}
+
+// Precision casts of the V-cycle's boundary vectors, four elements per
+// thread with 16-byte loads and stores (both arrays 16-byte aligned; the
+// host checks), the last n % 4 elements one per thread.
+__device__ __forceinline__ void cast4_ld(const double *p, double (&v)[4]) {
+  const double2 a = reinterpret_cast<const double2 *>(p)[0], b = reinterpret_cast<const double2 *>(p)[1];
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void cast4_ld(const float *p, float (&v)[4]) {
+  const float4 a = *reinterpret_cast<const float4 *>(p);
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+__device__ __forceinline__ void cast4_st(double *p, const double (&v)[4]) {
+  reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+  reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+}
+__device__ __forceinline__ void cast4_st(float *p, const float (&v)[4]) {
+  *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+template <typename A, typename B>
+__global__ void __launch_bounds__(256) k_cast4(int n, const A *__restrict__ x, B *__restrict__ y) {
+  const int n4 = n >> 2, stride = gridDim.x * blockDim.x, t = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int i = t; i < n4; i += stride) {
+    A a[4];
+    B b[4];
+    cast4_ld(x + 4 * (int64_t)i, a);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) b[u] = (B)a[u];
+    cast4_st(y + 4 * (int64_t)i, b);
+  }
+  for (int i = 4 * n4 + t; i < n; i += stride) y[i] = (B)x[i];
 }
 
 template <typename T>

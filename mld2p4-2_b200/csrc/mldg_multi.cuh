@@ -65,18 +65,8 @@ __global__ void __launch_bounds__(256) k_jacobi_m(int nr, const int *__restrict_
     } else {
       for (int k = irp[row]; k < e; ++k) s = fma(val[k], __ldg(ty + (size_t)ja[k] * K + c), s);
     }
-    const T di = d[row], xi = x[t];
-    const T tt = di * (xi - s);
-    T v;
-    if (omega == T(1)) {
-      v = tt;
-    } else {
-      const T tyi = first ? omega * (di * xi) : ty[t];
-      v = (T(1) - omega) * tyi + omega * tt;
-    }
-    T r = alpha * v;
-    if (beta != T(0)) r = fma(beta, out[t], r);
-    out[t] = r;
+    out[t] = jac_row(d[row], x[t], s, (!first && omega != T(1)) ? ty[t] : T(0), first != 0, omega, alpha, beta,
+                     beta != T(0) ? out[t] : T(0));
   }
 }
 

@@ -3,32 +3,35 @@
 //
 // The rows of an operator are cut (on the host, once) into tiles of
 // consecutive rows: at most rmax rows and emax entries each, described by
-// int4 {first row, end row, first entry, end entry}.  A persistent grid
-// walks the tiles round robin (tile t goes to CTA t mod grid).  In each CTA
-// one producer thread copies whole tiles -- the tile's slice of the row
-// offsets, of the column indices, of the values and of up to kStgVecs row
-// vectors (the right-hand side b, the output's old values, the Jacobi
-// diagonal and iterate) -- into a ring of `stages` shared-memory stages with
-// cp.async.bulk, each stage's full mbarrier counting the bytes; eight
-// consumer warps compute the tile's rows from shared memory (TPR lanes per
-// row, entries summed in stored order per lane, lanes combined by a
-// butterfly exactly like k_spmv / k_jacobi) and gather the multiplied vector
-// through L1/L2, then release the stage on its empty mbarrier.  The copies
-// are large and contiguous (one to three requests of several KB per array
-// and tile) and run `stages` tiles ahead of the compute, so the DRAM stream
-// does not wait on the dependent load chain (row offsets, then entries, then
-// gathers) that limits the per-thread CSR and SELL kernels.
+// int4 {first row, end row, first entry, end entry}, sized so that one
+// warp's share of shared memory holds `stages` of them.  Every warp of a
+// persistent grid walks its own tiles (tile t goes to warp t mod (warps of
+// the grid)) through its own ring of `stages` shared-memory stages: lane 0
+// copies a whole tile -- its slice of the row offsets, of the column indices,
+// of the values and of up to kStgVecs row vectors (the right-hand side b,
+// the output's old values, the Jacobi diagonal and iterate) -- with
+// cp.async.bulk into a stage whose mbarrier counts the bytes, `stages - 1`
+// tiles ahead of the one the warp computes.  The warp computes a tile's rows
+// from shared memory, TPR lanes per row and StgRows rows per lane group at a
+// time, every lane issuing the gathers of kStgU entries of each of its rows
+// before it sums any of them.  So the DRAM stream is a few large contiguous
+// requests per tile in flight on every warp, independent of the dependent
+// load chain (row offsets, then entries, then gathers) that limits the
+// per-thread CSR and SELL kernels, and the gathers of many rows overlap.
+// A row's entries are summed per lane in stored order and the lanes combined
+// by a butterfly, exactly as k_spmv / k_jacobi with the same lanes per row
+// do: the results are bit for bit theirs.
 //
 // A bulk copy needs a 16-byte aligned source and a size that is a multiple
 // of 16 bytes: every slice is widened to 16-byte boundaries (the arrays are
 // cudaMalloc'd with slack past their end, so the widened slices stay inside
-// the allocations), and the consumers index the staged slices relative to
-// the widened starts.
+// the allocations), and the warp indexes the staged slices relative to the
+// widened starts.  Before lane 0 refills a stage, the warp's reads of it are
+// ordered before the asynchronous copy by __syncwarp and a proxy fence.
 //
-// Every wait is bounded: an mbarrier wait that gives up sets error 4021; a
-// consumer that gave up stops computing, the producer then gives up on its
-// empty barrier, and before the CTA exits the producer waits (bounded) for
-// every copy it issued.
+// Every wait is bounded: an mbarrier wait that gives up sets error 4021 and
+// the warp stops; lane 0 then waits (bounded) for every copy it issued
+// before the warp exits.
 #pragma once
 
 #include <cuda_fp16.h>
@@ -40,16 +43,19 @@
 
 namespace mldg {
 
-constexpr int kStgConsumers = 8;                     // consumer warps
-constexpr int kStgThreads = 32 * (kStgConsumers + 1);  // + one producer warp
-constexpr int kStgVecs = 4;                          // row vectors staged per tile (at most)
-constexpr int kStgMaxStages = 8;
+constexpr int kStgWarps = 16;               // warps per CTA, each with its own ring
+constexpr int kStgThreads = 32 * kStgWarps;
+constexpr int kStgVecs = 4;                 // row vectors staged per tile (at most)
+constexpr int kStgStages = 2;     // stages per warp the plans are sized for
+constexpr int kStgMaxStages = 4;  // MLDG_STG_S may ask for up to this many (fewer when they do not fit)
 constexpr size_t kStgSmemMax = 227 * 1024;  // dynamic shared memory a CTA may opt in to
+constexpr int kStgU = 8;                    // entries per lane and row whose gathers are issued together
 
-__device__ __forceinline__ void stg_arrive(uint64_t *bar) {
-  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}" ::"r"(smem_u32(bar))
-               : "memory");
-}
+// rows a lane group holds in flight: 4 with 4-byte vectors, 2 with 8-byte ones
+template <typename T>
+struct StgRows {
+  static constexpr int value = sizeof(T) == 8 ? 2 : 4;
+};
 
 // Byte layout of one stage (all offsets 16-byte multiples):
 //   int  irp[rmax + 8]                 row offsets of the tile (widened slice)
@@ -75,8 +81,10 @@ __host__ inline StgLayout stg_layout(int rmax, int emax, int stages, int nvec) {
   L.stage_bytes = L.off_vec + nvec * L.vec_bytes;
   return L;
 }
-// dynamic shared memory of a launch: the stages and the 2 * stages mbarriers
-__host__ inline size_t stg_smem(const StgLayout &L) { return (size_t)L.stages * L.stage_bytes + 16 * L.stages; }
+// dynamic shared memory of a launch: every warp's stages and mbarriers
+__host__ inline size_t stg_smem(const StgLayout &L) {
+  return (size_t)kStgWarps * ((size_t)L.stages * L.stage_bytes + 8 * (size_t)L.stages);
+}
 
 template <typename T, typename V, typename CI>
 struct StgArgs {
@@ -98,104 +106,135 @@ __device__ __forceinline__ int stg_lo(int i) { return i & ~(16 / E - 1); }
 template <int E>
 __device__ __forceinline__ int stg_hi(int i) { return (i + 16 / E - 1) & ~(16 / E - 1); }
 
-// The tile loop shared by both kernels: tile_fn(tile descriptor, its stage)
-// runs on every consumer thread once the tile's copies have landed.
+__device__ __forceinline__ void stg_fence_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// lane 0: copy tile t into the stage st of the warp's ring, counted on bar
+template <typename T, typename V, typename CI>
+__device__ __forceinline__ void stg_issue(const StgArgs<T, V, CI> &a, int t, unsigned char *st, uint64_t *bar) {
+  const StgLayout &L = a.L;
+  const int4 d = a.tiles[t];
+  const int ia0 = stg_lo<4>(d.x), ia1 = stg_hi<4>(d.y + 1);
+  const int ec0 = stg_lo<sizeof(CI)>(d.z), ec1 = stg_hi<sizeof(CI)>(d.w);
+  const int ev0 = stg_lo<sizeof(V)>(d.z), ev1 = stg_hi<sizeof(V)>(d.w);
+  const int rv0 = stg_lo<sizeof(T)>(d.x), rv1 = stg_hi<sizeof(T)>(d.y);
+  const unsigned bi = 4u * (unsigned)(ia1 - ia0), bc = (unsigned)sizeof(CI) * (unsigned)(ec1 - ec0),
+                 bv = (unsigned)sizeof(V) * (unsigned)(ev1 - ev0), bw = (unsigned)sizeof(T) * (unsigned)(rv1 - rv0);
+  mbar_expect_tx(bar, bi + bc + bv + (unsigned)L.nvec * bw);
+  tma_bulk_g2s(st, a.irp + ia0, bi, bar);
+  if (bc) tma_bulk_g2s(st + L.off_col, a.cj + ec0, bc, bar);
+  if (bv) tma_bulk_g2s(st + L.off_val, a.val + ev0, bv, bar);
+#pragma unroll
+  for (int q = 0; q < kStgVecs; ++q)  // static indices: the arguments stay in the parameter space
+    if (q < L.nvec) tma_bulk_g2s(st + L.off_vec + q * L.vec_bytes, a.vec[q] + rv0, bw, bar);
+}
+
+// The tile loop of one warp: tile_fn(tile descriptor, its stage) runs on all
+// 32 lanes once the tile's copies have landed.
 template <typename T, typename V, typename CI, typename F>
 __device__ __forceinline__ void stg_run(const StgArgs<T, V, CI> &a, F tile_fn) {
   extern __shared__ __align__(128) unsigned char smem[];
   const StgLayout &L = a.L;
-  uint64_t *full = reinterpret_cast<uint64_t *>(smem + (size_t)L.stages * L.stage_bytes);
-  uint64_t *empty = full + L.stages;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  if (tid == 0) {
-    for (int s = 0; s < L.stages; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], kStgConsumers);
-    }
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned char *ring = smem + (size_t)w * L.stages * L.stage_bytes;
+  uint64_t *full =
+      reinterpret_cast<uint64_t *>(smem + (size_t)kStgWarps * L.stages * L.stage_bytes) + (size_t)w * L.stages;
+  const int gw = blockIdx.x * kStgWarps + w, nw = gridDim.x * kStgWarps;
+  int issued = 0;  // lane 0: tiles of this warp whose copies were issued
+  if (lane == 0) {
+    for (int s = 0; s < L.stages; ++s) mbar_init(&full[s], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (int s = 0; s < L.stages && gw + s * nw < a.ntiles; ++s, ++issued)
+      stg_issue(a, gw + s * nw, ring + (size_t)s * L.stage_bytes, &full[s]);
   }
-  __syncthreads();
-  if (warp == kStgConsumers) {
-    // producer: one thread issues every copy of the CTA's tiles
-    if (lane != 0) return;
-    int i = 0;
-    for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, ++i) {
-      const int s = i % L.stages;
-      if (i >= L.stages && !mbar_wait(&empty[s], (unsigned)(((i / L.stages) - 1) & 1))) {
-        atomicExch(a.err, 4021);
-        break;
-      }
-      const int4 d = a.tiles[t];
-      unsigned char *st = smem + (size_t)s * L.stage_bytes;
-      const int ia0 = stg_lo<4>(d.x), ia1 = stg_hi<4>(d.y + 1);
-      const int ec0 = stg_lo<sizeof(CI)>(d.z), ec1 = stg_hi<sizeof(CI)>(d.w);
-      const int ev0 = stg_lo<sizeof(V)>(d.z), ev1 = stg_hi<sizeof(V)>(d.w);
-      const int rv0 = stg_lo<sizeof(T)>(d.x), rv1 = stg_hi<sizeof(T)>(d.y);
-      const unsigned bi = 4u * (unsigned)(ia1 - ia0), bc = (unsigned)sizeof(CI) * (unsigned)(ec1 - ec0),
-                     bv = (unsigned)sizeof(V) * (unsigned)(ev1 - ev0), bw = (unsigned)sizeof(T) * (unsigned)(rv1 - rv0);
-      mbar_expect_tx(&full[s], bi + bc + bv + (unsigned)L.nvec * bw);
-      tma_bulk_g2s(st, a.irp + ia0, bi, &full[s]);
-      if (bc) tma_bulk_g2s(st + L.off_col, a.cj + ec0, bc, &full[s]);
-      if (bv) tma_bulk_g2s(st + L.off_val, a.val + ev0, bv, &full[s]);
-#pragma unroll
-      for (int q = 0; q < kStgVecs; ++q)  // static indices: the arguments stay in the parameter space
-        if (q < L.nvec) tma_bulk_g2s(st + L.off_vec + q * L.vec_bytes, a.vec[q] + rv0, bw, &full[s]);
-    }
-    // every copy issued must land before the CTA exits
-    for (int j = i > L.stages ? i - L.stages : 0; j < i; ++j)
-      mbar_wait(&full[j % L.stages], (unsigned)((j / L.stages) & 1));
-    return;
-  }
-  int i = 0;
-  for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x, ++i) {
-    const int s = i % L.stages;
-    if (!mbar_wait(&full[s], (unsigned)((i / L.stages) & 1))) {
+  __syncwarp();
+  int k = 0;
+  for (; gw + k * nw < a.ntiles; ++k) {
+    const int s = k % L.stages;
+    if (!mbar_wait(&full[s], (unsigned)((k / L.stages) & 1))) {
       if (lane == 0) atomicExch(a.err, 4021);
       break;
     }
-    tile_fn(a.tiles[t], smem + (size_t)s * L.stage_bytes);
+    tile_fn(a.tiles[gw + k * nw], ring + (size_t)s * L.stage_bytes);
     __syncwarp();
-    if (lane == 0) stg_arrive(&empty[s]);
+    const int kn = k + L.stages;
+    if (lane == 0 && gw + kn * nw < a.ntiles) {
+      stg_fence_async();  // the warp's reads of this stage before the copy that overwrites it
+      stg_issue(a, gw + kn * nw, ring + (size_t)s * L.stage_bytes, &full[s]);
+      ++issued;
+    }
   }
+  // after a wait that gave up: every copy issued must land before the warp exits
+  if (lane == 0)
+    for (int j = k; j < issued; ++j) mbar_wait(&full[j % L.stages], (unsigned)((j / L.stages) & 1));
 }
 
-// Rows of one staged tile, TPR lanes per row: the row sum of val * gather(col)
-// over the row's staged entries (csr_lane_sum per lane, then the butterfly),
-// then done(row, the row's position in the staged vectors, sum) on the
-// row's first lane.
+// Rows of one staged tile: TPR lanes per row, StgRows rows per lane group at
+// a time; per row each lane sums val * gather(col) over its entries k =
+// first + lane, + TPR, ... in order (the loads and gathers of kStgU entries
+// of every row of the group issued before the sums), then the butterfly,
+// then done(row, the row's position in the staged vectors, sum) on the row's
+// first lane.
 template <typename T, typename V, typename CI, int TPR, typename G, typename D>
 __device__ __forceinline__ void stg_rows(const StgLayout &L, const int4 d, const unsigned char *st,
                                          const float *__restrict__ rs, G gather, D done) {
-  constexpr int RPP = 32 * kStgConsumers / TPR;  // rows per pass
-  const int c = threadIdx.x;                     // consumer thread 0..255
-  const int grp = c / TPR, sub = c % TPR;
+  constexpr int R = StgRows<T>::value, NG = 32 / TPR;
+  const int lane = threadIdx.x & 31, grp = lane / TPR, sub = lane % TPR;
   const int ia0 = stg_lo<4>(d.x), ec0 = stg_lo<sizeof(CI)>(d.z), ev0 = stg_lo<sizeof(V)>(d.z);
   const int rv0 = stg_lo<sizeof(T)>(d.x);
   const int *irs = reinterpret_cast<const int *>(st);
   const CI *cs = reinterpret_cast<const CI *>(st + L.off_col);
-  const V *vs = reinterpret_cast<const V *>(st + L.off_val);
+  // the value of staged column position k is at k + (ec0 - ev0) of the staged values
+  const V *vs = reinterpret_cast<const V *>(st + L.off_val) + (ec0 - ev0);
   const int nrow = d.y - d.x;
-  for (int p = 0; p < nrow; p += RPP) {  // uniform over the CTA: full-warp shuffles below
-    const int lr = p + grp;
-    const bool ok = lr < nrow;
-    const int row = d.x + lr;
-    T s = T(0);
-    if (ok) {
-      // entry k of the row is staged at k - ec0 (columns) and k - ev0 (values)
-      const int k0 = irs[row - ia0] + sub, k1 = irs[row + 1 - ia0];
-      s = csr_lane_sum<T, TPR>(k0 - ec0, k1 - ec0, row, cs, vs + (ec0 - ev0), gather);
+  for (int p = 0; p < nrow; p += NG * R) {  // uniform over the warp: full-warp shuffles below
+    int kb[R], ke[R], row[R];
+    T s[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int lr = p + grp + r * NG;
+      const bool ok = lr < nrow;
+      row[r] = d.x + lr;
+      kb[r] = ok ? irs[row[r] - ia0] + sub - ec0 : 0;  // staged column positions
+      ke[r] = ok ? irs[row[r] + 1 - ia0] - ec0 : 0;
+      s[r] = T(0);
+    }
+    for (;;) {
+      bool more = false;
+#pragma unroll
+      for (int r = 0; r < R; ++r) more |= kb[r] < ke[r];
+      if (!more) break;
+      T vv[R][kStgU], xv[R][kStgU];
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int u = 0; u < kStgU; ++u) {
+          const int k = kb[r] + u * TPR;
+          const bool ok = k < ke[r];
+          vv[r][u] = ok ? ldval<T>(vs, k) : T(0);
+          xv[r][u] = ok ? gather(colof(cs, k, row[r])) : T(0);
+        }
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+#pragma unroll
+        for (int u = 0; u < kStgU; ++u)
+          if (kb[r] + u * TPR < ke[r]) s[r] = fma(vv[r][u], xv[r][u], s[r]);
+        kb[r] += kStgU * TPR;
+      }
     }
 #pragma unroll
-    for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, TPR);
-    if (ok && sub == 0) done(row, row - rv0, row_scaled<T, V>(s, rs, row));
+    for (int r = 0; r < R; ++r) {
+#pragma unroll
+      for (int o = TPR / 2; o > 0; o >>= 1) s[r] += __shfl_down_sync(0xffffffffu, s[r], o, TPR);
+      if (row[r] < d.y && sub == 0) done(row[r], row[r] - rv0, row_scaled<T, V>(s[r], rs, row[r]));
+    }
   }
 }
 
 // out = a1*(A v) + a0*b + a2*out  (k_spmv's operation); staged vectors:
 // slot 0 = b when b is given, the next slot = out when a2 != 0
 template <typename T, typename V, typename CI, int TPR>
-__global__ void __launch_bounds__(kStgThreads) k_spmv_stg(StgArgs<T, V, CI> a, const T *__restrict__ v, T a1,
-                                                          int has_b, T a0, T *out, T a2) {
+__global__ void __launch_bounds__(kStgThreads, 1) k_spmv_stg(StgArgs<T, V, CI> a, const T *__restrict__ v, T a1,
+                                                             int has_b, T a0, T *out, T a2) {
   const int sb = 0, so = has_b ? 1 : 0;
   stg_run<T, V, CI>(a, [&](const int4 d, const unsigned char *st) {
     const T *vb = reinterpret_cast<const T *>(st + a.L.off_vec + sb * a.L.vec_bytes);
@@ -214,9 +253,9 @@ __global__ void __launch_bounds__(kStgThreads) k_spmv_stg(StgArgs<T, V, CI> a, c
 // the Jacobi sweep of k_jacobi; staged vectors: slot 0 = d, 1 = x, then ty
 // (when !first and omega != 1), then out (when beta != 0)
 template <typename T, typename V, typename CI, int TPR>
-__global__ void __launch_bounds__(kStgThreads) k_jacobi_stg(StgArgs<T, V, CI> a, const T *__restrict__ d,
-                                                            const T *__restrict__ x, const T *__restrict__ ty,
-                                                            int first, T omega, T alpha, T beta, T *out) {
+__global__ void __launch_bounds__(kStgThreads, 1) k_jacobi_stg(StgArgs<T, V, CI> a, const T *__restrict__ d,
+                                                               const T *__restrict__ x, const T *__restrict__ ty,
+                                                               int first, T omega, T alpha, T beta, T *out) {
   const bool use_ty = !first && omega != T(1);
   const int sty = 2, sout = use_ty ? 3 : 2;
   stg_run<T, V, CI>(a, [&](const int4 dd, const unsigned char *st) {
@@ -225,18 +264,8 @@ __global__ void __launch_bounds__(kStgThreads) k_jacobi_stg(StgArgs<T, V, CI> a,
     const T *vt = reinterpret_cast<const T *>(st + a.L.off_vec + sty * a.L.vec_bytes);
     const T *vo = reinterpret_cast<const T *>(st + a.L.off_vec + sout * a.L.vec_bytes);
     auto done = [&](int row, int q, T s) {
-      const T di = vd[q], xi = vx[q];
-      const T t = di * (xi - s);
-      T vv;
-      if (omega == T(1)) {
-        vv = t;
-      } else {
-        const T tyi = first ? omega * (di * xi) : vt[q];
-        vv = (T(1) - omega) * tyi + omega * t;
-      }
-      T r = alpha * vv;
-      if (beta != T(0)) r = fma(beta, vo[q], r);
-      out[row] = r;
+      out[row] = jac_row(vd[q], vx[q], s, use_ty ? vt[q] : T(0), first != 0, omega, alpha, beta,
+                         beta != T(0) ? vo[q] : T(0));
     };
     if (first)
       stg_rows<T, V, CI, TPR>(a.L, dd, st, a.rs, [&](int j) { return omega * (__ldg(d + j) * __ldg(x + j)); },

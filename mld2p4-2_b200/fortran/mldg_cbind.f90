@@ -37,6 +37,7 @@ module mldg_cbind
   integer(c_int), parameter :: MLDG_PREC_FP64 = 0
   integer(c_int), parameter :: MLDG_PREC_FP32 = 1
   integer(c_int), parameter :: MLDG_PREC_FP32_P16 = 2
+  integer(c_int), parameter :: MLDG_PREC_FP32_H16 = 3
   ! memory kinds of vector arguments
   integer(c_int), parameter :: MLDG_MEM_HOST = 0
   integer(c_int), parameter :: MLDG_MEM_DEVICE = 1

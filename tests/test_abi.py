@@ -133,3 +133,19 @@ int main(void) {
     assert r.returncode == 0, r.stdout + r.stderr
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0 and "c99 ok" in r.stdout, (r.returncode, r.stdout, r.stderr)
+
+
+def test_fortran_constants_match_header():
+    """Every named constant of the Fortran binding (mldg_cbind.f90) has the
+    value the C header defines, and every MLDG_PREC_ / MLDG_SMOOTHER_ /
+    MLDG_ERR_ constant of the header is bound."""
+    h = open(os.path.join(ROOT, "include", "mldg.h")).read()
+    defs = {k: int(v) for k, v in re.findall(r"#define\s+(MLDG_[A-Z0-9_]+)\s+(-?\d+)\b", h)}
+    f = open(os.path.join(ROOT, "mld2p4-2_b200", "fortran", "mldg_cbind.f90")).read()
+    params = {k: int(v) for k, v in re.findall(r"parameter\s*::\s*(MLDG_[A-Z0-9_]+)\s*=\s*(-?\d+)", f)}
+    assert params, "no constants found in mldg_cbind.f90"
+    for k, v in params.items():
+        assert k in defs and defs[k] == v, (k, v, defs.get(k))
+    for k in defs:
+        if k.startswith(("MLDG_PREC_", "MLDG_SMOOTHER_", "MLDG_ERR_")):
+            assert k in params, f"{k} not bound in mldg_cbind.f90"
