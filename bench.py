@@ -189,11 +189,17 @@ def oracle_prec(orc, ao, smoother):
     return op
 
 
+# the V-cycle precision forms (PRECISION keyword of the host mirror)
+FORM_TEXT = {"FP64": "FP64", "FP32": "FP32",
+             "FP32_P16": "FP32 with FP16 prolongator values (FP32 row scales)",
+             "FP32_H16": "FP32 arithmetic on FP16 operator values (FP32 row scales for A, P, R, ND)"}
+
+
 def workload_config(args, world, a=None, p=None, precision=None):
     pr = precision or args.precision
     c = {"workload": f"pdegen 3D anisotropic convection-diffusion (0.01 u_zz) idim={args.idim}, "
                      f"b uniform[-1,1] seed 0, ML V-cycle point-Jacobi 2+2 sweeps (damping 0.8) in "
-                     f"{pr}, FP64 FCG to {args.eps:g}",
+                     f"{FORM_TEXT[pr]}, FP64 FCG to {args.eps:g}",
          "idim": args.idim, "rows": args.idim ** 3, "smoother": HEADLINE_SMOOTHER,
          "precision": pr, "outer": "FP64 FCG (istop 2)",
          "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
@@ -541,7 +547,7 @@ def run_ours(args, rank, world, local_rank):
     def summary(pr):
         f = forms[pr]
         s = form_summary(f["r"], *f["apply"], peak, world, args.steps,
-                         f"point-Jacobi V-cycle in {pr}, FP64 FCG")
+                         f"point-Jacobi V-cycle in {FORM_TEXT[pr]}, FP64 FCG")
         if "err_vs_cpu" in f:
             s["rel_error_vs_cpu_fp64"] = f["err_vs_cpu"]
         return s
@@ -551,7 +557,9 @@ def run_ours(args, rank, world, local_rank):
         "metric": METRIC, "value": world * args.steps / (r["tot_ms"] * 1e-3), "unit": "solves/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": r["tot_ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32 V-cycle / f64 FCG" if args.precision != "FP64" else "f64",
+        "vs_baseline": None,
+        "dtype": {"FP64": "f64", "FP32": "f32 V-cycle / f64 FCG", "FP32_P16": "f32 V-cycle (f16 P) / f64 FCG",
+                  "FP32_H16": "f32 V-cycle on f16 operator values / f64 FCG"}[args.precision],
         "data": "synthetic (seeded generator, no dataset)",
         "config": workload_config(args, world, a) | {"levels": main["levels"]},
         "iterations": r["iters"], "time_to_1e-10_ms": r["tot_ms"] / args.steps,
@@ -587,7 +595,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--idim", type=int, default=160)
-    ap.add_argument("--precision", default="FP32", choices=["FP64", "FP32", "FP32_P16", "FP32_H16"])
+    ap.add_argument("--precision", default="FP32_H16", choices=["FP64", "FP32", "FP32_P16", "FP32_H16"])
     ap.add_argument("--eps", type=float, default=1e-10)
     ap.add_argument("--sample-its", type=int, default=8,
                     help="reference arm: FCG iterations timed per step (scaled to the full solve)")

@@ -231,13 +231,14 @@ struct DCSR {
   int64_t slots = 0;
   // 0: CSR kernels; 1 or 2: SELL kernels with that many slices per warp
   // iteration; 3: the software-pipelined SELL kernels (k_spmv_sellp,
-  // k_jacobi_sellp); 4: the staged CSR kernels (k_spmv_stg, k_jacobi_stg)
+  // k_jacobi_sellp); 4: the staged SELL kernels (k_spmv_stg, k_jacobi_stg)
   int sell = 0;
-  // staged CSR plan (k_spmv_stg, k_jacobi_stg): tiles of consecutive rows
-  // {first row, end row, first entry, end entry}, at most trmax rows and
-  // temax entries each, computed with stpr lanes per row; used when sell == 4
+  // staged SELL tiles (k_spmv_stg, k_jacobi_stg): packed blocks of
+  // consecutive slices and their descriptors, the largest block tblock
+  // bytes; used when sell == 4
   int4 *tiles = nullptr;
-  int ntiles = 0, trmax = 0, temax = 0, tvecs = 0, stpr = 1, stpr0 = 1;
+  uint4 *pk = nullptr;
+  int ntiles = 0, tblock = 0;
   // FP16 operator form (float engines only): FP16 copies of val and sval
   // scaled by rows, a_ij = rs_i * h_ij with rs_i = max_j |a_ij| in FP32;
   // the single-vector SpMV and Jacobi kernels read these instead of val/sval
@@ -413,57 +414,12 @@ static void build_sell(Arena &ar, const HostCSR &h, DCSR<T> &d) {
   d.slots = slots;
 }
 
-// Staged CSR plan (mldg_spmv_stg.cuh): consecutive rows cut into tiles of
-// at most trmax rows and temax entries, sized so that kStgStages stages of
-// the widest launch (T values and vectors, tvecs staged vectors: 2 for an
-// operator the SpMV reads, 4 for a Jacobi off-diagonal part) for each of a
-// CTA's kStgWarps warps fit the shared memory a CTA may have: trmax is the
-// largest power of two (32..256) whose rows at the mean length fit the entry
-// budget left beside them.  No plan when a row is longer than the budget
-// (the long-row levels keep the CSR kernels) or with MLDG_NO_STG.
-template <typename T>
-static void build_stg_plan(Arena &ar, const HostCSR &h, DCSR<T> &d, int tvecs) {
-  if (std::getenv("MLDG_NO_STG") || h.nr == 0 || h.nnz() == 0) return;
-  const int ci = d.jd ? 2 : 4, es = (int)sizeof(T) + ci;
-  const int budget = (int)((kStgSmemMax - 1024) / ((size_t)kStgWarps * kStgStages)) & ~15;
-  const double avg = (double)h.nnz() / h.nr;
-  auto emax_for = [&](int rmax) {
-    const int fixed = stg_al16(4 * (rmax + 8)) + tvecs * stg_al16((int)sizeof(T) * (rmax + 8));
-    return ((budget - fixed) / es - 16 - 16) & ~15;  // the col/val slices round up to 16 bytes each
-  };
-  int rmax = 32, emax = emax_for(32);
-  for (int r = 256; r >= 32; r /= 2)
-    if (emax_for(r) > 0 && r * avg <= emax_for(r)) {
-      rmax = r;
-      emax = emax_for(r);
-      break;
-    }
-  int maxrow = 0;
-  for (int i = 0; i < h.nr; ++i) maxrow = std::max(maxrow, h.irp[i + 1] - h.irp[i]);
-  if (emax <= 0 || maxrow > emax) return;
-  std::vector<int4> tiles;
-  tiles.reserve((size_t)h.nr / rmax + 1);
-  for (int r = 0; r < h.nr;) {
-    int r1 = r + 1;  // a tile holds at least one row (maxrow <= emax)
-    while (r1 < h.nr && r1 - r < rmax && h.irp[r1 + 1] - h.irp[r] <= emax) ++r1;
-    tiles.push_back(make_int4(r, r1, h.irp[r], h.irp[r1]));
-    r = r1;
-  }
-  d.tiles = ar.upload(tiles);
-  d.ntiles = (int)tiles.size();
-  d.trmax = rmax;
-  d.temax = emax;
-  d.tvecs = tvecs;
-  d.stpr = d.stpr0 = pick_tpr(h.nnz(), h.nr);
-}
-
 // FP16 row-scaled copies of a level operator's values (CSR and, when built,
 // SELL order): rs_i = max_j |a_ij| rounded to FP32, h_ij = a_ij / rs_i
 // rounded to FP32 and then to FP16 (round to nearest even), so |h_ij| <= 1.
-template <typename T>
-static void make_h16(Arena &ar, const HostCSR &h, DCSR<T> &d) {
-  std::vector<float> sc((size_t)h.nr, 1.f);
-  std::vector<__half> hv(h.val.size());
+static void h16_values(const HostCSR &h, std::vector<float> &sc, std::vector<__half> &hv) {
+  sc.assign((size_t)h.nr, 1.f);
+  hv.resize(h.val.size());
 #pragma omp parallel for schedule(static, 4096)
   for (int i = 0; i < h.nr; ++i) {
     double mx = 0;
@@ -472,6 +428,12 @@ static void make_h16(Arena &ar, const HostCSR &h, DCSR<T> &d) {
     sc[i] = s;
     for (int k = h.irp[i]; k < h.irp[i + 1]; ++k) hv[k] = __float2half_rn((float)(h.val[k] / (double)s));
   }
+}
+template <typename T>
+static void make_h16(Arena &ar, const HostCSR &h, DCSR<T> &d) {
+  std::vector<float> sc;
+  std::vector<__half> hv;
+  h16_values(h, sc, hv);
   d.rs = ar.upload(sc);
   d.hval = ar.upload(hv);
   if (d.soff) {
@@ -491,8 +453,95 @@ static void make_h16(Arena &ar, const HostCSR &h, DCSR<T> &d) {
   }
 }
 
+// Staged SELL tiles (mldg_spmv_stg.cuh): the SELL-32 slots of the operator,
+// in the order build_sell stores them (same widths, same padding columns,
+// zero padding values), cut into tiles of consecutive slices whose packed
+// block fits kStgBlockMax bytes, and packed: header {slices, slots, col
+// offset, val offset}, the slices' slot offsets from the tile's first slot,
+// the column offsets (int16 from the row, or int32), the values (T, or the
+// FP16 row-scaled values in the FP16 form), each part 16-byte aligned.
+// Built only on request (MLDG_STG: offered to the autotuner; MLDG_STG_FORCE:
+// used), and not without a SELL copy or when one slice alone exceeds the
+// budget.
 template <typename T>
-static DCSR<T> to_dev(Arena &ar, const HostCSR &h, bool h16 = false, int stg_vecs = 2) {
+static void build_stg_pack(Arena &ar, const HostCSR &h, DCSR<T> &d, bool h16) {
+  if (!(std::getenv("MLDG_STG") || std::getenv("MLDG_STG_FORCE")) || !d.soff || h.nr == 0) return;
+  const int ns = d.nslice();
+  std::vector<int> soff((size_t)ns + 1, 0);
+  for (int sl = 0; sl < ns; ++sl) {
+    int w = 0;
+    for (int i = sl * 32; i < std::min(h.nr, sl * 32 + 32); ++i) w = std::max(w, h.irp[i + 1] - h.irp[i]);
+    soff[sl + 1] = soff[sl] + 32 * w;
+  }
+  if ((int64_t)soff[ns] != d.slots) return;  // not the SELL copy's layout: no tiles
+  const bool rel = d.jd != nullptr;
+  const int ci = rel ? 2 : 4, vb = h16 ? 2 : (int)sizeof(T);
+  auto block_bytes = [&](int s0, int s1) {
+    const int slots = soff[s1] - soff[s0];
+    return 16 + stg_al16(4 * (s1 - s0 + 1)) + stg_al16(ci * slots) + stg_al16(vb * slots);
+  };
+  std::vector<int4> tiles;
+  int64_t total = 0;
+  int tmax = 0;
+  for (int s0 = 0; s0 < ns;) {
+    if (block_bytes(s0, s0 + 1) > kStgBlockMax) return;
+    int s1 = s0 + 1;
+    while (s1 < ns && block_bytes(s0, s1 + 1) <= kStgBlockMax) ++s1;
+    const int bb = block_bytes(s0, s1);
+    if ((total + bb) / 16 > INT32_MAX) return;
+    tiles.push_back(make_int4(s0, s1, (int)(total / 16), bb / 16));
+    total += bb;
+    tmax = std::max(tmax, bb);
+    s0 = s1;
+  }
+  std::vector<float> sc;
+  std::vector<__half> hv;
+  if (h16) h16_values(h, sc, hv);
+  std::vector<uint4> pk((size_t)(total / 16), make_uint4(0, 0, 0, 0));
+  unsigned char *base = reinterpret_cast<unsigned char *>(pk.data());
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int t = 0; t < (int)tiles.size(); ++t) {
+    const int4 td = tiles[t];
+    unsigned char *blk = base + (size_t)td.z * 16;
+    const int nsl = td.y - td.x, slots = soff[td.y] - soff[td.x];
+    const int off_col = 16 + stg_al16(4 * (nsl + 1)), off_val = off_col + stg_al16(ci * slots);
+    int *hdr = reinterpret_cast<int *>(blk);
+    hdr[0] = nsl;
+    hdr[1] = slots;
+    hdr[2] = off_col;
+    hdr[3] = off_val;
+    for (int q = 0; q <= nsl; ++q) hdr[4 + q] = soff[td.x + q] - soff[td.x];
+    for (int sl = td.x; sl < td.y; ++sl) {
+      const int w = (soff[sl + 1] - soff[sl]) / 32;
+      for (int lane = 0; lane < 32; ++lane) {
+        const int i = sl * 32 + lane;
+        const int len = i < h.nr ? h.irp[i + 1] - h.irp[i] : 0;
+        const int pad_col = i < h.nr ? (h.nr == h.nc ? i : 0) : (h.nr == h.nc ? h.nr - 1 : 0);
+        for (int k = 0; k < w; ++k) {
+          const size_t e = (size_t)(soff[sl] - soff[td.x]) + 32 * (size_t)k + lane;
+          const int col = k < len ? h.ja[h.irp[i] + k] : pad_col;
+          if (rel)
+            reinterpret_cast<short *>(blk + off_col)[e] = (short)(col - i);
+          else
+            reinterpret_cast<int *>(blk + off_col)[e] = col;
+          if (k < len) {
+            if (h16)
+              reinterpret_cast<__half *>(blk + off_val)[e] = hv[h.irp[i] + k];
+            else
+              reinterpret_cast<T *>(blk + off_val)[e] = (T)h.val[h.irp[i] + k];
+          }
+        }
+      }
+    }
+  }
+  d.tiles = ar.upload(tiles);
+  d.pk = ar.upload(pk);
+  d.ntiles = (int)tiles.size();
+  d.tblock = tmax;
+}
+
+template <typename T>
+static DCSR<T> to_dev(Arena &ar, const HostCSR &h, bool h16 = false) {
   DCSR<T> d;
   if (!h.present()) return d;
   d.nr = h.nr;
@@ -517,8 +566,8 @@ static DCSR<T> to_dev(Arena &ar, const HostCSR &h, bool h16 = false, int stg_vec
   d.val = ar.upload(v);
   d.tpr = pick_tpr(d.nnz, d.nr);
   build_sell(ar, h, d);
-  build_stg_plan(ar, h, d, stg_vecs);
   if (h16) make_h16(ar, h, d);
+  build_stg_pack(ar, h, d, h16);
   return d;
 }
 
@@ -770,6 +819,9 @@ struct EngineT : Engine {
     // coarsest level: explicit inverse of its ILU(0) factorisation (and its transpose)
     T *minv = nullptr, *minvT = nullptr;
     T *rp0 = nullptr, *rp1 = nullptr;  // right-hand sides in position order
+    // point-Jacobi levels with at most two sweeps (every sweep a first one):
+    // ND and ND^T stored with their columns scaled by d (k_jacobi first == 2)
+    bool nd_scaled = false;
     // FP16 prolongator values + FP32 row scale (MLDG_PREC_FP32_P16)
     __half *Ph = nullptr;
     float *Pscale = nullptr;
@@ -796,69 +848,40 @@ struct EngineT : Engine {
   }
   // values of type V (T, or FP16 with the row scales rs)
   int stg_stages = kStgStages;
-  template <int K, typename F>
-  static void tpr_case(int tpr, F &&f) {
-    if (tpr == K) f(std::integral_constant<int, K>());
-  }
-  template <typename F>
-  void tpr_dispatch(int tpr, F &&f) {
-    if (tpr != 1 && tpr != 2 && tpr != 4 && tpr != 8 && tpr != 16 && tpr != 32) fail(MLDG_ERR_INTERNAL, "bad tpr %d", tpr);
-    tpr_case<1>(tpr, f);
-    tpr_case<2>(tpr, f);
-    tpr_case<4>(tpr, f);
-    tpr_case<8>(tpr, f);
-    tpr_case<16>(tpr, f);
-    tpr_case<32>(tpr, f);
-  }
-  // the staged kernels' bulk copies read every array from a 16-byte boundary
-  static bool al16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
-  // ring depth of a launch: the configured stages, fewer if they would not fit
-  template <typename V, typename CI>
-  int stg_fit(const DCSR<T> &A, int nvec) const {
+  // ring depth of a staged launch: the configured stages, fewer if they would not fit
+  int stg_fit(const DCSR<T> &A) const {
     int sgs = stg_stages;
-    while (sgs > 2 && stg_smem(stg_layout<T, V, CI>(A.trmax, A.temax, sgs, nvec)) > kStgSmemMax) --sgs;
+    while (sgs > kStgStages && stg_smem(sgs, A.tblock) > kStgSmemMax) --sgs;
     return sgs;
   }
-  template <typename V, typename CI>
-  StgArgs<T, V, CI> stg_args(const DCSR<T> &A, const CI *cj, const V *val, const float *rs, int nvec) {
-    StgArgs<T, V, CI> a{};
+  StgArgs stg_args(const DCSR<T> &A, const float *rs) {
+    StgArgs a{};
     a.ntiles = A.ntiles;
+    a.nr = A.nr;
+    a.stages = stg_fit(A);
+    a.block_bytes = A.tblock;
     a.tiles = A.tiles;
-    a.irp = A.irp;
-    a.cj = cj;
-    a.val = val;
+    a.pk = A.pk;
     a.rs = rs;
-    a.L = stg_layout<T, V, CI>(A.trmax, A.temax, stg_fit<V, CI>(A, nvec), nvec);
     a.err = err;
     return a;
   }
   // fill the staged kernels' launch cache for every (kernel, shared memory)
-  // pair an operator can launch: both kinds, the autotuner's three lanes-per-
-  // row choices, every count of staged vectors
-  template <typename V, typename CI>
-  void stg_prepare_op(const DCSR<T> &A) {
-    for (int sp : {A.stpr0 / 2, A.stpr0, A.stpr0 * 2}) {
-      if (sp < 1 || sp > 32) continue;
-      for (int nv = 0; nv <= A.tvecs; ++nv) {
-        const size_t sm = stg_smem(stg_layout<T, V, CI>(A.trmax, A.temax, stg_fit<V, CI>(A, nv), nv));
-        tpr_dispatch(sp, [&](auto kc) {
-          constexpr int K = decltype(kc)::value;
-          if (nv <= 2) stg_occ(k_spmv_stg<T, V, CI, K>, sm);
-          if (nv >= 2) stg_occ(k_jacobi_stg<T, V, CI, K>, sm);
-        });
-      }
-    }
-  }
+  // pair the operators can launch, before any stream capture
   void stg_prepare() {
     for (auto &L : lv)
       for (DCSR<T> *op : {&L.A, &L.AT, &L.P, &L.R, &L.ND, &L.NDT}) {
         if (!op->tiles) continue;
+        const size_t sm = stg_smem(stg_fit(*op), op->tblock);
         auto go = [&](auto vtag) {
           using V = typename decltype(vtag)::type;
-          if (op->jd)
-            stg_prepare_op<V, short>(*op);
-          else
-            stg_prepare_op<V, int>(*op);
+          if (op->jd) {
+            stg_occ(k_spmv_stg<T, V, short>, sm);
+            stg_occ(k_jacobi_stg<T, V, short>, sm);
+          } else {
+            stg_occ(k_spmv_stg<T, V, int>, sm);
+            stg_occ(k_jacobi_stg<T, V, int>, sm);
+          }
         };
         if constexpr (std::is_same<T, float>::value) {
           if (op->h16()) {
@@ -870,56 +893,31 @@ struct EngineT : Engine {
       }
   }
   template <typename V>
-  void spmv_stg(const DCSR<T> &A, const V *val, const float *rs, const T *v, T a1, const T *b, T a0, T *out,
-                T a2) {
-    const int nvec = (b ? 1 : 0) + (a2 != T(0) ? 1 : 0);
-    auto go = [&](auto *cj) {
-      using CI = std::remove_const_t<std::remove_pointer_t<decltype(cj)>>;
-      StgArgs<T, V, CI> a = stg_args<V, CI>(A, cj, val, rs, nvec);
-      int q = 0;
-      if (b) a.vec[q++] = b;
-      if (a2 != T(0)) a.vec[q++] = out;
-      tpr_dispatch(A.stpr, [&](auto kc) {
-        stg_launch(k_spmv_stg<T, V, CI, decltype(kc)::value>, stg_smem(a.L), A.ntiles, nsm, st, a, v, a1,
-                   b ? 1 : 0, a0, out, a2);
-      });
-    };
+  void spmv_stg(const DCSR<T> &A, const float *rs, const T *v, T a1, const T *b, T a0, T *out, T a2) {
+    const StgArgs a = stg_args(A, rs);
+    const size_t sm = stg_smem(a.stages, a.block_bytes);
     if (A.jd)
-      go((const short *)A.jd);
+      stg_launch(k_spmv_stg<T, V, short>, sm, A.ntiles, nsm, st, a, v, a1, b, a0, out, a2);
     else
-      go((const int *)A.ja);
+      stg_launch(k_spmv_stg<T, V, int>, sm, A.ntiles, nsm, st, a, v, a1, b, a0, out, a2);
   }
   template <typename V>
-  void jacobi_stg(const DCSR<T> &ND, const V *val, const float *rs, const T *d, const T *x, const T *ty, int first,
-                  T omega, T alpha, T beta, T *out) {
-    const bool use_ty = !first && omega != T(1);
-    const int nvec = 2 + (use_ty ? 1 : 0) + (beta != T(0) ? 1 : 0);
-    auto go = [&](auto *cj) {
-      using CI = std::remove_const_t<std::remove_pointer_t<decltype(cj)>>;
-      StgArgs<T, V, CI> a = stg_args<V, CI>(ND, cj, val, rs, nvec);
-      int q = 0;
-      a.vec[q++] = d;
-      a.vec[q++] = x;
-      if (use_ty) a.vec[q++] = ty;
-      if (beta != T(0)) a.vec[q++] = out;
-      tpr_dispatch(ND.stpr, [&](auto kc) {
-        stg_launch(k_jacobi_stg<T, V, CI, decltype(kc)::value>, stg_smem(a.L), ND.ntiles, nsm, st, a, d, x, ty,
-                   first, omega, alpha, beta, out);
-      });
-    };
+  void jacobi_stg(const DCSR<T> &ND, const float *rs, const T *d, const T *x, const T *ty, int first, T omega,
+                  T alpha, T beta, T *out) {
+    const StgArgs a = stg_args(ND, rs);
+    const size_t sm = stg_smem(a.stages, a.block_bytes);
     if (ND.jd)
-      go((const short *)ND.jd);
+      stg_launch(k_jacobi_stg<T, V, short>, sm, ND.ntiles, nsm, st, a, d, x, ty, first, omega, alpha, beta, out);
     else
-      go((const int *)ND.ja);
+      stg_launch(k_jacobi_stg<T, V, int>, sm, ND.ntiles, nsm, st, a, d, x, ty, first, omega, alpha, beta, out);
   }
   template <typename V>
   void spmv_v(const DCSR<T> &A, const V *val, const V *sval, const float *rs, const T *v, T a1, const T *b,
               T a0, T *out, T a2) {
     const int64_t vec = (int64_t)A.nc * sizeof(T) + (int64_t)A.nr * sizeof(T) * (1 + (b ? 1 : 0) + (a2 != T(0) ? 1 : 0));
-    if (A.sell == 4 && (b ? 1 : 0) + (a2 != T(0) ? 1 : 0) <= A.tvecs && al16(A.irp) && al16(A.jd ? (const void *)A.jd : (const void *)A.ja) && al16(val) &&
-        al16(b) && (a2 == T(0) || al16(out))) {
+    if (A.sell == 4 && A.tiles) {
       begin(MLDG_KERNEL_SPMV);
-      spmv_stg<V>(A, val, rs, v, a1, b, a0, out, a2);
+      spmv_stg<V>(A, rs, v, a1, b, a0, out, a2);
       end(A.alg_bytes() + vec);
       return;
     }
@@ -975,11 +973,9 @@ struct EngineT : Engine {
   void jacobi_v(const DCSR<T> &ND, const V *val, const V *sval, const float *rs, const T *d, const T *x,
                 const T *ty, int first, T omega, T alpha, T beta, T *out) {
     const int64_t vec = (int64_t)ND.nr * sizeof(T) * (3 + (first ? 0 : 1) + (beta != T(0) ? 1 : 0));
-    if (ND.sell == 4 && 2 + (!first && omega != T(1) ? 1 : 0) + (beta != T(0) ? 1 : 0) <= ND.tvecs &&
-        al16(ND.irp) && al16(ND.jd ? (const void *)ND.jd : (const void *)ND.ja) && al16(val) &&
-        al16(d) && al16(x) && al16(ty) && (beta == T(0) || al16(out))) {
+    if (ND.sell == 4 && ND.tiles) {
       begin(MLDG_KERNEL_JACOBI);
-      jacobi_stg<V>(ND, val, rs, d, x, ty, first, omega, alpha, beta, out);
+      jacobi_stg<V>(ND, rs, d, x, ty, first, omega, alpha, beta, out);
       end(ND.alg_bytes() + vec);
       return;
     }
@@ -1404,7 +1400,7 @@ struct EngineT : Engine {
     for (int s = 1; s < sweeps; ++s) {
       const bool last = (s == sweeps - 1);
       T *dst = last ? y : bufs[s & 1];
-      jacobi(ND, L.d, x, src, s == 1 ? 1 : 0, w, T(1), last ? beta : T(0), dst);
+      jacobi(ND, L.d, x, src, s == 1 ? (L.nd_scaled ? 2 : 1) : 0, w, T(1), last ? beta : T(0), dst);
       src = dst;
     }
   }
@@ -1617,22 +1613,15 @@ struct EngineT : Engine {
         const bool sweep = oi >= 4 && L.kind == MLDG_SMOOTHER_JACOBI && L.d && op->nr == op->nc;
         auto run = [&]() {
           if (sweep)
-            jacobi(*op, L.d, v, nullptr, 1, (T)L.damp, T(1), T(0), o);
+            jacobi(*op, L.d, v, nullptr, L.nd_scaled ? 2 : 1, (T)L.damp, T(1), T(0), o);
           else
             spmv(*op, v, T(1), nullptr, T(0), o, T(0));
         };
-        int best_stpr = op->stpr0;
-        // t = -4, -5, -6: the staged kernels with the mean-length lanes per
-        // row, twice and half that
-        for (int t : {1, 2, 4, 8, 16, 32, -1, -2, -3, -4, -5, -6}) {
+        // t = -4: the staged SELL kernels
+        for (int t : {1, 2, 4, 8, 16, 32, -1, -2, -3, -4}) {
           if (t < 0 && t >= -3 && !op->soff) continue;
-          if (t <= -4) {
-            if (!op->tiles) continue;
-            const int sp = t == -4 ? op->stpr0 : (t == -5 ? op->stpr0 * 2 : op->stpr0 / 2);
-            if (sp < 1 || sp > 32 || (t != -4 && sp == op->stpr0)) continue;
-            op->stpr = sp;
-          }
-          op->sell = t < 0 ? std::min(-t, 4) : 0;
+          if (t == -4 && !op->tiles) continue;
+          op->sell = t < 0 ? -t : 0;
           if (t > 0) op->tpr = t;
           run();  // warm
           MLDG_CUDA(cudaEventRecord(e0, st));
@@ -1644,18 +1633,16 @@ struct EngineT : Engine {
           if (ms < best) {
             best = ms;
             best_t = t > 0 ? t : best_t;
-            best_sell = t < 0 ? std::min(-t, 4) : 0;
-            if (t <= -4) best_stpr = op->stpr;
+            best_sell = t < 0 ? -t : 0;
           }
         }
         op->tpr = best_t;
         op->sell = best_sell;
-        op->stpr = best_stpr;
         if (std::getenv("MLDG_VERBOSE"))
           std::fprintf(stderr, "mldg: spmv autotune level %zu %-4s n=%d nnz=%lld -> %s%d %.4f ms\n", l,
                        names[oi], op->nr, (long long)op->nnz,
-                       best_sell == 4 ? "staged tpr " : (best_sell ? "sell" : "csr tpr "),
-                       best_sell == 4 ? best_stpr : (best_sell ? best_sell : best_t), best / reps);
+                       best_sell == 4 ? "staged sell" : (best_sell ? "sell" : "csr tpr "),
+                       best_sell == 4 ? 1 : (best_sell ? best_sell : best_t), best / reps);
       }
     }
     launches = 0;
@@ -2196,7 +2183,7 @@ struct EngineT : Engine {
     for (int s = 1; s < sweeps; ++s) {
       const bool last = (s == sweeps - 1);
       T *dst = last ? y : bufs[s & 1];
-      jacobi_m(ND, L.d, x, src, s == 1 ? 1 : 0, w, T(1), last ? beta : T(0), dst);
+      jacobi_m(ND, L.d, x, src, s == 1 ? (L.nd_scaled ? 2 : 1) : 0, w, T(1), last ? beta : T(0), dst);
       src = dst;
     }
   }
@@ -3890,8 +3877,20 @@ static Engine *make_engine(Handle *h) {
       }
     }
     if (H.ND.present() && L.nnz_nd > 0) {
-      L.ND = to_dev<T>(ar, H.ND, h16, kStgVecs);
-      L.NDT = to_dev<T>(ar, transpose(H.ND), h16, kStgVecs);
+      if (H.kind == MLDG_SMOOTHER_JACOBI && std::max(H.sweeps_pre, H.sweeps_post) <= 2 &&
+          !std::getenv("MLDG_NO_ND_SCALE")) {
+        // only first sweeps: ND D and ND^T D (columns scaled by d = 1/a_jj)
+        auto colscale = [&](HostCSR m) {
+          for (size_t k = 0; k < m.ja.size(); ++k) m.val[k] *= dh[m.ja[k]];
+          return m;
+        };
+        L.ND = to_dev<T>(ar, colscale(H.ND), h16);
+        L.NDT = to_dev<T>(ar, colscale(transpose(H.ND)), h16);
+        L.nd_scaled = true;
+      } else {
+        L.ND = to_dev<T>(ar, H.ND, h16);
+        L.NDT = to_dev<T>(ar, transpose(H.ND), h16);
+      }
     }
     tick("FBGS factors, ND");
     if (H.kind == MLDG_SMOOTHER_BJAC && l == h->nlev - 1 && h->nlev > 1 && L.n <= kDenseCoarseRows &&
@@ -4050,8 +4049,7 @@ static Engine *make_engine(Handle *h) {
           const int f = std::atoi(std::getenv("MLDG_SELL_FORCE"));
           op->sell = (f >= 1 && f <= 3) ? f : 1;
         }
-  // MLDG_STG_FORCE: every operator with a staged plan uses it (lanes per row
-  // from the mean row length unless the autotuner chose)
+  // MLDG_STG_FORCE: every operator with staged tiles uses them
   if (std::getenv("MLDG_STG_FORCE"))
     for (auto &L : e->lv)
       for (DCSR<T> *op : {&L.A, &L.AT, &L.P, &L.R, &L.ND, &L.NDT})

@@ -124,12 +124,18 @@ __device__ __forceinline__ T ldval(const V *__restrict__ p, int64_t k) {
   else
     return p[k];
 }
+// (a rounded product that is never contracted into a later add: every
+// kernel rounds the scaled row sum alike)
 template <typename T, typename V>
 __device__ __forceinline__ T row_scaled(T acc, const float *__restrict__ rs, int row) {
-  if constexpr (std::is_same<V, __half>::value)
-    return acc * (T)rs[row];
-  else
+  if constexpr (std::is_same<V, __half>::value) {
+    if constexpr (std::is_same<T, float>::value)
+      return __fmul_rn(acc, rs[row]);
+    else
+      return __dmul_rn(acc, (double)rs[row]);
+  } else {
     return acc;
+  }
 }
 
 // The point-Jacobi update of one row from its off-diagonal sum s, every
@@ -151,13 +157,20 @@ __device__ __forceinline__ T jac_row(T di, T xi, T s, T tyi, bool first, T omega
 
 // One lane's part of a CSR row sum: entries k = k0, k0 + TPR, ... < e,
 // s = fma(val[k], g(col k), s) in that order from zero.  The loads are
-// issued kCsrU entries at a time (column indices and values, then the
-// gathers g, then the sums), so a long row costs two memory latencies per
-// kCsrU entries instead of two per entry; the sums are the plain loop's.
-constexpr int kCsrU = 4;
+// issued U entries at a time (column indices and values, then the gathers
+// g, then the sums), so a long row costs two memory latencies per U entries
+// instead of two per entry; the sums are the plain loop's.  U grows with the
+// lanes per row, which the autotuner picks wide for long rows: 4 entries per
+// lane below 4 lanes per row, 8 up to 8 lanes, 16 from 16 lanes (a coarse
+// level's row of ~300 entries then takes one batch).
+template <int TPR>
+struct CsrU {
+  static constexpr int value = TPR >= 16 ? 16 : (TPR >= 4 ? 8 : 4);
+};
 template <typename T, int TPR, typename CI, typename V, typename G>
 __device__ __forceinline__ T csr_lane_sum(int k0, int e, int row, const CI *__restrict__ ja,
                                           const V *__restrict__ val, G g) {
+  constexpr int kCsrU = CsrU<TPR>::value;
   T s = T(0);
   for (int k = k0; k < e; k += TPR * kCsrU) {
     T vv[kCsrU], xv[kCsrU];
@@ -383,7 +396,9 @@ __global__ void __launch_bounds__(256) k_jacobi_sellp(int nr, const int *__restr
     out[row] = jac_row(d[row], x[row], row_scaled<T, V>(acc, rs, row), (!first && omega != T(1)) ? ty[row] : T(0),
                        first != 0, omega, alpha, beta, beta != T(0) ? out[row] : T(0));
   };
-  if (first)
+  if (first == 2)
+    sellp_loop<T, CI>(nr, soff, sj, sv, [&](int j) { return omega * __ldg(x + j); }, done);
+  else if (first)
     sellp_loop<T, CI>(
         nr, soff, sj, sv, [&](int j) { return omega * (__ldg(d + j) * __ldg(x + j)); }, done);
   else
@@ -403,7 +418,9 @@ __global__ void __launch_bounds__(256) k_jacobi_sell(int nr, const int *__restri
   const int ns = (nr + 31) >> 5;
   for (int sl0 = warp * S; sl0 < ns; sl0 += nwarps * S) {
     T acc[S];
-    if (first)
+    if (first == 2)
+      sell_rows<T, CI, S>(soff, sj, sv, sl0, ns, lane, [&](int j) { return omega * __ldg(x + j); }, acc);
+    else if (first)
       sell_rows<T, CI, S>(soff, sj, sv, sl0, ns, lane,
                           [&](int j) { return omega * (__ldg(d + j) * __ldg(x + j)); }, acc);
     else
@@ -454,7 +471,10 @@ __global__ void __launch_bounds__(256) k_spmv_h(int nr, const int *__restrict__ 
 //   v_i  = (omega == 1) ? t_i : (1-omega)*ty_i + omega*t_i        (damping: extension)
 //   out_i = alpha*v_i + beta*out_i
 // When first != 0 the incoming iterate is ty = omega*d o x (the unrolled first
-// sweep, :136), computed on the fly from x and d instead of being stored.
+// sweep, :136), computed on the fly from x and d instead of being stored;
+// first == 2 says that ND's columns were scaled by d when it was stored
+// (ND D), so the sweep gathers omega*x_j alone: one vector gather per entry
+// instead of two.
 template <typename T, int TPR, typename CI = int, typename V = T>
 __global__ void __launch_bounds__(256) k_jacobi(int nr, const int *__restrict__ irp,
                                                 const CI *__restrict__ ja,
@@ -475,7 +495,9 @@ __global__ void __launch_bounds__(256) k_jacobi(int nr, const int *__restrict__ 
     T s = T(0);
     if (row < nr) {
       const int k0 = irp[row] + sub, e = irp[row + 1];
-      if (first)
+      if (first == 2)
+        s = csr_lane_sum<T, TPR>(k0, e, row, ja, val, [&](int j) { return omega * __ldg(x + j); });
+      else if (first)
         s = csr_lane_sum<T, TPR>(k0, e, row, ja, val, [&](int j) { return omega * (__ldg(d + j) * __ldg(x + j)); });
       else
         s = csr_lane_sum<T, TPR>(k0, e, row, ja, val, [&](int j) { return __ldg(ty + j); });

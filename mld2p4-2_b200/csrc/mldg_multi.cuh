@@ -57,7 +57,9 @@ __global__ void __launch_bounds__(256) k_jacobi_m(int nr, const int *__restrict_
     const int row = (int)(t / K), c = (int)(t % K);
     T s = T(0);
     const int e = irp[row + 1];
-    if (first) {
+    if (first == 2) {
+      for (int k = irp[row]; k < e; ++k) s = fma(val[k], omega * __ldg(x + (size_t)ja[k] * K + c), s);
+    } else if (first) {
       for (int k = irp[row]; k < e; ++k) {
         const int j = ja[k];
         s = fma(val[k], omega * (__ldg(d + j) * __ldg(x + (size_t)j * K + c)), s);

@@ -3,7 +3,9 @@
 Every level's A, P, R and Jacobi off-diagonal part ND is stored as FP16
 values with an FP32 row scale: rs_i = max_j |a_ij| rounded to FP32,
 h_ij = a_ij / rs_i rounded to FP32 and then to FP16 (nearest even), and the
-kernels form rs_i * sum_j h_ij x_j.  Two bars:
+kernels form rs_i * sum_j h_ij x_j.  (A point-Jacobi level of at most two
+sweeps stores ND with its columns scaled by the inverse diagonal, so there
+the quantized matrix is ND D.)  Two bars:
 
 * exactness of the form: the FP16 apply equals, to FP32 accuracy, the FP64
   apply of the same hierarchy whose A, P, R and ND were quantized that way
@@ -58,11 +60,23 @@ def _upload(mld, orc, op, quantized, precision):
             return mld.CSR(m.irp, m.ja, v, ncols=m.ncols)
 
         d = op.level_vec(l, "d") if tri else op.level_vec(l, "dinv")
+
+        def conv_nd(m):
+            # a point-Jacobi level of at most two sweeps stores ND with its
+            # columns scaled by d, and the FP16 form quantizes that product
+            if m is None or not quantized or tri or info["sweeps_pre"] > 2:
+                return conv(m)
+            dc = np.asarray(d)[np.asarray(m.ja)]
+
+            class S:
+                irp, val = m.irp, np.asarray(m.val) * dc
+            return mld.CSR(m.irp, m.ja, quantize_h16(S) / dc, ncols=m.ncols)
+
         h.upload_level(
             l, conv(op.level_csr(l, "A")),
             P=conv(op.level_csr(l, "P")) if l else None,
             R=conv(op.level_csr(l, "R")) if l else None,
-            ND=conv(op.level_csr(l, "ND")) if info["nnzND"] else None,
+            ND=conv_nd(op.level_csr(l, "ND")) if info["nnzND"] else None,
             L=conv(op.level_csr(l, "L"), False) if tri else None,
             U=conv(op.level_csr(l, "U"), False) if tri else None,
             d=d, smoother=kind, sweeps_pre=info["sweeps_pre"], sweeps_post=info["sweeps_pre"],

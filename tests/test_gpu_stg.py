@@ -1,15 +1,15 @@
-"""GPU: the staged CSR kernels (k_spmv_stg, k_jacobi_stg: TMA bulk copies of
-row tiles into a shared-memory ring, mldg_spmv_stg.cuh).
+"""GPU: the staged SELL kernels (k_spmv_stg, k_jacobi_stg: one TMA bulk copy
+of a packed tile of SELL-32 slices per stage of a per-warp shared-memory
+ring, mldg_spmv_stg.cuh).
 
-A staged kernel sums each row exactly like the per-thread CSR kernel with
-the same lanes per row (stored order per lane, then the butterfly), so with
-launch shapes pinned (no autotuning: CSR with the mean-row-length lanes per
-row) a hierarchy whose operators all take the staged kernels
-(MLDG_STG_FORCE) must apply bit for bit like the CSR one -- in every
-precision form, for trans 'N' and 'T', with the default tiles, with small
-tiles that force rows longer than a tile's entry budget into tiles of their
-own and a two-stage ring that wraps many times, and with an eight-stage
-ring.  The staged applies also meet the FP64 bar against the oracle."""
+A staged kernel sums each row exactly like the SELL kernel (slots in stored
+order from zero, padding included), so with launch shapes pinned (no
+autotuning) a hierarchy whose operators take the staged kernels
+(MLDG_STG_FORCE) must apply bit for bit like the one whose operators take
+the SELL kernel (MLDG_SELL_FORCE=1) -- in every precision form, for trans 'N'
+and 'T', with the two-stage ring the tiles are sized for and with the
+deepest ring that fits.  The staged applies also meet the FP64 bar against
+the oracle."""
 import numpy as np
 import pytest
 
@@ -17,7 +17,7 @@ from conftest import ANISO, ISO, oracle_params, upload_oracle_hierarchy
 
 pytestmark = pytest.mark.gpu
 
-CASES = [{}, {"MLDG_STG_E": "256", "MLDG_STG_S": "2"}, {"MLDG_STG_S": "8"}]
+CASES = [{}, {"MLDG_STG_S": "4"}]
 
 
 @pytest.fixture(scope="module")
@@ -31,11 +31,12 @@ def hier(orc):
 
 @pytest.mark.parametrize("env", CASES)
 @pytest.mark.parametrize("prec", [0, 1, 3])
-def test_staged_apply_bitwise_equal_to_csr(mld, orc, hier, monkeypatch, prec, env):
+def test_staged_apply_bitwise_equal_to_sell(mld, orc, hier, monkeypatch, prec, env):
     a, op = hier
     monkeypatch.setenv("MLDG_NO_AUTOTUNE", "1")
     monkeypatch.setenv("MLDG_NO_DENSE_INV", "1")
-    h_csr = upload_oracle_hierarchy(mld, orc, op, precision=prec)
+    monkeypatch.setenv("MLDG_SELL_FORCE", "1")
+    h_sell = upload_oracle_hierarchy(mld, orc, op, precision=prec)
     for k, v in env.items():
         monkeypatch.setenv(k, v)
     monkeypatch.setenv("MLDG_STG_FORCE", "1")
@@ -43,12 +44,12 @@ def test_staged_apply_bitwise_equal_to_csr(mld, orc, hier, monkeypatch, prec, en
     rng = np.random.default_rng(3)
     for trans in ("N", "T"):
         x = rng.uniform(-1, 1, a.nrows)
-        y_csr, y_stg = h_csr.apply(x, trans=trans), h_stg.apply(x, trans=trans)
-        assert np.array_equal(y_csr, y_stg), (trans, np.abs(y_csr - y_stg).max())
+        y_sell, y_stg = h_sell.apply(x, trans=trans), h_stg.apply(x, trans=trans)
+        assert np.array_equal(y_sell, y_stg), (trans, np.abs(y_sell - y_stg).max())
         if prec == 0:
             y_ref = op.apply(x, trans)
             assert np.linalg.norm(y_stg - y_ref) <= 1e-12 * np.linalg.norm(y_ref)
-    h_csr.close()
+    h_sell.close()
     h_stg.close()
 
 
