@@ -213,6 +213,29 @@ static void stg_launch(K kern, size_t smem, int ntiles, int nsm, cudaStream_t st
   kern<<<grid, kStgThreads, smem, st>>>(args...);
 }
 
+// Launch of a streaming kernel, with programmatic dependent launch when pdl
+// is set: the kernel (which calls pdl_enter first) may be scheduled while
+// the previous kernel in the stream finishes, so the gap between dependent
+// launches of a V-cycle or a Krylov iteration shrinks.
+template <typename... KArgs, typename... Args>
+static void launch_k(bool pdl, void (*kern)(KArgs...), int grid, int block, cudaStream_t st, Args... args) {
+  if (!pdl) {
+    kern<<<grid, block, 0, st>>>(args...);
+    return;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  MLDG_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
+}
+
 template <typename T>
 struct DCSR {
   int nr = 0, nc = 0;
@@ -231,8 +254,20 @@ struct DCSR {
   int64_t slots = 0;
   // 0: CSR kernels; 1 or 2: SELL kernels with that many slices per warp
   // iteration; 3: the software-pipelined SELL kernels (k_spmv_sellp,
-  // k_jacobi_sellp); 4: the staged SELL kernels (k_spmv_stg, k_jacobi_stg)
+  // k_jacobi_sellp); 4: the staged SELL kernels (k_spmv_stg, k_jacobi_stg);
+  // 5: the HDIA kernels (k_spmv_hdia, k_jacobi_hdia)
   int sell = 0;
+  // hacked-diagonal copy (HDIA-32, see k_spmv_hdia) of a square operator:
+  // per slice of 32 rows its ascending column offsets (hdoff from
+  // hdptr[s]) and one value per (offset, row); values of type T, or FP16
+  // row-scaled (hdhval) in the FP16 operator form; built when the slices
+  // share few diagonals, used when the autotuner finds it faster
+  int *hdptr = nullptr, *hdoff = nullptr;
+  T *hdval = nullptr;
+  __half *hdhval = nullptr;
+  int64_t hdslots = 0;
+  bool hdia() const { return sell == 5 && hdptr != nullptr; }
+  int hd_nslice() const { return nslice(); }
   // staged SELL tiles (k_spmv_stg, k_jacobi_stg): packed blocks of
   // consecutive slices and their descriptors, the largest block tblock
   // bytes; used when sell == 4
@@ -252,12 +287,24 @@ struct DCSR {
   int nslice() const { return (nr + 31) / 32; }
   // bytes of the matrix as the chosen kernel reads it
   int64_t mat_bytes() const {
+    if (hdia())
+      return hdslots * val_bytes() + 4 * ((int64_t)hd_nslice() + 1) + 4 * (hdslots / 32) +
+             scale_bytes();
     return ((sell >= 1 && sell <= 3) ? slots * (val_bytes() + idx_bytes()) + 4 * ((int64_t)nslice() + 1)
                  : nnz * (val_bytes() + idx_bytes()) + 4 * ((int64_t)nr + 1)) +
            scale_bytes();
   }
-  // algorithmic CSR bytes nnz*(value + index) + 4*(rows + 1) (+ the row scales)
-  int64_t alg_bytes() const { return nnz * (val_bytes() + idx_bytes()) + 4 * ((int64_t)nr + 1) + scale_bytes(); }
+  // algorithmic bytes: CSR nnz*(value + index) + 4*(rows + 1) (+ the row
+  // scales), or, for an operator that also has its HDIA copy, that copy's
+  // compulsory bytes when fewer: one value per entry (no padding), the slice
+  // pointers and offsets (+ the row scales)
+  int64_t csr_bytes() const { return nnz * (val_bytes() + idx_bytes()) + 4 * ((int64_t)nr + 1) + scale_bytes(); }
+  int64_t alg_bytes() const {
+    const int64_t csr = csr_bytes();
+    if (!hdptr) return csr;
+    return std::min(csr, nnz * val_bytes() + 4 * ((int64_t)hd_nslice() + 1) +
+                             4 * (hdslots / 32) + scale_bytes());
+  }
 };
 
 template <typename T>
@@ -453,6 +500,92 @@ static void make_h16(Arena &ar, const HostCSR &h, DCSR<T> &d) {
   }
 }
 
+// The HDIA-32 copy of a square CSR matrix (k_spmv_hdia): rows in slices of
+// 32, per slice the ascending
+// distinct column offsets j - i of its entries, and one value per (offset,
+// row), zero where the row has no entry on that offset.  Built only when
+// every row is sorted by column (the kernels then sum a row in its stored
+// order), no slice has more than kHdiaMaxDiag offsets, and the slices store
+// at most an eighth more values than the matrix has entries; MLDG_NO_HDIA
+// skips it.  In the FP16 operator form the values are the FP16 row-scaled
+// ones of make_h16 (its row scales rs are shared).
+constexpr int kHdiaMaxDiag = 64;
+template <typename T>
+static void build_hdia(Arena &ar, const HostCSR &h, DCSR<T> &d, bool h16) {
+  if (std::getenv("MLDG_NO_HDIA") || h.nr == 0 || h.nr != h.nc || h.nnz() == 0) return;
+  constexpr int H = 32;
+  const int ns = (h.nr + H - 1) / H;
+  std::vector<int> cnt((size_t)ns, 0);
+  int bad = 0;
+  // pass 1: offsets per slice (counted), sortedness
+#pragma omp parallel for reduction(| : bad) schedule(static, 64)
+  for (int s = 0; s < ns; ++s) {
+    int o[kHdiaMaxDiag];
+    int no = 0;
+    for (int i = s * H; i < std::min(h.nr, s * H + H) && !bad; ++i)
+      for (int k = h.irp[i]; k < h.irp[i + 1]; ++k) {
+        if (k > h.irp[i] && h.ja[k] <= h.ja[k - 1]) {
+          bad = 1;
+          break;
+        }
+        const int off = h.ja[k] - i;
+        int q = 0;
+        while (q < no && o[q] != off) ++q;
+        if (q == no) {
+          if (no == kHdiaMaxDiag) {
+            bad = 1;
+            break;
+          }
+          o[no++] = off;
+        }
+      }
+    cnt[s] = no;
+  }
+  if (bad) return;
+  std::vector<int> dptr((size_t)ns + 1, 0);
+  for (int s = 0; s < ns; ++s) dptr[s + 1] = dptr[s] + cnt[s];
+  const int64_t slots = (int64_t)H * dptr[ns];
+  if (slots * 8 > h.nnz() * 9 || slots > INT32_MAX) return;
+  std::vector<int> doff((size_t)dptr[ns]);
+  std::vector<float> sc;
+  std::vector<__half> hv;
+  if (h16) h16_values(h, sc, hv);
+  std::vector<T> tv(h16 ? 0 : (size_t)slots, T(0));
+  std::vector<__half> th(h16 ? (size_t)slots : 0, __float2half_rn(0.f));
+#pragma omp parallel for schedule(static, 64)
+  for (int s = 0; s < ns; ++s) {
+    int *o = doff.data() + dptr[s];
+    int no = 0;
+    for (int i = s * H; i < std::min(h.nr, s * H + H); ++i)
+      for (int k = h.irp[i]; k < h.irp[i + 1]; ++k) {
+        const int off = h.ja[k] - i;
+        int q = 0;
+        while (q < no && o[q] != off) ++q;
+        if (q == no) o[no++] = off;
+      }
+    std::sort(o, o + no);
+    for (int i = s * H; i < std::min(h.nr, s * H + H); ++i) {
+      int q = 0;
+      for (int k = h.irp[i]; k < h.irp[i + 1]; ++k) {
+        const int off = h.ja[k] - i;
+        while (o[q] != off) ++q;  // the row's offsets ascend, like the slice's
+        const size_t e = (size_t)H * ((size_t)dptr[s] + q) + (size_t)(i - s * H);
+        if (h16)
+          th[e] = hv[k];
+        else
+          tv[e] = (T)h.val[k];
+      }
+    }
+  }
+  d.hdptr = ar.upload(dptr);
+  d.hdoff = ar.upload(doff);
+  if (h16)
+    d.hdhval = ar.upload(th);
+  else
+    d.hdval = ar.upload(tv);
+  d.hdslots = slots;
+}
+
 // Staged SELL tiles (mldg_spmv_stg.cuh): the SELL-32 slots of the operator,
 // in the order build_sell stores them (same widths, same padding columns,
 // zero padding values), cut into tiles of consecutive slices whose packed
@@ -567,6 +700,7 @@ static DCSR<T> to_dev(Arena &ar, const HostCSR &h, bool h16 = false) {
   d.tpr = pick_tpr(d.nnz, d.nr);
   build_sell(ar, h, d);
   if (h16) make_h16(ar, h, d);
+  build_hdia(ar, h, d, h16);
   build_stg_pack(ar, h, d, h16);
   return d;
 }
@@ -662,6 +796,15 @@ struct Engine {
   };
   std::vector<Prof> *prof = nullptr;
   bool capturing = false;  // inside stream capture: probe events become graph nodes
+  // programmatic dependent launch of the streaming kernels (launch_k); off
+  // while probe or profile events are recorded between kernels, and with
+  // MLDG_NO_PDL
+  bool pdl = std::getenv("MLDG_NO_PDL") == nullptr;
+  bool pdl_on() const { return pdl && probe_kind == 0 && !prof; }
+  template <typename... KArgs, typename... Args>
+  void kl(void (*kern)(KArgs...), int grid, int block, Args... args) {
+    launch_k(pdl_on(), kern, grid, block, st, args...);
+  }
   void rec(cudaEvent_t e) {
     if (capturing)
       MLDG_CUDA(cudaEventRecordWithFlags(e, st, cudaEventRecordExternal));
@@ -772,6 +915,7 @@ __global__ void __launch_bounds__(kRedThreads) k_dotsT(int n, int np, const T *_
 
 template <typename T>
 __global__ void k_axpby1(int n, const T *__restrict__ x, T beta, T *y) {
+  pdl_enter();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     y[i] = (beta == T(0)) ? x[i] : fma(beta, y[i], x[i]);
 }
@@ -840,11 +984,11 @@ struct EngineT : Engine {
   void spmv(const DCSR<T> &A, const T *v, T a1, const T *b, T a0, T *out, T a2) {
     if constexpr (std::is_same<T, float>::value) {
       if (A.h16()) {
-        spmv_v<__half>(A, A.hval, A.shval, A.rs, v, a1, b, a0, out, a2);
+        spmv_v<__half>(A, A.hval, A.shval, A.rs, v, a1, b, a0, out, a2, A.hdhval);
         return;
       }
     }
-    spmv_v<T>(A, A.val, A.sval, nullptr, v, a1, b, a0, out, a2);
+    spmv_v<T>(A, A.val, A.sval, nullptr, v, a1, b, a0, out, a2, A.hdval);
   }
   // values of type V (T, or FP16 with the row scales rs)
   int stg_stages = kStgStages;
@@ -913,12 +1057,19 @@ struct EngineT : Engine {
   }
   template <typename V>
   void spmv_v(const DCSR<T> &A, const V *val, const V *sval, const float *rs, const T *v, T a1, const T *b,
-              T a0, T *out, T a2) {
+              T a0, T *out, T a2, const V *hdv) {
     const int64_t vec = (int64_t)A.nc * sizeof(T) + (int64_t)A.nr * sizeof(T) * (1 + (b ? 1 : 0) + (a2 != T(0) ? 1 : 0));
+    if (A.hdia() && hdv) {
+      begin(MLDG_KERNEL_SPMV);
+      kl(k_spmv_hdia<T, V>, blocks_for((int64_t)A.hd_nslice() * 32), 256, A.nr, A.hdptr, A.hdoff, hdv, v, a1,
+                                                                                 b, a0, out, a2, rs);
+      end(A.mat_bytes() + vec, A.alg_bytes() + vec);
+      return;
+    }
     if (A.sell == 4 && A.tiles) {
       begin(MLDG_KERNEL_SPMV);
       spmv_stg<V>(A, rs, v, a1, b, a0, out, a2);
-      end(A.alg_bytes() + vec);
+      end(A.csr_bytes() + vec, A.alg_bytes() + vec);
       return;
     }
     if (A.sell >= 1 && A.sell <= 3 && A.soff) {
@@ -926,19 +1077,19 @@ struct EngineT : Engine {
       const int g = blocks_for((int64_t)A.nslice() * 32 / (A.sell == 2 ? 2 : 1));
       if (A.sell == 3) {
         if (A.sjd)
-          k_spmv_sellp<T, short, V><<<g, 256, 0, st>>>(A.nr, A.soff, A.sjd, sval, v, a1, b, a0, out, a2, rs);
+          kl(k_spmv_sellp<T, short, V>, g, 256, A.nr, A.soff, A.sjd, sval, v, a1, b, a0, out, a2, rs);
         else
-          k_spmv_sellp<T, int, V><<<g, 256, 0, st>>>(A.nr, A.soff, A.sja, sval, v, a1, b, a0, out, a2, rs);
+          kl(k_spmv_sellp<T, int, V>, g, 256, A.nr, A.soff, A.sja, sval, v, a1, b, a0, out, a2, rs);
       } else if (A.sell == 2) {
         if (A.sjd)
-          k_spmv_sell<T, short, 2, V><<<g, 256, 0, st>>>(A.nr, A.soff, A.sjd, sval, v, a1, b, a0, out, a2, rs);
+          kl(k_spmv_sell<T, short, 2, V>, g, 256, A.nr, A.soff, A.sjd, sval, v, a1, b, a0, out, a2, rs);
         else
-          k_spmv_sell<T, int, 2, V><<<g, 256, 0, st>>>(A.nr, A.soff, A.sja, sval, v, a1, b, a0, out, a2, rs);
+          kl(k_spmv_sell<T, int, 2, V>, g, 256, A.nr, A.soff, A.sja, sval, v, a1, b, a0, out, a2, rs);
       } else {
         if (A.sjd)
-          k_spmv_sell<T, short, 1, V><<<g, 256, 0, st>>>(A.nr, A.soff, A.sjd, sval, v, a1, b, a0, out, a2, rs);
+          kl(k_spmv_sell<T, short, 1, V>, g, 256, A.nr, A.soff, A.sjd, sval, v, a1, b, a0, out, a2, rs);
         else
-          k_spmv_sell<T, int, 1, V><<<g, 256, 0, st>>>(A.nr, A.soff, A.sja, sval, v, a1, b, a0, out, a2, rs);
+          kl(k_spmv_sell<T, int, 1, V>, g, 256, A.nr, A.soff, A.sja, sval, v, a1, b, a0, out, a2, rs);
       }
       end(A.mat_bytes() + vec, A.alg_bytes() + vec);
       return;
@@ -949,34 +1100,41 @@ struct EngineT : Engine {
 #define CASE(K)                                                                                         \
   case K:                                                                                               \
     if (A.jd)                                                                                           \
-      k_spmv<T, K, short, V><<<g, 256, 0, st>>>(A.nr, A.irp, A.jd, val, v, a1, b, a0, out, a2, rs);    \
+      kl(k_spmv<T, K, short, V>, g, 256, A.nr, A.irp, A.jd, val, v, a1, b, a0, out, a2, rs);    \
     else                                                                                                \
-      k_spmv<T, K, int, V><<<g, 256, 0, st>>>(A.nr, A.irp, A.ja, val, v, a1, b, a0, out, a2, rs);      \
+      kl(k_spmv<T, K, int, V>, g, 256, A.nr, A.irp, A.ja, val, v, a1, b, a0, out, a2, rs);      \
     break;
       CASE(1) CASE(2) CASE(4) CASE(8) CASE(16) CASE(32)
 #undef CASE
       default: fail(MLDG_ERR_INTERNAL, "bad tpr %d", A.tpr);
     }
-    end(A.alg_bytes() + vec);
+    end(A.csr_bytes() + vec, A.alg_bytes() + vec);
   }
   void jacobi(const DCSR<T> &ND, const T *d, const T *x, const T *ty, int first, T omega,
               T alpha, T beta, T *out) {
     if constexpr (std::is_same<T, float>::value) {
       if (ND.h16()) {
-        jacobi_v<__half>(ND, ND.hval, ND.shval, ND.rs, d, x, ty, first, omega, alpha, beta, out);
+        jacobi_v<__half>(ND, ND.hval, ND.shval, ND.rs, d, x, ty, first, omega, alpha, beta, out, ND.hdhval);
         return;
       }
     }
-    jacobi_v<T>(ND, ND.val, ND.sval, nullptr, d, x, ty, first, omega, alpha, beta, out);
+    jacobi_v<T>(ND, ND.val, ND.sval, nullptr, d, x, ty, first, omega, alpha, beta, out, ND.hdval);
   }
   template <typename V>
   void jacobi_v(const DCSR<T> &ND, const V *val, const V *sval, const float *rs, const T *d, const T *x,
-                const T *ty, int first, T omega, T alpha, T beta, T *out) {
+                const T *ty, int first, T omega, T alpha, T beta, T *out, const V *hdv) {
     const int64_t vec = (int64_t)ND.nr * sizeof(T) * (3 + (first ? 0 : 1) + (beta != T(0) ? 1 : 0));
+    if (ND.hdia() && hdv) {
+      begin(MLDG_KERNEL_JACOBI);
+      kl(k_jacobi_hdia<T, V>, blocks_for((int64_t)ND.hd_nslice() * 32), 256, 
+          ND.nr, ND.hdptr, ND.hdoff, hdv, d, x, ty, first, omega, alpha, beta, out, rs);
+      end(ND.mat_bytes() + vec, ND.alg_bytes() + vec);
+      return;
+    }
     if (ND.sell == 4 && ND.tiles) {
       begin(MLDG_KERNEL_JACOBI);
       jacobi_stg<V>(ND, rs, d, x, ty, first, omega, alpha, beta, out);
-      end(ND.alg_bytes() + vec);
+      end(ND.csr_bytes() + vec, ND.alg_bytes() + vec);
       return;
     }
     if (ND.sell >= 1 && ND.sell <= 3 && ND.soff) {
@@ -984,24 +1142,24 @@ struct EngineT : Engine {
       const int g = blocks_for((int64_t)ND.nslice() * 32 / (ND.sell == 2 ? 2 : 1));
       if (ND.sell == 3) {
         if (ND.sjd)
-          k_jacobi_sellp<T, short, V><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sjd, sval, d, x, ty, first, omega,
+          kl(k_jacobi_sellp<T, short, V>, g, 256, ND.nr, ND.soff, ND.sjd, sval, d, x, ty, first, omega,
                                                          alpha, beta, out, rs);
         else
-          k_jacobi_sellp<T, int, V><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sja, sval, d, x, ty, first, omega,
+          kl(k_jacobi_sellp<T, int, V>, g, 256, ND.nr, ND.soff, ND.sja, sval, d, x, ty, first, omega,
                                                        alpha, beta, out, rs);
       } else if (ND.sell == 2) {
         if (ND.sjd)
-          k_jacobi_sell<T, short, 2, V><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sjd, sval, d, x, ty, first, omega,
+          kl(k_jacobi_sell<T, short, 2, V>, g, 256, ND.nr, ND.soff, ND.sjd, sval, d, x, ty, first, omega,
                                                            alpha, beta, out, rs);
         else
-          k_jacobi_sell<T, int, 2, V><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sja, sval, d, x, ty, first, omega,
+          kl(k_jacobi_sell<T, int, 2, V>, g, 256, ND.nr, ND.soff, ND.sja, sval, d, x, ty, first, omega,
                                                          alpha, beta, out, rs);
       } else {
         if (ND.sjd)
-          k_jacobi_sell<T, short, 1, V><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sjd, sval, d, x, ty, first, omega,
+          kl(k_jacobi_sell<T, short, 1, V>, g, 256, ND.nr, ND.soff, ND.sjd, sval, d, x, ty, first, omega,
                                                            alpha, beta, out, rs);
         else
-          k_jacobi_sell<T, int, 1, V><<<g, 256, 0, st>>>(ND.nr, ND.soff, ND.sja, sval, d, x, ty, first, omega,
+          kl(k_jacobi_sell<T, int, 1, V>, g, 256, ND.nr, ND.soff, ND.sja, sval, d, x, ty, first, omega,
                                                          alpha, beta, out, rs);
       }
       end(ND.mat_bytes() + vec, ND.alg_bytes() + vec);
@@ -1013,34 +1171,34 @@ struct EngineT : Engine {
 #define CASE(K)                                                                                          \
   case K:                                                                                                \
     if (ND.jd)                                                                                           \
-      k_jacobi<T, K, short, V><<<g, 256, 0, st>>>(ND.nr, ND.irp, ND.jd, val, d, x, ty, first, omega,    \
+      kl(k_jacobi<T, K, short, V>, g, 256, ND.nr, ND.irp, ND.jd, val, d, x, ty, first, omega,    \
                                                   alpha, beta, out, rs);                                 \
     else                                                                                                 \
-      k_jacobi<T, K, int, V><<<g, 256, 0, st>>>(ND.nr, ND.irp, ND.ja, val, d, x, ty, first, omega,      \
+      kl(k_jacobi<T, K, int, V>, g, 256, ND.nr, ND.irp, ND.ja, val, d, x, ty, first, omega,      \
                                                 alpha, beta, out, rs);                                   \
     break;
       CASE(1) CASE(2) CASE(4) CASE(8) CASE(16) CASE(32)
 #undef CASE
       default: fail(MLDG_ERR_INTERNAL, "bad tpr %d", ND.tpr);
     }
-    end(ND.alg_bytes() + vec);
+    end(ND.csr_bytes() + vec, ND.alg_bytes() + vec);
   }
   void diag(int n, const T *d, const T *x, T alpha, T beta, T *out) {
     begin(MLDG_KERNEL_VEC);
-    k_diag<T><<<blocks_for(n), 256, 0, st>>>(n, d, x, alpha, beta, out);
+    kl(k_diag<T>, blocks_for(n), 256, n, d, x, alpha, beta, out);
     end((int64_t)n * sizeof(T) * (3 + (beta != T(0) ? 1 : 0)));
   }
   // precision cast of a boundary vector (k_cast4 when both are 16-byte aligned)
   template <typename A, typename B>
   void cast(int n, const A *x, B *y) {
     if ((((uintptr_t)x | (uintptr_t)y) & 15u) == 0)
-      k_cast4<A, B><<<blocks_for(((int64_t)n + 3) / 4), 256, 0, st>>>(n, x, y);
+      kl(k_cast4<A, B>, blocks_for(((int64_t)n + 3) / 4), 256, n, x, y);
     else
-      k_cast<A, B><<<blocks_for(n), 256, 0, st>>>(n, x, y);
+      kl(k_cast<A, B>, blocks_for(n), 256, n, x, y);
   }
   void fill(int n, T v, T *y) {
     begin(MLDG_KERNEL_VEC);
-    k_fill<T><<<blocks_for(n), 256, 0, st>>>(n, v, y);
+    kl(k_fill<T>, blocks_for(n), 256, n, v, y);
     end((int64_t)n * sizeof(T));
   }
   void trsv(const DTri<T> &t, const T *rhs, const T *scale, T *cur, T *other, T *out, T alpha,
@@ -1243,7 +1401,7 @@ struct EngineT : Engine {
     if (L.minv) {
       const T *M = (trans == 'N') ? L.minv : L.minvT;
       begin(MLDG_KERNEL_VEC);
-      k_gemv<T><<<blocks_for((int64_t)L.n * 32), 256, 0, st>>>(L.n, M, x, T(1), beta, y);
+      kl(k_gemv<T>, blocks_for((int64_t)L.n * 32), 256, L.n, M, x, T(1), beta, y);
       // algorithmic: the two sparse solves and the pivot scaling it replaces
       end((int64_t)L.n * L.n * sizeof(T) + (int64_t)L.n * sizeof(T) * (2 + (beta != T(0))),
           (L.nnz_l + L.nnz_u) * (int64_t)(sizeof(T) + 4) + 8 * ((int64_t)L.n + 1) +
@@ -1304,7 +1462,7 @@ struct EngineT : Engine {
     if (L.gsF) {
       const T *M = backward ? L.gsB : L.gsF;
       begin(MLDG_KERNEL_VEC);
-      k_gemv<T><<<blocks_for((int64_t)L.n * 32), 256, 0, st>>>(L.n, M, rhs, T(1), beta, out);
+      kl(k_gemv<T>, blocks_for((int64_t)L.n * 32), 256, L.n, M, rhs, T(1), beta, out);
       // algorithmic: the sparse triangular solve (with its diagonal) it replaces
       end((int64_t)L.n * L.n * sizeof(T) + (int64_t)L.n * sizeof(T) * (2 + (beta != T(0))),
           (backward ? L.nnz_u : L.nnz_l) * (int64_t)(sizeof(T) + 4) + 4 * ((int64_t)L.n + 1) +
@@ -1617,10 +1775,12 @@ struct EngineT : Engine {
           else
             spmv(*op, v, T(1), nullptr, T(0), o, T(0));
         };
-        // t = -4: the staged SELL kernels
-        for (int t : {1, 2, 4, 8, 16, 32, -1, -2, -3, -4}) {
+        // t = -4: the staged SELL kernels; t = -5: the HDIA copy
+        const bool has_hd = op->hdptr && (op->h16() ? op->hdhval != nullptr : op->hdval != nullptr);
+        for (int t : {1, 2, 4, 8, 16, 32, -1, -2, -3, -4, -5}) {
           if (t < 0 && t >= -3 && !op->soff) continue;
           if (t == -4 && !op->tiles) continue;
+          if (t == -5 && !has_hd) continue;
           op->sell = t < 0 ? -t : 0;
           if (t > 0) op->tpr = t;
           run();  // warm
@@ -1641,8 +1801,9 @@ struct EngineT : Engine {
         if (std::getenv("MLDG_VERBOSE"))
           std::fprintf(stderr, "mldg: spmv autotune level %zu %-4s n=%d nnz=%lld -> %s%d %.4f ms\n", l,
                        names[oi], op->nr, (long long)op->nnz,
-                       best_sell == 4 ? "staged sell" : (best_sell ? "sell" : "csr tpr "),
-                       best_sell == 4 ? 1 : (best_sell ? best_sell : best_t), best / reps);
+                       best_sell >= 5 ? "hdia" : (best_sell == 4 ? "staged sell" : (best_sell ? "sell" : "csr tpr ")),
+                       best_sell >= 4 ? 1 : (best_sell ? best_sell : best_t),
+                       best / reps);
       }
     }
     launches = 0;
@@ -2424,7 +2585,7 @@ struct EngineT : Engine {
 template <typename T>
 void EngineT<T>::k_axpby_impl(int n, const T *x, T beta, T *y) {
   begin(MLDG_KERNEL_VEC);
-  k_axpby1<T><<<blocks_for(n), 256, 0, st>>>(n, x, beta, y);
+  kl(k_axpby1<T>, blocks_for(n), 256, n, x, beta, y);
   end((int64_t)n * sizeof(T) * (2 + (beta != T(0))));
 }
 
@@ -2443,7 +2604,7 @@ void EngineT<float>::prolong(Lev &C, float *y) {
   begin(MLDG_KERNEL_SPMV);
   switch (C.P.tpr) {
 #define CASE(K) \
-  case K: k_spmv_h<K><<<g, 256, 0, st>>>(C.P.nr, C.P.irp, C.P.ja, C.Ph, C.Pscale, C.y, y); break;
+  case K: kl(k_spmv_h<K>, g, 256, C.P.nr, C.P.irp, C.P.ja, C.Ph, C.Pscale, C.y, y); break;
     CASE(1) CASE(2) CASE(4) CASE(8) CASE(16) CASE(32)
 #undef CASE
     default: fail(MLDG_ERR_INTERNAL, "bad tpr");
@@ -4049,6 +4210,13 @@ static Engine *make_engine(Handle *h) {
           const int f = std::atoi(std::getenv("MLDG_SELL_FORCE"));
           op->sell = (f >= 1 && f <= 3) ? f : 1;
         }
+  // MLDG_HDIA_FORCE: every operator with an HDIA copy uses it (measurement
+  // aid and test hook)
+  if (std::getenv("MLDG_HDIA_FORCE"))
+    for (auto &L : e->lv)
+      for (DCSR<T> *op : {&L.A, &L.AT, &L.P, &L.R, &L.ND, &L.NDT})
+        if (op->hdptr && (op->h16() ? op->hdhval != nullptr : op->hdval != nullptr))
+          op->sell = 5;
   // MLDG_STG_FORCE: every operator with staged tiles uses them
   if (std::getenv("MLDG_STG_FORCE"))
     for (auto &L : e->lv)
@@ -4161,6 +4329,7 @@ static void finalize(Handle *h, int nlev, int precision) {
   h->serial = next_serial();
   if (h->opts.autotune && !std::getenv("MLDG_NO_AUTOTUNE")) tune_krylov_spmv(h);
   if (std::getenv("MLDG_SELL_FORCE")) h->A0.sell = h->A0.soff != nullptr ? 1 : 0;
+  if (std::getenv("MLDG_HDIA_FORCE") && h->A0.hdptr && h->A0.hdval) h->A0.sell = 5;
 }
 
 static bool kcycle_handle(const Handle *h) { return h->cycle == MLDG_CYCLE_K || h->cycle == MLDG_CYCLE_KSYM; }
@@ -4383,16 +4552,24 @@ static void krylov_prefix(Handle *h, const DCSR<double> &A, cudaGraphConditional
 // three fused kernels (mldg_kernels.cuh, k_kry_*); every kernel returns at
 // once when the device state says the solve is done.
 static void kry_spmv(Handle *h, const DCSR<double> &A) {
+  const bool pdl = h->eng->pdl_on();
   double *r = h->xin, *z = h->yout;
+  if (A.hdia() && A.hdval) {
+    const int64_t thr = (int64_t)A.hd_nslice() * 32;
+    const int g = (int)std::max<int64_t>(1, std::min<int64_t>((thr + 255) / 256, (int64_t)h->nsm * 16));
+    launch_k(pdl, k_kry_spmv_hdia, g, 256, h->st, A.nr, A.hdptr, A.hdoff, A.hdval, z, h->kd, h->kd1, h->kq, r, h->kst,
+                                          h->kpart);
+    return;
+  }
   if (A.sell) {
     // grid: at most 16 blocks per SM (the partials hold 2 per block)
     const int64_t thr = (int64_t)A.nslice() * 32;
     const int g = (int)std::max<int64_t>(1, std::min<int64_t>((thr + 255) / 256, (int64_t)h->nsm * 16));
     if (A.sjd)
-      k_kry_spmv_sell<short><<<g, 256, 0, h->st>>>(A.nr, A.soff, A.sjd, A.sval, z, h->kd, h->kd1, h->kq, r,
+      launch_k(pdl, k_kry_spmv_sell<short>, g, 256, h->st, A.nr, A.soff, A.sjd, A.sval, z, h->kd, h->kd1, h->kq, r,
                                                    h->kst, h->kpart);
     else
-      k_kry_spmv_sell<int><<<g, 256, 0, h->st>>>(A.nr, A.soff, A.sja, A.sval, z, h->kd, h->kd1, h->kq, r,
+      launch_k(pdl, k_kry_spmv_sell<int>, g, 256, h->st, A.nr, A.soff, A.sja, A.sval, z, h->kd, h->kd1, h->kq, r,
                                                  h->kst, h->kpart);
     return;
   }
@@ -4402,10 +4579,10 @@ static void kry_spmv(Handle *h, const DCSR<double> &A) {
 #define CASE(K)                                                                                  \
   case K:                                                                                        \
     if (A.jd)                                                                                    \
-      k_kry_spmv<K, short><<<g, 256, 0, h->st>>>(A.nr, A.irp, A.jd, A.val, z, h->kd, h->kd1, h->kq, r, \
+      launch_k(pdl, k_kry_spmv<K, short>, g, 256, h->st, A.nr, A.irp, A.jd, A.val, z, h->kd, h->kd1, h->kq, r, \
                                                  h->kst, h->kpart);                              \
     else                                                                                         \
-      k_kry_spmv<K, int><<<g, 256, 0, h->st>>>(A.nr, A.irp, A.ja, A.val, z, h->kd, h->kd1, h->kq, r,   \
+      launch_k(pdl, k_kry_spmv<K, int>, g, 256, h->st, A.nr, A.irp, A.ja, A.val, z, h->kd, h->kd1, h->kq, r,   \
                                                h->kst, h->kpart);                                \
     break;
     CASE(1) CASE(2) CASE(4) CASE(8) CASE(16) CASE(32)
@@ -4415,14 +4592,15 @@ static void kry_spmv(Handle *h, const DCSR<double> &A) {
 }
 
 static void krylov_iteration(Handle *h, const DCSR<double> &A, cudaGraphConditionalHandle hc) {
+  const bool pdl = h->eng->pdl_on();
   const int n = h->n0;
   double *r = h->xin, *z = h->yout;
   // vector kernels: 8 blocks of 256 threads per SM (64 warps), so that enough
   // loads are in flight to stream the vectors at HBM bandwidth
   const int gv = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)n + 255) / 256, (int64_t)h->nsm * 8));
-  k_kry_beta<<<gv, kRedThreads, 0, h->st>>>(n, z, h->kq, r, h->kst, h->kpart);
+  launch_k(pdl, k_kry_beta, gv, kRedThreads, h->st, n, z, h->kq, r, h->kst, h->kpart);
   kry_spmv(h, A);
-  k_kry_update<<<gv, kRedThreads, 0, h->st>>>(n, h->kd, h->kd1, h->kq, h->kx, r, h->kst, h->kpart,
+  launch_k(pdl, k_kry_update, gv, kRedThreads, h->st, n, h->kd, h->kd1, h->kq, h->kx, r, h->kst, h->kpart,
                                                       hc);
   h->last_launches += 3;
 }
@@ -4446,10 +4624,12 @@ static void tune_krylov_spmv(Handle *h) {
   int best_t = A.tpr;
   int best_sell = 0;
   for (double *v : {h->kd, h->kd1, h->kq}) MLDG_CUDA(cudaMemsetAsync(v, 0, sizeof(double) * (size_t)h->n0, h->st));
-  for (int t : {1, 2, 4, 8, 16, 32, 0}) {
+  // t = 0: the SELL copy; t = -1: the HDIA copy
+  for (int t : {1, 2, 4, 8, 16, 32, 0, -1}) {
     if (t == 0 && !A.soff) continue;
-    A.sell = t == 0 ? 1 : 0;
-    if (t) A.tpr = t;
+    if (t == -1 && !(A.hdptr && A.hdval)) continue;
+    A.sell = t == 0 ? 1 : (t == -1 ? 5 : 0);
+    if (t > 0) A.tpr = t;
     *h->hkst = s0;
     MLDG_CUDA(cudaMemcpyAsync(h->kst, h->hkst, sizeof(KState), cudaMemcpyHostToDevice, h->st));
     kry_spmv(h, A);  // warm
@@ -4461,8 +4641,8 @@ static void tune_krylov_spmv(Handle *h) {
     MLDG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
     if (ms < best) {
       best = ms;
-      best_t = t ? t : best_t;
-      best_sell = t == 0 ? 1 : 0;
+      best_t = t > 0 ? t : best_t;
+      best_sell = t == 0 ? 1 : (t == -1 ? 5 : 0);
     }
   }
   A.tpr = best_t;

@@ -70,6 +70,20 @@ template <> struct Bits<float> {
   __device__ static float canon(float v) { return isnan(v) ? __uint_as_float(0x7FC00000u) : v; }
 };
 
+// Programmatic dependent launch.  A kernel launched with the programmatic
+// stream-serialization attribute may be scheduled while the kernel before it
+// in the stream is still finishing; pdl_enter() first waits until that
+// kernel has completed and its writes are visible (so it must run before
+// the kernel touches any memory), then allows the next kernel in the stream
+// to be scheduled early in turn.  Both instructions are no-ops in a kernel
+// launched without the attribute.  Every kernel that the host may launch
+// with the attribute calls it first, so completion stays transitive along
+// the stream.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Spin-wait limits: a wait that exceeds kSpinLimit polls records
 // MLDG_ERR_TIMEOUT in *err and returns 0; every other waiter checks *err every
 // kSpinCheck polls and leaves at once, so a failed solve drains quickly.
@@ -195,6 +209,7 @@ __global__ void __launch_bounds__(256) k_spmv(int nr, const int *__restrict__ ir
                                               const T *__restrict__ v, T a1,
                                               const T *__restrict__ b, T a0, T *out, T a2,
                                               const float *__restrict__ rs = nullptr) {
+  pdl_enter();
   constexpr int RPW = 32 / TPR;
   const int lane = threadIdx.x & 31;
   const int sub = lane % TPR;
@@ -281,6 +296,7 @@ __global__ void __launch_bounds__(256) k_spmv_sell(int nr, const int *__restrict
                                                    const T *__restrict__ v, T a1, const T *__restrict__ b,
                                                    T a0, T *out, T a2,
                                                    const float *__restrict__ rs = nullptr) {
+  pdl_enter();
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -375,6 +391,7 @@ __global__ void __launch_bounds__(256) k_spmv_sellp(int nr, const int *__restric
                                                     const T *__restrict__ v, T a1, const T *__restrict__ b,
                                                     T a0, T *out, T a2,
                                                     const float *__restrict__ rs = nullptr) {
+  pdl_enter();
   sellp_loop<T, CI>(
       nr, soff, sj, sv, [&](int j) { return __ldg(v + j); },
       [&](int row, T acc) {
@@ -392,6 +409,7 @@ __global__ void __launch_bounds__(256) k_jacobi_sellp(int nr, const int *__restr
                                                       const T *__restrict__ d, const T *__restrict__ x,
                                                       const T *__restrict__ ty, int first, T omega, T alpha,
                                                       T beta, T *out, const float *__restrict__ rs = nullptr) {
+  pdl_enter();
   auto done = [&](int row, T acc) {
     out[row] = jac_row(d[row], x[row], row_scaled<T, V>(acc, rs, row), (!first && omega != T(1)) ? ty[row] : T(0),
                        first != 0, omega, alpha, beta, beta != T(0) ? out[row] : T(0));
@@ -412,6 +430,7 @@ __global__ void __launch_bounds__(256) k_jacobi_sell(int nr, const int *__restri
                                                      const T *__restrict__ d, const T *__restrict__ x,
                                                      const T *__restrict__ ty, int first, T omega, T alpha,
                                                      T beta, T *out, const float *__restrict__ rs = nullptr) {
+  pdl_enter();
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -436,6 +455,102 @@ __global__ void __launch_bounds__(256) k_jacobi_sell(int nr, const int *__restri
   }
 }
 
+// ---------------------------------------------------------------------------
+// The same operators on a hacked-diagonal copy (HDIA-32) of a square matrix:
+// rows in slices of 32; slice s lists the distinct column offsets j - i of
+// its rows' entries, ascending, in doff[dptr[s] .. dptr[s+1]), and stores the
+// value of its k-th offset for row `lane` at hv[32*(dptr[s] + k) + lane]
+// (zero where the row has no entry there).  No column index is stored per
+// entry, so a level whose slices share a few diagonals (a stencil) moves
+// only its values: 2 bytes per entry in the FP16 operator form instead of 4.
+// A row's entries are summed in ascending column order from zero, the
+// stored order of a column-sorted CSR row (the host builds the copy only for
+// such matrices); a padding slot adds fma(0, v_j, s) = s for finite v_j, its
+// column clamped into [0, n).  One warp per slice; the offsets are loaded by
+// every lane (one broadcast access), kHdiaU diagonals' loads issued together.
+// (Measured on the idim=160 level 0 against wider forms: 4 rows per thread
+// with 8/16-byte accesses, 2 slices per warp, and offsets staged in shared
+// memory per block all ran slower than this one-row-per-thread form, which
+// the register limit of __launch_bounds__ keeps at full occupancy.)
+constexpr int kHdiaU = 4;
+template <typename T>
+struct HdiaMinBlocks {  // 256-thread blocks per SM: 32 registers (FP32), 40 (FP64)
+  static constexpr int value = sizeof(T) == 8 ? 6 : 8;
+};
+
+template <typename T, typename F, typename V>
+__device__ __forceinline__ T hdia_row(const int *__restrict__ dptr, const int *__restrict__ doff,
+                                      const V *__restrict__ hv, int sl, int row, int n, int lane, F f) {
+  int k = __ldg(dptr + sl);
+  const int k1 = __ldg(dptr + sl + 1);
+  T acc = T(0);
+  for (; k < k1; k += kHdiaU) {  // k, k1 are the same in every lane of the warp
+    T vv[kHdiaU], xv[kHdiaU];
+#pragma unroll
+    for (int u = 0; u < kHdiaU; ++u) {
+      const bool ok = k + u < k1;
+      const int off = ok ? __ldg(doff + k + u) : 0;
+      vv[u] = ok ? ldval<T>(hv, ((k + u) << 5) + lane) : T(0);
+      xv[u] = ok ? f(min(max(row + off, 0), n - 1)) : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kHdiaU; ++u)
+      if (k + u < k1) acc = fma(vv[u], xv[u], acc);
+  }
+  return acc;
+}
+
+// out[i] = a0*b[i] + a1*(A v)[i] + a2*out[i] on the HDIA copy of A
+template <typename T, typename V = T>
+__global__ void __launch_bounds__(256, HdiaMinBlocks<T>::value)
+    k_spmv_hdia(int nr, const int *__restrict__ dptr, const int *__restrict__ doff, const V *__restrict__ hv,
+                const T *__restrict__ v, T a1, const T *__restrict__ b, T a0, T *out, T a2,
+                const float *__restrict__ rs = nullptr) {
+  pdl_enter();
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int ns = (nr + 31) >> 5;
+  for (int sl = warp; sl < ns; sl += nwarps) {
+    const int row = (sl << 5) + lane;
+    const T acc = hdia_row<T>(dptr, doff, hv, sl, row, nr, lane, [&](int j) { return __ldg(v + j); });
+    if (row < nr) {
+      T r = a1 * row_scaled<T, V>(acc, rs, row);
+      if (b) r = fma(a0, b[row], r);
+      if (a2 != T(0)) r = fma(a2, out[row], r);
+      out[row] = r;
+    }
+  }
+}
+
+// the point-Jacobi sweep of k_jacobi on the HDIA copy of ND
+template <typename T, typename V = T>
+__global__ void __launch_bounds__(256, HdiaMinBlocks<T>::value)
+    k_jacobi_hdia(int nr, const int *__restrict__ dptr, const int *__restrict__ doff, const V *__restrict__ hv,
+                  const T *__restrict__ d, const T *__restrict__ x, const T *__restrict__ ty, int first, T omega,
+                  T alpha, T beta, T *out, const float *__restrict__ rs = nullptr) {
+  pdl_enter();
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int ns = (nr + 31) >> 5;
+  for (int sl = warp; sl < ns; sl += nwarps) {
+    const int row = (sl << 5) + lane;
+    T acc;
+    if (first == 2)
+      acc = hdia_row<T>(dptr, doff, hv, sl, row, nr, lane, [&](int j) { return omega * __ldg(x + j); });
+    else if (first)
+      acc = hdia_row<T>(dptr, doff, hv, sl, row, nr, lane,
+                        [&](int j) { return omega * (__ldg(d + j) * __ldg(x + j)); });
+    else
+      acc = hdia_row<T>(dptr, doff, hv, sl, row, nr, lane, [&](int j) { return __ldg(ty + j); });
+    if (row < nr)
+      out[row] = jac_row(d[row], x[row], row_scaled<T, V>(acc, rs, row),
+                         (!first && omega != T(1)) ? ty[row] : T(0), first != 0, omega, alpha, beta,
+                         beta != T(0) ? out[row] : T(0));
+  }
+}
+
 // FP16-valued prolongator with an FP32 per-row scale (precision form):
 // out[i] += scale[i] * sum_j h_ij v_j
 template <int TPR>
@@ -444,6 +559,7 @@ __global__ void __launch_bounds__(256) k_spmv_h(int nr, const int *__restrict__ 
                                                 const __half *__restrict__ hval,
                                                 const float *__restrict__ scale,
                                                 const float *__restrict__ v, float *out) {
+  pdl_enter();
   constexpr int RPW = 32 / TPR;
   const int lane = threadIdx.x & 31;
   const int sub = lane % TPR;
@@ -484,6 +600,7 @@ __global__ void __launch_bounds__(256) k_jacobi(int nr, const int *__restrict__ 
                                                 const T *__restrict__ ty, int first,
                                                 T omega, T alpha, T beta, T *out,
                                                 const float *__restrict__ rs = nullptr) {
+  pdl_enter();
   constexpr int RPW = 32 / TPR;
   const int lane = threadIdx.x & 31;
   const int sub = lane % TPR;
@@ -516,6 +633,7 @@ __global__ void __launch_bounds__(256) k_jacobi(int nr, const int *__restrict__ 
 template <typename T>
 __global__ void __launch_bounds__(256) k_gemv(int n, const T *__restrict__ M, const T *__restrict__ x,
                                               T alpha, T beta, T *out) {
+  pdl_enter();
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -561,6 +679,7 @@ __global__ void k_kappa_grad(int idim, double ih2, const double *__restrict__ ka
 template <typename T>
 __global__ void k_diag(int n, const T *__restrict__ d, const T *__restrict__ x, T alpha, T beta,
                        T *out) {
+  pdl_enter();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     T r = alpha * (d[i] * x[i]);
     if (beta != T(0)) r = fma(beta, out[i], r);
@@ -570,6 +689,7 @@ __global__ void k_diag(int n, const T *__restrict__ d, const T *__restrict__ x, 
 
 template <typename A, typename B>
 __global__ void k_cast(int n, const A *__restrict__ x, B *__restrict__ y) {
+  pdl_enter();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     y[i] = (B)x[i];
 }
@@ -594,6 +714,7 @@ __device__ __forceinline__ void cast4_st(float *p, const float (&v)[4]) {
 }
 template <typename A, typename B>
 __global__ void __launch_bounds__(256) k_cast4(int n, const A *__restrict__ x, B *__restrict__ y) {
+  pdl_enter();
   const int n4 = n >> 2, stride = gridDim.x * blockDim.x, t = blockIdx.x * blockDim.x + threadIdx.x;
   for (int i = t; i < n4; i += stride) {
     A a[4];
@@ -608,6 +729,7 @@ __global__ void __launch_bounds__(256) k_cast4(int n, const A *__restrict__ x, B
 
 template <typename T>
 __global__ void k_fill(int n, T v, T *__restrict__ y) {
+  pdl_enter();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     y[i] = v;
 }
@@ -1110,6 +1232,7 @@ __global__ void __launch_bounds__(kRedThreads) k_kry_beta(int n, const double *_
                                                          const double *__restrict__ q,
                                                          const double *__restrict__ r, KState *st,
                                                          double *partial) {
+  pdl_enter();
   __shared__ double sh[32];
   if (st->done) return;
   const int it = st->it, method = st->method;
@@ -1149,6 +1272,7 @@ __global__ void __launch_bounds__(256) k_kry_spmv(int nr, const int *__restrict_
                                                   const double *__restrict__ z, double *d0, double *d1,
                                                   double *__restrict__ q, const double *__restrict__ r,
                                                   KState *st, double *partial) {
+  pdl_enter();
   __shared__ double sh[32];
   if (st->done) return;
   constexpr int RPW = 32 / TPR;
@@ -1208,6 +1332,7 @@ __global__ void __launch_bounds__(256) k_kry_spmv_sell(int nr, const int *__rest
                                                        const double *__restrict__ z, double *d0, double *d1,
                                                        double *__restrict__ q, const double *__restrict__ r,
                                                        KState *st, double *partial) {
+  pdl_enter();
   __shared__ double sh[32];
   if (st->done) return;
   const int it = st->it;
@@ -1255,10 +1380,63 @@ __global__ void __launch_bounds__(256) k_kry_spmv_sell(int nr, const int *__rest
   }
 }
 
+// k_kry_spmv on the HDIA copy of A (one thread per row, a warp per slice:
+// the rows and the reduction order of k_kry_spmv_sell)
+__global__ void __launch_bounds__(256) k_kry_spmv_hdia(int nr, const int *__restrict__ dptr,
+                                                       const int *__restrict__ doff, const double *__restrict__ hv,
+                                                       const double *__restrict__ z, double *d0, double *d1,
+                                                       double *__restrict__ q, const double *__restrict__ r,
+                                                       KState *st, double *partial) {
+  pdl_enter();
+  __shared__ double sh[32];
+  if (st->done) return;
+  const int it = st->it;
+  const bool first = it == 0;
+  const double beta = st->beta;
+  const double *dold = (it & 1) ? d0 : d1;
+  double *dnew = (it & 1) ? d1 : d0;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int ns = (nr + 31) >> 5;
+  double sdq = 0, sdr = 0;
+  for (int sl = warp; sl < ns; sl += nwarps) {
+    const int row = (sl << 5) + lane;
+    const double s =
+        first ? hdia_row<double>(dptr, doff, hv, sl, row, nr, lane, [&](int j) { return __ldg(z + j); })
+              : hdia_row<double>(dptr, doff, hv, sl, row, nr, lane,
+                                 [&](int j) { return fma(beta, dold[j], __ldg(z + j)); });
+    if (row < nr) {
+      const double di = first ? z[row] : fma(beta, dold[row], z[row]);
+      dnew[row] = di;
+      q[row] = s;
+      sdq = fma(di, s, sdq);
+      sdr = fma(di, r[row], sdr);
+    }
+  }
+  sdq = block_sum(sdq, sh);
+  sdr = block_sum(sdr, sh);
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = sdq;
+    partial[2 * blockIdx.x + 1] = sdr;
+  }
+  if (kry_last_block(&st->ticket[1])) {
+    const double dq = kry_sum_partials(partial, gridDim.x, 2, 0, sh);
+    const double dr = kry_sum_partials(partial, gridDim.x, 2, 1, sh);
+    if (threadIdx.x == 0) {
+      st->dq = dq;
+      st->dr = dr;
+      st->alpha = (st->method == 1) ? dr / dq : st->rho / dq;
+      st->ticket[1] = 0u;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kRedThreads) k_kry_update(int n, const double *d0, const double *d1,
                                                            const double *__restrict__ q, double *x,
                                                            double *r, KState *st, double *partial,
                                                            cudaGraphConditionalHandle hc) {
+  pdl_enter();
   __shared__ double sh[32];
   if (st->done) return;
   const int it = st->it;
