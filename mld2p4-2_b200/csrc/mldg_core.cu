@@ -267,6 +267,7 @@ struct DCSR {
   __half *hdhval = nullptr;
   int64_t hdslots = 0;
   bool hdia() const { return sell == 5 && hdptr != nullptr; }
+  bool hd16 = false;  // HDIA kernels with 16 diagonals' loads per pass (long rows) instead of 4
   int hd_nslice() const { return nslice(); }
   // staged SELL tiles (k_spmv_stg, k_jacobi_stg): packed blocks of
   // consecutive slices and their descriptors, the largest block tblock
@@ -761,6 +762,13 @@ static int ilog2(int K) {
 struct Engine {
   virtual ~Engine() {}
   virtual void record(char trans) = 0;  // issue one V-cycle: xin (FP64) -> yout (FP64)
+  // With kry_io set (inside a CG/FCG solve of an FP32 V-cycle) record()
+  // leaves out its two precision casts: the V-cycle starts from the FP32 copy
+  // of r that the Krylov kernels write to kry_x32() and ends in kry_y32(),
+  // which they read as z.  Both are null for an FP64 V-cycle.
+  bool kry_io = false;
+  virtual float *kry_x32() { return nullptr; }
+  virtual float *kry_y32() { return nullptr; }
   // Multi-RHS V-cycle on K row-interleaved columns: xin_m -> yout_m (FP64,
   // n0 x K interleaved).  ensure_multi allocates the K-wide buffers (true when
   // they were reallocated, which invalidates captured multi graphs).
@@ -1061,7 +1069,11 @@ struct EngineT : Engine {
     const int64_t vec = (int64_t)A.nc * sizeof(T) + (int64_t)A.nr * sizeof(T) * (1 + (b ? 1 : 0) + (a2 != T(0) ? 1 : 0));
     if (A.hdia() && hdv) {
       begin(MLDG_KERNEL_SPMV);
-      kl(k_spmv_hdia<T, V>, blocks_for((int64_t)A.hd_nslice() * 32), 256, A.nr, A.hdptr, A.hdoff, hdv, v, a1,
+      if (A.hd16)
+        kl(k_spmv_hdia<T, V, 16>, blocks_for((int64_t)A.hd_nslice() * 32), 256, A.nr, A.hdptr, A.hdoff, hdv, v, a1,
+           b, a0, out, a2, rs);
+      else
+      kl(k_spmv_hdia<T, V, 4>, blocks_for((int64_t)A.hd_nslice() * 32), 256, A.nr, A.hdptr, A.hdoff, hdv, v, a1,
                                                                                  b, a0, out, a2, rs);
       end(A.mat_bytes() + vec, A.alg_bytes() + vec);
       return;
@@ -1126,7 +1138,11 @@ struct EngineT : Engine {
     const int64_t vec = (int64_t)ND.nr * sizeof(T) * (3 + (first ? 0 : 1) + (beta != T(0) ? 1 : 0));
     if (ND.hdia() && hdv) {
       begin(MLDG_KERNEL_JACOBI);
-      kl(k_jacobi_hdia<T, V>, blocks_for((int64_t)ND.hd_nslice() * 32), 256, 
+      if (ND.hd16)
+        kl(k_jacobi_hdia<T, V, 16>, blocks_for((int64_t)ND.hd_nslice() * 32), 256, ND.nr, ND.hdptr, ND.hdoff, hdv, d,
+           x, ty, first, omega, alpha, beta, out, rs);
+      else
+      kl(k_jacobi_hdia<T, V, 4>, blocks_for((int64_t)ND.hd_nslice() * 32), 256, 
           ND.nr, ND.hdptr, ND.hdoff, hdv, d, x, ty, first, omega, alpha, beta, out, rs);
       end(ND.mat_bytes() + vec, ND.alg_bytes() + vec);
       return;
@@ -1563,6 +1579,14 @@ struct EngineT : Engine {
     }
   }
   void k_axpby_impl(int n, const T *x, T beta, T *y);
+  float *kry_x32() override {
+    if constexpr (std::is_same<T, float>::value) return lv.empty() ? nullptr : lv[0].x;
+    return nullptr;
+  }
+  float *kry_y32() override {
+    if constexpr (std::is_same<T, float>::value) return lv.empty() ? nullptr : lv[0].y;
+    return nullptr;
+  }
 
   // V-cycle body (mld_d_inner_mult)
   void vcycle(int l, char trans) {
@@ -1777,11 +1801,13 @@ struct EngineT : Engine {
         };
         // t = -4: the staged SELL kernels; t = -5: the HDIA copy
         const bool has_hd = op->hdptr && (op->h16() ? op->hdhval != nullptr : op->hdval != nullptr);
-        for (int t : {1, 2, 4, 8, 16, 32, -1, -2, -3, -4, -5}) {
+        bool best_hd16 = false;
+        for (int t : {1, 2, 4, 8, 16, 32, -1, -2, -3, -4, -5, -6}) {
           if (t < 0 && t >= -3 && !op->soff) continue;
           if (t == -4 && !op->tiles) continue;
-          if (t == -5 && !has_hd) continue;
-          op->sell = t < 0 ? -t : 0;
+          if (t <= -5 && !has_hd) continue;
+          op->sell = t < 0 ? std::min(-t, 5) : 0;
+          op->hd16 = t == -6;
           if (t > 0) op->tpr = t;
           run();  // warm
           MLDG_CUDA(cudaEventRecord(e0, st));
@@ -1793,16 +1819,18 @@ struct EngineT : Engine {
           if (ms < best) {
             best = ms;
             best_t = t > 0 ? t : best_t;
-            best_sell = t < 0 ? -t : 0;
+            best_sell = t < 0 ? std::min(-t, 5) : 0;
+            best_hd16 = t == -6;
           }
         }
         op->tpr = best_t;
         op->sell = best_sell;
+        op->hd16 = best_hd16;
         if (std::getenv("MLDG_VERBOSE"))
           std::fprintf(stderr, "mldg: spmv autotune level %zu %-4s n=%d nnz=%lld -> %s%d %.4f ms\n", l,
                        names[oi], op->nr, (long long)op->nnz,
-                       best_sell >= 5 ? "hdia" : (best_sell == 4 ? "staged sell" : (best_sell ? "sell" : "csr tpr ")),
-                       best_sell >= 4 ? 1 : (best_sell ? best_sell : best_t),
+                       best_sell >= 5 ? "hdia u" : (best_sell == 4 ? "staged sell" : (best_sell ? "sell" : "csr tpr ")),
+                       best_sell >= 5 ? (best_hd16 ? 16 : 4) : (best_sell == 4 ? 1 : (best_sell ? best_sell : best_t)),
                        best / reps);
       }
     }
@@ -2547,7 +2575,7 @@ struct EngineT : Engine {
     probe_armed = false;
     std::memset(seen, 0, sizeof seen);
     Lev &F = lv[0];
-    if (!std::is_same<T, double>::value) {
+    if (!std::is_same<T, double>::value && !kry_io) {
       begin(MLDG_KERNEL_VEC);
       cast(F.n, xin, F.x);
       end((int64_t)F.n * (8 + sizeof(T)));
@@ -2573,7 +2601,7 @@ struct EngineT : Engine {
       vcycle(0, trans);
     }
     end_fbgs();
-    if (!std::is_same<T, double>::value) {
+    if (!std::is_same<T, double>::value && !kry_io) {
       cur_lev = 0;
       begin(MLDG_KERNEL_VEC);
       cast(F.n, F.y, yout);
@@ -2615,6 +2643,9 @@ void EngineT<float>::prolong(Lev &C, float *y) {
 // ---------------------------------------------------------------------------
 struct Handle {
   mldg_opts opts{};
+  // the CG/FCG kernels being recorded read z in FP32 and write the FP32 copy
+  // of r (EngineBase::kry_io); set while a whole solve or a batch is captured
+  bool kio = false;
   // changes at every finalize and destroy: identifies the finalized state
   // that a cached batch graph was captured from
   uint64_t serial = 0;
@@ -4211,12 +4242,15 @@ static Engine *make_engine(Handle *h) {
           op->sell = (f >= 1 && f <= 3) ? f : 1;
         }
   // MLDG_HDIA_FORCE: every operator with an HDIA copy uses it (measurement
-  // aid and test hook)
+  // aid and test hook; the value 16 picks the 16-diagonal passes)
   if (std::getenv("MLDG_HDIA_FORCE"))
     for (auto &L : e->lv)
       for (DCSR<T> *op : {&L.A, &L.AT, &L.P, &L.R, &L.ND, &L.NDT})
         if (op->hdptr && (op->h16() ? op->hdhval != nullptr : op->hdval != nullptr))
+        {
           op->sell = 5;
+          op->hd16 = std::atoi(std::getenv("MLDG_HDIA_FORCE")) == 16;
+        }
   // MLDG_STG_FORCE: every operator with staged tiles uses them
   if (std::getenv("MLDG_STG_FORCE"))
     for (auto &L : e->lv)
@@ -4542,6 +4576,11 @@ static void spmv64(Handle *h, const DCSR<double> &A, const double *v, double a1,
 static void krylov_prefix(Handle *h, const DCSR<double> &A, cudaGraphConditionalHandle hc) {
   const int n = h->n0;
   spmv64(h, A, h->kx, -1.0, h->kb, 1.0, h->xin);  // r = b - A x
+  if (h->kio) {  // the first V-cycle's FP32 input
+    k_cast<double, float><<<(int)std::min<int64_t>(((int64_t)n + 255) / 256, (int64_t)h->nsm * 8), 256, 0, h->st>>>(
+        n, h->xin, h->eng->kry_x32());
+    h->last_launches++;
+  }
   k_dots<<<kRedBlocks, kRedThreads, 0, h->st>>>(n, 2, h->kb, h->kb, h->xin, h->xin, nullptr, nullptr,
                                                 h->kpart);
   k_kry_init<<<1, kRedThreads, 0, h->st>>>(kRedBlocks, h->kpart, h->kpar, h->kst, hc);
@@ -4551,13 +4590,14 @@ static void krylov_prefix(Handle *h, const DCSR<double> &A, cudaGraphConditional
 // One CG/FCG iteration after the preconditioner apply z = M^{-1} r (in yout):
 // three fused kernels (mldg_kernels.cuh, k_kry_*); every kernel returns at
 // once when the device state says the solve is done.
-static void kry_spmv(Handle *h, const DCSR<double> &A) {
+template <typename ZT>
+static void kry_spmv_z(Handle *h, const DCSR<double> &A, const ZT *z) {
   const bool pdl = h->eng->pdl_on();
-  double *r = h->xin, *z = h->yout;
+  double *r = h->xin;
   if (A.hdia() && A.hdval) {
     const int64_t thr = (int64_t)A.hd_nslice() * 32;
     const int g = (int)std::max<int64_t>(1, std::min<int64_t>((thr + 255) / 256, (int64_t)h->nsm * 16));
-    launch_k(pdl, k_kry_spmv_hdia, g, 256, h->st, A.nr, A.hdptr, A.hdoff, A.hdval, z, h->kd, h->kd1, h->kq, r, h->kst,
+    launch_k(pdl, k_kry_spmv_hdia<ZT>, g, 256, h->st, A.nr, A.hdptr, A.hdoff, A.hdval, z, h->kd, h->kd1, h->kq, r, h->kst,
                                           h->kpart);
     return;
   }
@@ -4566,10 +4606,10 @@ static void kry_spmv(Handle *h, const DCSR<double> &A) {
     const int64_t thr = (int64_t)A.nslice() * 32;
     const int g = (int)std::max<int64_t>(1, std::min<int64_t>((thr + 255) / 256, (int64_t)h->nsm * 16));
     if (A.sjd)
-      launch_k(pdl, k_kry_spmv_sell<short>, g, 256, h->st, A.nr, A.soff, A.sjd, A.sval, z, h->kd, h->kd1, h->kq, r,
+      launch_k(pdl, k_kry_spmv_sell<short, ZT>, g, 256, h->st, A.nr, A.soff, A.sjd, A.sval, z, h->kd, h->kd1, h->kq, r,
                                                    h->kst, h->kpart);
     else
-      launch_k(pdl, k_kry_spmv_sell<int>, g, 256, h->st, A.nr, A.soff, A.sja, A.sval, z, h->kd, h->kd1, h->kq, r,
+      launch_k(pdl, k_kry_spmv_sell<int, ZT>, g, 256, h->st, A.nr, A.soff, A.sja, A.sval, z, h->kd, h->kd1, h->kq, r,
                                                  h->kst, h->kpart);
     return;
   }
@@ -4579,10 +4619,10 @@ static void kry_spmv(Handle *h, const DCSR<double> &A) {
 #define CASE(K)                                                                                  \
   case K:                                                                                        \
     if (A.jd)                                                                                    \
-      launch_k(pdl, k_kry_spmv<K, short>, g, 256, h->st, A.nr, A.irp, A.jd, A.val, z, h->kd, h->kd1, h->kq, r, \
+      launch_k(pdl, k_kry_spmv<K, short, ZT>, g, 256, h->st, A.nr, A.irp, A.jd, A.val, z, h->kd, h->kd1, h->kq, r, \
                                                  h->kst, h->kpart);                              \
     else                                                                                         \
-      launch_k(pdl, k_kry_spmv<K, int>, g, 256, h->st, A.nr, A.irp, A.ja, A.val, z, h->kd, h->kd1, h->kq, r,   \
+      launch_k(pdl, k_kry_spmv<K, int, ZT>, g, 256, h->st, A.nr, A.irp, A.ja, A.val, z, h->kd, h->kd1, h->kq, r,   \
                                                h->kst, h->kpart);                                \
     break;
     CASE(1) CASE(2) CASE(4) CASE(8) CASE(16) CASE(32)
@@ -4591,17 +4631,30 @@ static void kry_spmv(Handle *h, const DCSR<double> &A) {
   }
 }
 
+// z: the V-cycle's FP64 output, or its FP32 output when h->kio is set
+static void kry_spmv(Handle *h, const DCSR<double> &A) {
+  if (h->kio)
+    kry_spmv_z<float>(h, A, h->eng->kry_y32());
+  else
+    kry_spmv_z<double>(h, A, h->yout);
+}
+
 static void krylov_iteration(Handle *h, const DCSR<double> &A, cudaGraphConditionalHandle hc) {
   const bool pdl = h->eng->pdl_on();
   const int n = h->n0;
-  double *r = h->xin, *z = h->yout;
+  double *r = h->xin;
   // vector kernels: 8 blocks of 256 threads per SM (64 warps), so that enough
   // loads are in flight to stream the vectors at HBM bandwidth
   const int gv = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)n + 255) / 256, (int64_t)h->nsm * 8));
-  launch_k(pdl, k_kry_beta, gv, kRedThreads, h->st, n, z, h->kq, r, h->kst, h->kpart);
+  if (h->kio)
+    launch_k(pdl, k_kry_beta<float>, gv, kRedThreads, h->st, n, (const float *)h->eng->kry_y32(), h->kq, r, h->kst,
+             h->kpart);
+  else
+    launch_k(pdl, k_kry_beta<double>, gv, kRedThreads, h->st, n, (const double *)h->yout, h->kq, r, h->kst,
+             h->kpart);
   kry_spmv(h, A);
-  launch_k(pdl, k_kry_update, gv, kRedThreads, h->st, n, h->kd, h->kd1, h->kq, h->kx, r, h->kst, h->kpart,
-                                                      hc);
+  launch_k(pdl, k_kry_update, gv, kRedThreads, h->st, n, (const double *)h->kd, (const double *)h->kd1,
+           (const double *)h->kq, h->kx, r, h->kst, h->kpart, hc, h->kio ? h->eng->kry_x32() : (float *)nullptr);
   h->last_launches += 3;
 }
 
@@ -4660,12 +4713,28 @@ static void tune_krylov_spmv(Handle *h) {
 // graph: prefix, then a WHILE node whose body is the V-cycle and one
 // iteration.  The stopping test runs on the device, so the solve makes no
 // host round trip; the iteration count is read back afterwards.
+// FP32 V-cycle inside a captured CG/FCG solve: no precision casts at its
+// ends (EngineBase::kry_io); MLDG_NO_KRY_IO keeps them
+static bool kry_io_ok(Handle *h) { return h->eng->kry_y32() != nullptr && !std::getenv("MLDG_NO_KRY_IO"); }
+struct KioScope {  // sets h->kio and the engine's kry_io for one capture
+  Handle *h;
+  KioScope(Handle *hh, bool on) : h(hh) {
+    h->kio = on;
+    h->eng->kry_io = on;
+  }
+  ~KioScope() {
+    h->kio = false;
+    h->eng->kry_io = false;
+  }
+};
+
 static void capture_solve(Handle *h, int method, char trans, const DCSR<double> &A) {
   const int t = trans == 'N' ? 0 : 1;
   if (h->sgraph[method][t]) return;
   cudaGraph_t g = nullptr;
   MLDG_CUDA(cudaGraphCreate(&g, 0));
   const int64_t l0 = h->last_launches;
+  KioScope kio(h, kry_io_ok(h));
   try {
     cudaGraphConditionalHandle hc;
     MLDG_CUDA(cudaGraphConditionalHandleCreate(&hc, g, 0, cudaGraphCondAssignDefault));
@@ -5045,7 +5114,10 @@ static std::unique_ptr<BatchGraph> capture_batch(int nsys, Handle **hs, int meth
         Handle *h = hs[i];
         MLDG_CUDA(cudaStreamWaitEvent(h->st, evs[nsys], 0));
         const int64_t l0 = h->last_launches;
-        krylov_prefix(h, h->A0, 0);
+        {
+          KioScope kio(h, kry_io_ok(h));
+          krylov_prefix(h, h->A0, 0);
+        }
         bg->launches_pre += h->last_launches - l0;
         h->last_launches = l0;
         MLDG_CUDA(cudaEventRecord(evs[i], h->st));
@@ -5090,6 +5162,7 @@ static std::unique_ptr<BatchGraph> capture_batch(int nsys, Handle **hs, int meth
       cudaGraph_t br = ip.conditional.phGraph_out[0];
       const int64_t l0 = h->last_launches;
       MLDG_CUDA(cudaStreamBeginCaptureToGraph(h->st, br, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+      KioScope kio(h, kry_io_ok(h));
       h->eng->capturing = true;
       try {
         h->eng->record('N');

@@ -472,15 +472,18 @@ __global__ void __launch_bounds__(256) k_jacobi_sell(int nr, const int *__restri
 // with 8/16-byte accesses, 2 slices per warp, and offsets staged in shared
 // memory per block all ran slower than this one-row-per-thread form, which
 // the register limit of __launch_bounds__ keeps at full occupancy.)
-constexpr int kHdiaU = 4;
-template <typename T>
-struct HdiaMinBlocks {  // 256-thread blocks per SM: 32 registers (FP32), 40 (FP64)
-  static constexpr int value = sizeof(T) == 8 ? 6 : 8;
+// U = 4 for slices of a few diagonals (a stencil level), 16 for the long
+// rows of a coarse level (more loads in flight per pass); the autotuner
+// times both.
+template <typename T, int U>
+struct HdiaMinBlocks {  // 256-thread blocks per SM: 32 registers (FP32), 40 (FP64); U = 16 unbounded
+  static constexpr int value = U > 4 ? 1 : (sizeof(T) == 8 ? 6 : 8);
 };
 
-template <typename T, typename F, typename V>
+template <typename T, int U = 4, typename F, typename V>
 __device__ __forceinline__ T hdia_row(const int *__restrict__ dptr, const int *__restrict__ doff,
                                       const V *__restrict__ hv, int sl, int row, int n, int lane, F f) {
+  constexpr int kHdiaU = U;
   int k = __ldg(dptr + sl);
   const int k1 = __ldg(dptr + sl + 1);
   T acc = T(0);
@@ -501,8 +504,8 @@ __device__ __forceinline__ T hdia_row(const int *__restrict__ dptr, const int *_
 }
 
 // out[i] = a0*b[i] + a1*(A v)[i] + a2*out[i] on the HDIA copy of A
-template <typename T, typename V = T>
-__global__ void __launch_bounds__(256, HdiaMinBlocks<T>::value)
+template <typename T, typename V = T, int U = 4>
+__global__ void __launch_bounds__(256, (HdiaMinBlocks<T, U>::value))
     k_spmv_hdia(int nr, const int *__restrict__ dptr, const int *__restrict__ doff, const V *__restrict__ hv,
                 const T *__restrict__ v, T a1, const T *__restrict__ b, T a0, T *out, T a2,
                 const float *__restrict__ rs = nullptr) {
@@ -513,7 +516,7 @@ __global__ void __launch_bounds__(256, HdiaMinBlocks<T>::value)
   const int ns = (nr + 31) >> 5;
   for (int sl = warp; sl < ns; sl += nwarps) {
     const int row = (sl << 5) + lane;
-    const T acc = hdia_row<T>(dptr, doff, hv, sl, row, nr, lane, [&](int j) { return __ldg(v + j); });
+    const T acc = hdia_row<T, U>(dptr, doff, hv, sl, row, nr, lane, [&](int j) { return __ldg(v + j); });
     if (row < nr) {
       T r = a1 * row_scaled<T, V>(acc, rs, row);
       if (b) r = fma(a0, b[row], r);
@@ -524,8 +527,8 @@ __global__ void __launch_bounds__(256, HdiaMinBlocks<T>::value)
 }
 
 // the point-Jacobi sweep of k_jacobi on the HDIA copy of ND
-template <typename T, typename V = T>
-__global__ void __launch_bounds__(256, HdiaMinBlocks<T>::value)
+template <typename T, typename V = T, int U = 4>
+__global__ void __launch_bounds__(256, (HdiaMinBlocks<T, U>::value))
     k_jacobi_hdia(int nr, const int *__restrict__ dptr, const int *__restrict__ doff, const V *__restrict__ hv,
                   const T *__restrict__ d, const T *__restrict__ x, const T *__restrict__ ty, int first, T omega,
                   T alpha, T beta, T *out, const float *__restrict__ rs = nullptr) {
@@ -538,12 +541,12 @@ __global__ void __launch_bounds__(256, HdiaMinBlocks<T>::value)
     const int row = (sl << 5) + lane;
     T acc;
     if (first == 2)
-      acc = hdia_row<T>(dptr, doff, hv, sl, row, nr, lane, [&](int j) { return omega * __ldg(x + j); });
+      acc = hdia_row<T, U>(dptr, doff, hv, sl, row, nr, lane, [&](int j) { return omega * __ldg(x + j); });
     else if (first)
-      acc = hdia_row<T>(dptr, doff, hv, sl, row, nr, lane,
-                        [&](int j) { return omega * (__ldg(d + j) * __ldg(x + j)); });
+      acc = hdia_row<T, U>(dptr, doff, hv, sl, row, nr, lane,
+                           [&](int j) { return omega * (__ldg(d + j) * __ldg(x + j)); });
     else
-      acc = hdia_row<T>(dptr, doff, hv, sl, row, nr, lane, [&](int j) { return __ldg(ty + j); });
+      acc = hdia_row<T, U>(dptr, doff, hv, sl, row, nr, lane, [&](int j) { return __ldg(ty + j); });
     if (row < nr)
       out[row] = jac_row(d[row], x[row], row_scaled<T, V>(acc, rs, row),
                          (!first && omega != T(1)) ? ty[row] : T(0), first != 0, omega, alpha, beta,
@@ -1157,6 +1160,9 @@ __global__ void __launch_bounds__(kRedThreads) k_dots_final(int nblocks, const d
 //                that repeats the iteration (a whole solve is one graph launch)
 // Each kernel reduces deterministically: every block writes its partial sums,
 // and the last block to finish (a ticket counter) adds them in block order.
+// With an FP32 V-cycle the kernels read z as the V-cycle's FP32 output (ZT =
+// float, widened exactly) and k_kry_update also writes the FP32 copy of r
+// the next V-cycle starts from, so no separate precision casts run.
 // The direction lives in two buffers used alternately (d0 on even, d1 on odd
 // iterations), so q = A d reads the previous direction while the new one is
 // written.
@@ -1228,7 +1234,8 @@ __global__ void __launch_bounds__(kRedThreads) k_kry_init(int nblocks, const dou
   }
 }
 
-__global__ void __launch_bounds__(kRedThreads) k_kry_beta(int n, const double *__restrict__ z,
+template <typename ZT>
+__global__ void __launch_bounds__(kRedThreads) k_kry_beta(int n, const ZT *__restrict__ z,
                                                          const double *__restrict__ q,
                                                          const double *__restrict__ r, KState *st,
                                                          double *partial) {
@@ -1240,10 +1247,10 @@ __global__ void __launch_bounds__(kRedThreads) k_kry_beta(int n, const double *_
   if (method == 1) {
     if (it > 0)
       for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        s = fma(z[i], q[i], s);
+        s = fma((double)z[i], q[i], s);
   } else {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-      s = fma(r[i], z[i], s);
+      s = fma(r[i], (double)z[i], s);
   }
   s = block_sum(s, sh);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
@@ -1265,11 +1272,11 @@ __global__ void __launch_bounds__(kRedThreads) k_kry_beta(int n, const double *_
 // q = A d with d = z + beta*d_prev formed on the fly for every entry (the
 // same fma as the stored d, so both agree bit for bit); TPR lanes per row as
 // in k_spmv.  partial[2*b + {0,1}] = block sums of d_i q_i and d_i r_i.
-template <int TPR, typename CI>
+template <int TPR, typename CI, typename ZT>
 __global__ void __launch_bounds__(256) k_kry_spmv(int nr, const int *__restrict__ irp,
                                                   const CI *__restrict__ ja,
                                                   const double *__restrict__ val,
-                                                  const double *__restrict__ z, double *d0, double *d1,
+                                                  const ZT *__restrict__ z, double *d0, double *d1,
                                                   double *__restrict__ q, const double *__restrict__ r,
                                                   KState *st, double *partial) {
   pdl_enter();
@@ -1293,14 +1300,14 @@ __global__ void __launch_bounds__(256) k_kry_spmv(int nr, const int *__restrict_
     if (row < nr) {
       const int k0 = irp[row] + sub, e = irp[row + 1];
       if (first)
-        s = csr_lane_sum<double, TPR>(k0, e, row, ja, val, [&](int j) { return __ldg(z + j); });
+        s = csr_lane_sum<double, TPR>(k0, e, row, ja, val, [&](int j) { return (double)__ldg(z + j); });
       else
-        s = csr_lane_sum<double, TPR>(k0, e, row, ja, val, [&](int j) { return fma(beta, dold[j], __ldg(z + j)); });
+        s = csr_lane_sum<double, TPR>(k0, e, row, ja, val, [&](int j) { return fma(beta, dold[j], (double)__ldg(z + j)); });
     }
 #pragma unroll
     for (int o = TPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, TPR);
     if (row < nr && sub == 0) {
-      const double di = first ? z[row] : fma(beta, dold[row], z[row]);
+      const double di = first ? (double)z[row] : fma(beta, dold[row], (double)z[row]);
       dnew[row] = di;
       q[row] = s;
       sdq = fma(di, s, sdq);
@@ -1326,10 +1333,10 @@ __global__ void __launch_bounds__(256) k_kry_spmv(int nr, const int *__restrict_
 }
 
 // k_kry_spmv on the SELL copy of A (one thread per row)
-template <typename CI>
+template <typename CI, typename ZT>
 __global__ void __launch_bounds__(256) k_kry_spmv_sell(int nr, const int *__restrict__ soff,
                                                        const CI *__restrict__ sj, const double *__restrict__ sv,
-                                                       const double *__restrict__ z, double *d0, double *d1,
+                                                       const ZT *__restrict__ z, double *d0, double *d1,
                                                        double *__restrict__ q, const double *__restrict__ r,
                                                        KState *st, double *partial) {
   pdl_enter();
@@ -1349,13 +1356,13 @@ __global__ void __launch_bounds__(256) k_kry_spmv_sell(int nr, const int *__rest
     const int row = (sl << 5) + lane;
     double acc[1];
     if (first)
-      sell_rows<double, CI, 1>(soff, sj, sv, sl, ns, lane, [&](int j) { return __ldg(z + j); }, acc);
+      sell_rows<double, CI, 1>(soff, sj, sv, sl, ns, lane, [&](int j) { return (double)__ldg(z + j); }, acc);
     else
-      sell_rows<double, CI, 1>(soff, sj, sv, sl, ns, lane, [&](int j) { return fma(beta, dold[j], __ldg(z + j)); },
+      sell_rows<double, CI, 1>(soff, sj, sv, sl, ns, lane, [&](int j) { return fma(beta, dold[j], (double)__ldg(z + j)); },
                                acc);
     const double s = acc[0];
     if (row < nr) {
-      const double di = first ? z[row] : fma(beta, dold[row], z[row]);
+      const double di = first ? (double)z[row] : fma(beta, dold[row], (double)z[row]);
       dnew[row] = di;
       q[row] = s;
       sdq = fma(di, s, sdq);
@@ -1382,9 +1389,10 @@ __global__ void __launch_bounds__(256) k_kry_spmv_sell(int nr, const int *__rest
 
 // k_kry_spmv on the HDIA copy of A (one thread per row, a warp per slice:
 // the rows and the reduction order of k_kry_spmv_sell)
+template <typename ZT>
 __global__ void __launch_bounds__(256) k_kry_spmv_hdia(int nr, const int *__restrict__ dptr,
                                                        const int *__restrict__ doff, const double *__restrict__ hv,
-                                                       const double *__restrict__ z, double *d0, double *d1,
+                                                       const ZT *__restrict__ z, double *d0, double *d1,
                                                        double *__restrict__ q, const double *__restrict__ r,
                                                        KState *st, double *partial) {
   pdl_enter();
@@ -1403,11 +1411,11 @@ __global__ void __launch_bounds__(256) k_kry_spmv_hdia(int nr, const int *__rest
   for (int sl = warp; sl < ns; sl += nwarps) {
     const int row = (sl << 5) + lane;
     const double s =
-        first ? hdia_row<double>(dptr, doff, hv, sl, row, nr, lane, [&](int j) { return __ldg(z + j); })
+        first ? hdia_row<double>(dptr, doff, hv, sl, row, nr, lane, [&](int j) { return (double)__ldg(z + j); })
               : hdia_row<double>(dptr, doff, hv, sl, row, nr, lane,
-                                 [&](int j) { return fma(beta, dold[j], __ldg(z + j)); });
+                                 [&](int j) { return fma(beta, dold[j], (double)__ldg(z + j)); });
     if (row < nr) {
-      const double di = first ? z[row] : fma(beta, dold[row], z[row]);
+      const double di = first ? (double)z[row] : fma(beta, dold[row], (double)z[row]);
       dnew[row] = di;
       q[row] = s;
       sdq = fma(di, s, sdq);
@@ -1435,7 +1443,7 @@ __global__ void __launch_bounds__(256) k_kry_spmv_hdia(int nr, const int *__rest
 __global__ void __launch_bounds__(kRedThreads) k_kry_update(int n, const double *d0, const double *d1,
                                                            const double *__restrict__ q, double *x,
                                                            double *r, KState *st, double *partial,
-                                                           cudaGraphConditionalHandle hc) {
+                                                           cudaGraphConditionalHandle hc, float *r32) {
   pdl_enter();
   __shared__ double sh[32];
   if (st->done) return;
@@ -1447,6 +1455,7 @@ __global__ void __launch_bounds__(kRedThreads) k_kry_update(int n, const double 
     x[i] = fma(alpha, d[i], x[i]);
     const double ri = fma(-alpha, q[i], r[i]);
     r[i] = ri;
+    if (r32) r32[i] = (float)ri;  // the FP32 V-cycle's input, rounded as k_cast does
     s = fma(ri, ri, s);
   }
   s = block_sum(s, sh);

@@ -7,7 +7,8 @@ values on the offsets the row lacks; the SELL kernel sums the same row in
 its stored (ascending) order with zero padding at its end.  Adding an exact
 zero product leaves a sum unchanged, so with launch shapes pinned (no
 autotuning) a hierarchy whose square operators take the HDIA kernels
-(MLDG_HDIA_FORCE; the other operators the SELL kernel) applies bit for bit
+(MLDG_HDIA_FORCE, with 4 or 16 diagonals' loads per pass; the other
+operators the SELL kernel) applies bit for bit
 like the one whose operators all take the SELL kernel (MLDG_SELL_FORCE=1),
 in every precision form, for trans 'N' and 'T'; the FP64 applies also meet
 the oracle bar, and whole FCG solves (the fused Krylov SpMV on the HDIA copy
@@ -30,15 +31,16 @@ def hier(orc):
     return a, op
 
 
+@pytest.mark.parametrize("passes", ["1", "16"])
 @pytest.mark.parametrize("prec", [0, 1, 3])
-def test_hdia_apply_bitwise_equal_to_sell(mld, orc, hier, monkeypatch, prec):
+def test_hdia_apply_bitwise_equal_to_sell(mld, orc, hier, monkeypatch, prec, passes):
     a, op = hier
     monkeypatch.setenv("MLDG_NO_AUTOTUNE", "1")
     monkeypatch.setenv("MLDG_NO_DENSE_INV", "1")
     monkeypatch.setenv("MLDG_SELL_FORCE", "1")
     h_sell = upload_oracle_hierarchy(mld, orc, op, precision=prec)
     # operators without an HDIA copy stay on the SELL kernel
-    monkeypatch.setenv("MLDG_HDIA_FORCE", "1")
+    monkeypatch.setenv("MLDG_HDIA_FORCE", passes)
     h_hd = upload_oracle_hierarchy(mld, orc, op, precision=prec)
     rng = np.random.default_rng(3)
     for trans in ("N", "T"):

@@ -49,16 +49,20 @@ def test_fp32_vcycle_inside_fp64_fcg(mld, orc):
     assert np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref) < 1e-8
 
 
+@pytest.mark.parametrize("prec", [0, 1, 3])
 @pytest.mark.parametrize("method", ["CG", "FCG"])
-def test_graph_solve_equals_host_stepped_solve(mld, orc, method):
+def test_graph_solve_equals_host_stepped_solve(mld, orc, method, prec):
     """A solve without a probe is one graph launch (device-side stopping
     test in a conditional WHILE node); with a probe set, the same kernels run
-    with one host check per iteration.  Both must give the same bits."""
+    with one host check per iteration.  Both must give the same bits -- also
+    with an FP32 V-cycle (prec 1, 3), whose graph solve reads the V-cycle's
+    FP32 output and writes its FP32 input inside the Krylov kernels, while
+    the host-stepped solve casts at the V-cycle's ends."""
     a = orc.gen_pde3d(20, 1, ISO)
     op = orc.Prec(oracle_params(orc, "JACOBI", 2, 0.8, mcs=300))
     op.build(a)
     b = np.random.default_rng(5).uniform(-1, 1, a.nrows)
-    h = upload_oracle_hierarchy(mld, orc, op)
+    h = upload_oracle_hierarchy(mld, orc, op, precision=prec)
     x1, it1, r1 = h.krylov(method, b.copy(), eps=1e-10)
     _, nl1 = h.last_timing()
     h.probe_set(mld.KERNEL_SPMV, 0, 0)  # forces the host-stepped loop
