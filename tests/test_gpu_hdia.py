@@ -134,3 +134,21 @@ def test_hdia_ragged_and_unsorted(mld, orc, monkeypatch):
             y_ref = op.apply(x, trans)
             assert np.linalg.norm(h.apply(x, trans=trans) - y_ref) <= 1e-12 * np.linalg.norm(y_ref), (mangle, trans)
         h.close()
+
+
+def test_tune_file_round_trip(mld, orc, hier, monkeypatch, tmp_path):
+    """MLDG_TUNE_FILE: the first finalize times every operator and appends its
+    choice; a second finalize reads the choices instead of timing (adds no
+    line) and launches the same kernels (the same bits)."""
+    a, op = hier
+    fn = tmp_path / "tune.txt"
+    monkeypatch.setenv("MLDG_TUNE_FILE", str(fn))
+    h1 = upload_oracle_hierarchy(mld, orc, op, precision=3)
+    lines = fn.read_text().splitlines()
+    assert any(s.startswith("spmv 4 1 0 0 ") for s in lines)  # level-0 A of the FP16 operator form
+    h2 = upload_oracle_hierarchy(mld, orc, op, precision=3)
+    assert fn.read_text().splitlines() == lines
+    x = np.random.default_rng(7).uniform(-1, 1, a.nrows)
+    assert np.array_equal(h1.apply(x), h2.apply(x))
+    h1.close()
+    h2.close()
