@@ -440,7 +440,7 @@ constexpr int kRepTPR = 4;
 template <typename T>
 struct DBlk {
   bool ok = false;
-  int n = 0, nblocks = 0, nsteps = 0, W = 0, stage_bytes = 0;
+  int n = 0, nblocks = 0, nsteps = 0, W = 0, stage_bytes = 0, aux_cap = 0;
   size_t smem = 0;
   int64_t nnz = 0, plan_bytes = 0;
   int *bstep = nullptr;
@@ -548,45 +548,42 @@ static void make_h16(Arena &ar, const HostCSR &h, DCSR<T> &d) {
 }
 
 // The HDIA-32 copy of a square CSR matrix (k_spmv_hdia): rows in slices of
-// 32, per slice the ascending
-// distinct column offsets j - i of its entries, and one value per (offset,
-// row), zero where the row has no entry on that offset.  Built only when
+// 32, per slice the ascending distinct column offsets j - i of its entries,
+// and one value per (offset, row), zero where the row has no entry on that
+// offset.  Built only when
 // every row is sorted by column (the kernels then sum a row in its stored
 // order), no slice has more than kHdiaMaxDiag offsets, and the slices store
 // at most an eighth more values than the matrix has entries; MLDG_NO_HDIA
 // skips it.  In the FP16 operator form the values are the FP16 row-scaled
 // ones of make_h16 (its row scales rs are shared).
-constexpr int kHdiaMaxDiag = 64;
+constexpr int kHdiaMaxDiag = 512;
 template <typename T>
 static void build_hdia(Arena &ar, const HostCSR &h, DCSR<T> &d, bool h16) {
   if (std::getenv("MLDG_NO_HDIA") || h.nr == 0 || h.nr != h.nc || h.nnz() == 0) return;
   constexpr int H = 32;
   const int ns = (h.nr + H - 1) / H;
+  // the sorted distinct offsets of slice s, in o (cleared first)
+  auto slice_offsets = [&](int s, std::vector<int> &o) {
+    o.clear();
+    for (int i = s * H; i < std::min(h.nr, s * H + H); ++i)
+      for (int k = h.irp[i]; k < h.irp[i + 1]; ++k) o.push_back(h.ja[k] - i);
+    std::sort(o.begin(), o.end());
+    o.erase(std::unique(o.begin(), o.end()), o.end());
+  };
   std::vector<int> cnt((size_t)ns, 0);
   int bad = 0;
   // pass 1: offsets per slice (counted), sortedness
-#pragma omp parallel for reduction(| : bad) schedule(static, 64)
-  for (int s = 0; s < ns; ++s) {
-    int o[kHdiaMaxDiag];
-    int no = 0;
-    for (int i = s * H; i < std::min(h.nr, s * H + H) && !bad; ++i)
-      for (int k = h.irp[i]; k < h.irp[i + 1]; ++k) {
-        if (k > h.irp[i] && h.ja[k] <= h.ja[k - 1]) {
-          bad = 1;
-          break;
-        }
-        const int off = h.ja[k] - i;
-        int q = 0;
-        while (q < no && o[q] != off) ++q;
-        if (q == no) {
-          if (no == kHdiaMaxDiag) {
-            bad = 1;
-            break;
-          }
-          o[no++] = off;
-        }
-      }
-    cnt[s] = no;
+#pragma omp parallel reduction(| : bad)
+  {
+    std::vector<int> o;
+#pragma omp for schedule(static, 64)
+    for (int s = 0; s < ns; ++s) {
+      for (int i = s * H; i < std::min(h.nr, s * H + H); ++i)
+        for (int k = h.irp[i] + 1; k < h.irp[i + 1]; ++k) bad |= h.ja[k] <= h.ja[k - 1];
+      slice_offsets(s, o);
+      cnt[s] = (int)o.size();
+      bad |= cnt[s] > kHdiaMaxDiag;
+    }
   }
   if (bad) return;
   std::vector<int> dptr((size_t)ns + 1, 0);
@@ -599,28 +596,24 @@ static void build_hdia(Arena &ar, const HostCSR &h, DCSR<T> &d, bool h16) {
   if (h16) h16_values(h, sc, hv);
   std::vector<T> tv(h16 ? 0 : (size_t)slots, T(0));
   std::vector<__half> th(h16 ? (size_t)slots : 0, __float2half_rn(0.f));
-#pragma omp parallel for schedule(static, 64)
-  for (int s = 0; s < ns; ++s) {
-    int *o = doff.data() + dptr[s];
-    int no = 0;
-    for (int i = s * H; i < std::min(h.nr, s * H + H); ++i)
-      for (int k = h.irp[i]; k < h.irp[i + 1]; ++k) {
-        const int off = h.ja[k] - i;
-        int q = 0;
-        while (q < no && o[q] != off) ++q;
-        if (q == no) o[no++] = off;
-      }
-    std::sort(o, o + no);
-    for (int i = s * H; i < std::min(h.nr, s * H + H); ++i) {
-      int q = 0;
-      for (int k = h.irp[i]; k < h.irp[i + 1]; ++k) {
-        const int off = h.ja[k] - i;
-        while (o[q] != off) ++q;  // the row's offsets ascend, like the slice's
-        const size_t e = (size_t)H * ((size_t)dptr[s] + q) + (size_t)(i - s * H);
-        if (h16)
-          th[e] = hv[k];
-        else
-          tv[e] = (T)h.val[k];
+#pragma omp parallel
+  {
+    std::vector<int> o;
+#pragma omp for schedule(static, 64)
+    for (int s = 0; s < ns; ++s) {
+      slice_offsets(s, o);
+      std::copy(o.begin(), o.end(), doff.begin() + dptr[s]);
+      for (int i = s * H; i < std::min(h.nr, s * H + H); ++i) {
+        size_t q = 0;
+        for (int k = h.irp[i]; k < h.irp[i + 1]; ++k) {
+          const int off = h.ja[k] - i;
+          while (o[q] != off) ++q;  // the row's offsets ascend, like the slice's
+          const size_t e = (size_t)H * ((size_t)dptr[s] + q) + (size_t)(i - s * H);
+          if (h16)
+            th[e] = hv[k];
+          else
+            tv[e] = (T)h.val[k];
+        }
       }
     }
   }
@@ -1438,6 +1431,7 @@ struct EngineT : Engine {
     a.nblocks = w.nblocks;
     a.wmask = w.W - 1;
     a.stage_bytes = w.stage_bytes;
+    a.aux_cap = w.aux_cap;
     a.bstep = w.bstep;
     a.sdesc = w.sdesc;
     a.plan = w.plan;
@@ -3541,17 +3535,19 @@ static void rep_check_pair(const HostCSR &Lf, bool lupper, const HostCSR &Uf, bo
 // is cut into P contiguous blocks of about equal rows + entries.  A block's
 // rows are ordered by (global dependency level, row) and grouped into steps
 // of one level each, split where a step's plan would exceed kBlkStageCap
-// bytes.  A dependency on a row of the same block whose ring slot is still
-// intact at the end of the reading step reads the ring, every other one the
-// exchange vector.  The ring holds W values: the smallest power of two that
-// covers every local dependency's reach, at most kBlkWMax.
-constexpr int kBlkStageCap = 24 * 1024;
+// bytes (the pieces of one level are marked, the kernel takes no barrier
+// between them).  A dependency on a row of the same block whose ring slot is
+// still intact at the end of the reading step's level (rows of one level
+// are solved without a barrier between its steps) reads the ring, every
+// other one the exchange vector.  The ring holds W values: the smallest
+// power of two that covers every local dependency's reach, at most kBlkWMax.
+constexpr int kBlkStageCap = 8 * 1024;
 constexpr int kBlkWMax = 8192;
 
 template <typename T>
 struct HostBlk {
   bool ok = false;
-  int n = 0, nblocks = 0, nsteps = 0, W = 0, stage_bytes = 0;
+  int n = 0, nblocks = 0, nsteps = 0, W = 0, stage_bytes = 0, aux_cap = 0;
   size_t smem = 0;
   int64_t nnz = 0, plan_bytes = 0;
   std::vector<int> bstep;
@@ -3632,10 +3628,19 @@ static HostBlk<T> build_blk_host(const HostCSR &m, bool upper, int P) {
   }
   bstep[P] = (int)steps.size();
   const int ns = (int)steps.size();
+  // a step continues the level of the block's previous step; the end of each
+  // step's level (the rows of a level are solved without a barrier)
+  std::vector<int> same((size_t)ns, 0), lvl_end((size_t)ns, 0);
+  for (int b = 0; b < P; ++b) {
+    for (int s = bstep[b] + 1; s < bstep[b + 1]; ++s)
+      same[s] = lev[order[b][steps[s].p0]] == lev[order[b][steps[s - 1].p0]];
+    for (int s = bstep[b + 1] - 1; s >= bstep[b]; --s)
+      lvl_end[s] = (s + 1 < bstep[b + 1] && same[s + 1]) ? lvl_end[s + 1] : steps[s].p1;
+  }
   // ring size: the reach of the local dependencies (capped)
   std::vector<int> step_end((size_t)n);
-  for (const Step &st : steps)
-    for (int q = st.p0; q < st.p1; ++q) step_end[order[st.b][q]] = st.p1;
+  for (int s = 0; s < ns; ++s)
+    for (int q = steps[s].p0; q < steps[s].p1; ++q) step_end[order[steps[s].b][q]] = lvl_end[s];
   int reach = 1;
   for (int ip = 0; ip < n; ++ip) {
     const int o = orig(ip);
@@ -3648,12 +3653,14 @@ static HostBlk<T> build_blk_host(const HostCSR &m, bool upper, int P) {
   while (W < reach && W < kBlkWMax) W *= 2;
   // plan blocks
   std::vector<int64_t> boff((size_t)ns + 1, 0);
-  int capB = 16;
+  int capB = 16, capA = 1;
   for (int s = 0; s < ns; ++s) {
     const int bytes = blk_bytes<T>(steps[s].p1 - steps[s].p0, steps[s].nent);
     boff[s + 1] = boff[s] + bytes;
     capB = std::max(capB, bytes);
+    capA = std::max(capA, 2 * (steps[s].p1 - steps[s].p0) + steps[s].nent);
   }
+  capA = (capA + 1) & ~1;  // keeps the mbarriers after the aux buffers 8-byte aligned
   if (boff[ns] / 16 > INT32_MAX) return w;
   std::vector<uint4> plan((size_t)(boff[ns] / 16), make_uint4(0, 0, 0, 0));
   std::vector<int2> sdesc((size_t)ns);
@@ -3663,7 +3670,7 @@ static HostBlk<T> build_blk_host(const HostCSR &m, bool upper, int P) {
     const int nr = st.p1 - st.p0;
     unsigned char *base = reinterpret_cast<unsigned char *>(plan.data()) + boff[s];
     int4 *hdr = reinterpret_cast<int4 *>(base);
-    *hdr = make_int4(nr, st.nent, 0, 0);
+    *hdr = make_int4(nr, st.nent, same[s], 0);
     int4 *rows = reinterpret_cast<int4 *>(base + 16);
     int *code = reinterpret_cast<int *>(base + 16 + 16 * nr);
     T *val = reinterpret_cast<T *>(base + blk_off_val<T>(nr, st.nent));
@@ -3674,7 +3681,7 @@ static HostBlk<T> build_blk_host(const HostCSR &m, bool upper, int P) {
       rows[q - st.p0] = make_int4(o, e, m.irp[o + 1] - m.irp[o], q);
       for (int k = m.irp[o]; k < m.irp[o + 1]; ++k, ++e) {
         const int jp = lowcol(m.ja[k]);
-        const bool ring = blk[jp] == st.b && lpos[jp] >= st.p1 - W;
+        const bool ring = blk[jp] == st.b && lpos[jp] >= lvl_end[s] - W;
         code[e] = ring ? (lpos[jp] & (W - 1)) : -(orig(jp) + 1);
         val[e] = (T)m.val[k];
       }
@@ -3686,9 +3693,10 @@ static HostBlk<T> build_blk_host(const HostCSR &m, bool upper, int P) {
   w.nsteps = ns;
   w.W = W;
   w.stage_bytes = capB;
+  w.aux_cap = capA;
   w.nnz = m.nnz();
   w.plan_bytes = boff[ns];
-  w.smem = (size_t)W * sizeof(T) + (size_t)kBlkD * capB + 8 * kBlkD;
+  w.smem = blk_smem<T>(W, capB, capA);
   if (w.smem > 220 * 1024) return w;
   w.bstep = std::move(bstep);
   w.sdesc = std::move(sdesc);
@@ -3707,6 +3715,7 @@ static DBlk<T> build_blk_plan(Arena &ar, const HostCSR &m, bool upper, int P) {
   w.nsteps = hb.nsteps;
   w.W = hb.W;
   w.stage_bytes = hb.stage_bytes;
+  w.aux_cap = hb.aux_cap;
   w.nnz = hb.nnz;
   w.plan_bytes = hb.plan_bytes;
   w.smem = hb.smem;
@@ -3743,6 +3752,27 @@ static int64_t blk_emulate(const HostBlk<T> &w, const HostCSR &m, const std::vec
   for (int b = 0; b < w.nblocks; ++b) {
     std::vector<int> ring_row((size_t)W, -1);  // original row whose value a slot holds
     if (w.bstep[b + 1] < w.bstep[b]) return bad + 1;
+    // the steps of one level are solved without a barrier between them: their
+    // values become visible at the next level's barrier, and no slot the level
+    // reads may be written by it
+    std::vector<std::pair<int, double>> pend;  // original row, value
+    std::vector<int> pend_slot;
+    std::vector<char> read_slot((size_t)W, 0);
+    auto flush = [&]() {
+      for (size_t q = 0; q < pend.size(); ++q) {
+        const int slot = pend_slot[q], row = pend[q].first;
+        if (read_slot[slot]) ++bad;  // a slot written while the level still reads it
+        ring[slot] = pend[q].second;
+        ring_row[slot] = row;
+        if (written[row]) ++bad;
+        cur[row] = pend[q].second;
+        written[row] = 1;
+        t[row] = pend[q].second;
+      }
+      pend.clear();
+      pend_slot.clear();
+      std::fill(read_slot.begin(), read_slot.end(), 0);
+    };
     for (int s = w.bstep[b]; s < w.bstep[b + 1]; ++s) {
       const int2 dsc = w.sdesc[s];
       const int64_t off = (int64_t)dsc.x * 16, bytes = (int64_t)dsc.y * 16;
@@ -3752,15 +3782,15 @@ static int64_t blk_emulate(const HostBlk<T> &w, const HostCSR &m, const std::vec
       }
       const unsigned char *st = planb + off;
       const int4 hdr = *reinterpret_cast<const int4 *>(st);
-      if (hdr.x < 0 || hdr.y < 0 || blk_bytes<T>(hdr.x, hdr.y) > bytes) {
+      if (hdr.x < 0 || hdr.y < 0 || blk_bytes<T>(hdr.x, hdr.y) > bytes || 2 * hdr.x + hdr.y > w.aux_cap ||
+          (hdr.z != 0 && hdr.z != 1) || (hdr.z && s == w.bstep[b])) {
         ++bad;
         continue;
       }
+      if (!hdr.z) flush();  // a new level
       const int4 *rows = reinterpret_cast<const int4 *>(st + 16);
       const int *code = reinterpret_cast<const int *>(st + 16 + 16 * hdr.x);
       const T *val = reinterpret_cast<const T *>(st + blk_off_val<T>(hdr.x, hdr.y));
-      std::vector<std::pair<int, double>> outv;
-      std::vector<char> read_slot((size_t)W, 0);
       for (int r = 0; r < hdr.x; ++r) {
         const int4 rw = rows[r];
         if (rw.x < 0 || rw.x >= n || rw.y < 0 || rw.z < 0 || rw.y + rw.z > hdr.y ||
@@ -3792,21 +3822,11 @@ static int64_t blk_emulate(const HostBlk<T> &w, const HostCSR &m, const std::vec
           acc += (double)val[e] * dv;
         }
         const double sc = scale ? scale[rw.x] : 1.0;
-        outv.emplace_back(r, sc * rhs[rw.x] - acc);
-      }
-      // the step's values become visible after its barrier
-      for (auto &pr : outv) {
-        const int4 rw = rows[pr.first];
-        const int slot = rw.w & (W - 1);
-        if (read_slot[slot]) ++bad;  // a slot written while the step still reads it
-        ring[slot] = pr.second;
-        ring_row[slot] = rw.x;
-        if (written[rw.x]) ++bad;
-        cur[rw.x] = pr.second;
-        written[rw.x] = 1;
-        t[rw.x] = pr.second;
+        pend.emplace_back(rw.x, sc * rhs[rw.x] - acc);
+        pend_slot.push_back(rw.w & (W - 1));
       }
     }
+    flush();
   }
   for (int i = 0; i < n; ++i) bad += !written[i];
   return bad;
