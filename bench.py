@@ -192,7 +192,8 @@ def oracle_prec(orc, ao, smoother):
 # the V-cycle precision forms (PRECISION keyword of the host mirror)
 FORM_TEXT = {"FP64": "FP64", "FP32": "FP32",
              "FP32_P16": "FP32 with FP16 prolongator values (FP32 row scales)",
-             "FP32_H16": "FP32 arithmetic on FP16 operator values (FP32 row scales for A, P, R, ND)"}
+             "FP32_H16": "FP32 arithmetic on FP16 operator values (FP32 row scales for A, P, R, ND)",
+             "FP64_REFERENCE": "FP64, the reference's only form, on the host cores"}
 
 
 def workload_config(args, world, a=None, p=None, precision=None):
@@ -242,7 +243,7 @@ def run_reference(args, rank, world):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * s_per_solve, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(args, world, precision="FP64 (the reference's only form)"),
+        "config": workload_config(args, world, precision="FP64_REFERENCE"),
         "iterations": its_full, "final_relres": rr_full, "hierarchy_build_s": t_build,
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": orc.num_threads(),
                          "kind": "port",

@@ -1388,9 +1388,10 @@ __global__ void __launch_bounds__(256) k_kry_spmv_sell(int nr, const int *__rest
 }
 
 // k_kry_spmv on the HDIA copy of A (one thread per row, a warp per slice:
-// the rows and the reduction order of k_kry_spmv_sell)
+// the rows and the reduction order of k_kry_spmv_sell; two diagonals' loads
+// per pass keep it at 40 registers, six 256-thread blocks per SM)
 template <typename ZT>
-__global__ void __launch_bounds__(256) k_kry_spmv_hdia(int nr, const int *__restrict__ dptr,
+__global__ void __launch_bounds__(256, 6) k_kry_spmv_hdia(int nr, const int *__restrict__ dptr,
                                                        const int *__restrict__ doff, const double *__restrict__ hv,
                                                        const ZT *__restrict__ z, double *d0, double *d1,
                                                        double *__restrict__ q, const double *__restrict__ r,
@@ -1411,8 +1412,8 @@ __global__ void __launch_bounds__(256) k_kry_spmv_hdia(int nr, const int *__rest
   for (int sl = warp; sl < ns; sl += nwarps) {
     const int row = (sl << 5) + lane;
     const double s =
-        first ? hdia_row<double>(dptr, doff, hv, sl, row, nr, lane, [&](int j) { return (double)__ldg(z + j); })
-              : hdia_row<double>(dptr, doff, hv, sl, row, nr, lane,
+        first ? hdia_row<double, 2>(dptr, doff, hv, sl, row, nr, lane, [&](int j) { return (double)__ldg(z + j); })
+              : hdia_row<double, 2>(dptr, doff, hv, sl, row, nr, lane,
                                  [&](int j) { return fma(beta, dold[j], (double)__ldg(z + j)); });
     if (row < nr) {
       const double di = first ? (double)z[row] : fma(beta, dold[row], (double)z[row]);
