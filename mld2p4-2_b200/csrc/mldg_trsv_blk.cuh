@@ -5,13 +5,14 @@
 // dependency is an earlier row).  The rows are split into P contiguous
 // blocks; CTA b solves block b by itself, walking the block's rows in steps:
 // a step is a set of the block's rows on one global dependency level (or a
-// part of one), so the rows of a step are independent of each other and one
-// __syncthreads separates consecutive steps.  Dependencies are of two kinds:
+// part of one), so the rows of a level are independent of each other and a
+// barrier of the solving warps separates consecutive levels.  Dependencies
+// are of two kinds:
 //   * local: an earlier row of the same block, read from a shared-memory
 //     ring of the block's last W solution values (indexed by the row's local
-//     position mod W); the host checks that the slot has not been
-//     overwritten yet (q >= end of the reading step - W), else the entry is
-//     read as a remote one;
+//     position mod W); the host checks that the slot cannot be overwritten
+//     while the reading level runs (q >= end of the reading level - W), else
+//     the entry is read as a remote one;
 //   * remote: a row of an earlier block (or a local row older than the ring),
 //     read from the exchange vector `cur` in global memory, which holds a
 //     signalling-NaN sentinel until its row is solved; the reader re-polls,
